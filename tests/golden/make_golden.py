@@ -1,0 +1,142 @@
+"""Generate the golden fixtures in tests/golden/ from the pEVSL reference.
+
+Runs oracle/_ref/libpevsl_ref.so (the reference compiled from its own sources
+by oracle/Makefile; needs the reference tree, so this runs where the
+reference is mounted, never on a GPU box) and writes small JSON files that
+the CPU tests use to pin the oracle restatement and the GPU tests use as
+known answers.  Floats are written with repr() so they round-trip exactly.
+
+    python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+from checkers import Checker, RunSpec, laplacian  # noqa: E402
+
+
+def fl(x):
+    return [float(v) for v in np.asarray(x).ravel()]
+
+
+def dump(name, obj):
+    path = os.path.join(HERE, name)
+    with open(path, "w") as f:
+        json.dump(obj, f, indent=1)
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def pipeline_case(ref, grid, spec: RunSpec):
+    A = laplacian(*grid)
+    r = ref.pipeline(A, spec)
+    return dict(
+        grid=list(grid), spec=spec.__dict__, status=r.status, lmin=r.lmin, lmax=r.lmax,
+        ecount=r.ecount, npts=r.npts, mu=fl(r.mu) if spec.dos_type == 0 else None,
+        sli=fl(r.sli), deg=[int(v) for v in r.deg], ptype=[int(v) for v in r.ptype],
+        gam=fl(r.gam), bar=fl(r.bar), nev=[int(v) for v in r.nev], its=[int(v) for v in r.its],
+        lam=[fl(x) for x in r.lam], res=[fl(x) for x in r.res])
+
+
+def main():
+    ref = Checker("ref")
+
+    # 1. SpMV, input sin(i) as TESTS0/Matvec/test1.c:70-85 (3D and 2D grids)
+    mv = {}
+    for grid in ((8, 8, 8), (12, 10, 1)):
+        A = laplacian(*grid)
+        x = np.sin(np.arange(A.n, dtype=np.float64))
+        mv["x".join(map(str, grid))] = dict(grid=list(grid), y=fl(ref.matvec(A, x)))
+    dump("matvec_sin.json", mv)
+
+    # 2. KPM moments + slicer + filters on the README matrix (hand-set bounds)
+    A = laplacian(20, 20, 20)
+    intv = [0.6, 1.2, 0.0, 12.0]
+    kpm = {}
+    for mode in (0, 1):
+        ref.set_rng(mode, 0)
+        r, mu, ec = ref.kpmdos(A, 300, 1, 60, intv)
+        npts = int(10 * ec)
+        rs, sli = ref.spslicer_kpm(mu, 300, intv, 5, npts)
+        pols = []
+        for sl in range(5):
+            _, p = ref.findpol([sli[sl], sli[sl + 1], 0.0, 12.0])
+            pols.append(dict(intv=[float(sli[sl]), float(sli[sl + 1]), 0.0, 12.0],
+                             type=p["type"], deg=p["deg"], gam=p["gam"], bar=p["bar"],
+                             cc=p["cc"], dd=p["dd"], mu=fl(p["mu"])))
+        kpm["glibc" if mode == 0 else "gauss"] = dict(
+            status=r, mu=fl(mu), ecount=ec, npts=npts, slicer_status=rs, sli=fl(sli), pols=pols)
+    dump("lap20_kpm.json", dict(grid=[20, 20, 20], intv=intv, Mdeg=300, damping=1, nvec=60,
+                                seed=0, cases=kpm))
+
+    # 3. Filter design edge cases: end intervals (chext), forced degree,
+    #    every damping type, invalid intervals (check_intv codes)
+    cases = []
+    for intv_c, kw in (([0.0, 0.5, 0.0, 12.0], {}), ([-1.0, 0.5, 0.0, 12.0], {}),
+                       ([11.0, 12.0, 0.0, 12.0], {}), ([11.5, 13.0, 0.0, 12.0], {}),
+                       ([0.8, 0.82, 0.0, 12.0], {}), ([3.0, 3.5, 0.0, 12.0], {"damping": 0}),
+                       ([3.0, 3.5, 0.0, 12.0], {"damping": 1}), ([3.0, 3.5, 0.0, 12.0], {"deg_in": 40}),
+                       ([0.0, 0.5, 0.0, 12.0], {"deg_in": 25}),
+                       ([2.0, 2.5, 0.0, 8.0], {"thresh_int": 0.6, "thresh_ext": 0.15}),
+                       ([1.0, 0.5, 0.0, 12.0], {}), ([13.0, 14.0, 0.0, 12.0], {})):
+        r, p = ref.findpol(intv_c, **kw)
+        c = dict(intv=intv_c, kw=kw, status=r)
+        if p is not None:
+            c.update(type=p["type"], deg=p["deg"], gam=p["gam"], bar=p["bar"], cc=p["cc"],
+                     dd=p["dd"], mu=fl(p["mu"]))
+        cases.append(c)
+    dump("findpol_cases.json", dict(cases=cases))
+
+    # 4. Slicer edge cases: one slice, many slices, invalid interval
+    ref.set_rng(1, 7)
+    A = laplacian(10, 10, 10)
+    intv = [0.5, 3.0, 0.0, 12.0]
+    _, mu, ec = ref.kpmdos(A, 80, 1, 20, intv)
+    sl_cases = []
+    for n_int, npts in ((1, 50), (4, int(10 * ec)), (9, 30), (4, 3)):
+        r, sli = ref.spslicer_kpm(mu, 80, intv, n_int, npts)
+        sl_cases.append(dict(n_int=n_int, npts=npts, status=r, sli=fl(sli)))
+    r, _ = ref.spslicer_kpm(mu, 80, [3.0, 0.5, 0.0, 12.0], 4, 40)
+    sl_cases.append(dict(n_int=4, npts=40, intv=[3.0, 0.5, 0.0, 12.0], status=r))
+    dump("spslicer_cases.json", dict(grid=[10, 10, 10], intv=intv, Mdeg=80, mu=fl(mu),
+                                     ecount=ec, cases=sl_cases))
+
+    # 5. Lanczos DOS + its slicer, and thick-restart bounds
+    A = laplacian(12, 12, 12)
+    ref.set_rng(1, 3)
+    r, xd, yd, ne = ref.landos(A, 10, 40, 200, [0.5, 6.0, 0.0, 12.0])
+    sli = ref.spslicer_lan(xd, yd, 4)
+    v0 = np.cos(np.arange(A.n, dtype=np.float64))
+    bnd = {}
+    for bt in (1, 2):
+        ref.set_rng(1, 3)
+        rb, lo, hi = ref.lantrbounds(A, 50, 200, 1e-8, v0, bt)
+        bnd[str(bt)] = dict(status=rb, lmin=lo, lmax=hi)
+    dump("lanczos_cases.json", dict(grid=[12, 12, 12], landos=dict(
+        nvec=10, msteps=40, npts=200, intv=[0.5, 6.0, 0.0, 12.0], seed=3, status=r, xdos=fl(xd),
+        ydos=fl(yd), neig=ne, sli4=fl(sli)), lantrbounds=dict(v0="cos(i)", lanm=50, maxit=200,
+                                                              tol=1e-8, cases=bnd)))
+
+    # 6. Whole runs: small 3D and 2D Laplacians, and the README matrix with
+    #    (a) hand-set bounds / glibc stream, (b) LanTrbounds / Gaussian stream,
+    #    (c) Lanczos DOS
+    runs = {}
+    runs["lap10_kpm_gauss"] = pipeline_case(
+        ref, (10, 10, 10), RunSpec(0.6, 2.0, 3, Mdeg=100, nvec=20, rng_mode=1, seed=11))
+    runs["lap30x30_kpm_glibc"] = pipeline_case(
+        ref, (30, 30, 1), RunSpec(1.0, 2.0, 2, lmax=8.0, Mdeg=120, nvec=20, rng_mode=0, seed=5))
+    runs["lap20_readme_glibc"] = pipeline_case(ref, (20, 20, 20), RunSpec(0.6, 1.2, 5))
+    runs["lap20_lantr_gauss"] = pipeline_case(
+        ref, (20, 20, 20), RunSpec(0.6, 1.2, 5, bounds_mode=1, rng_mode=1, seed=0))
+    runs["lap12_landos_gauss"] = pipeline_case(
+        ref, (12, 12, 12), RunSpec(0.5, 2.5, 3, dos_type=1, nvec=10, rng_mode=1, seed=2))
+    dump("pipelines.json", runs)
+
+
+if __name__ == "__main__":
+    main()
