@@ -1,0 +1,546 @@
+"""pevsl_b200 — pEVSL's spectrum-slicing eigensolver on one NVIDIA B200.
+
+The product is the C-ABI library ``libpevsl_b200.so`` (built in-tree by
+``pevsl_b200.build``) that exports the pEVSL C API (include/pevsl.h) plus the
+extensions of include/pevsl_b200.h.  This module binds it with ctypes and
+mirrors the reference's driver-level interface (TESTS/Lap/LapPLanN.c,
+TESTS/MM/MMPLanN.c) so tests and benchmarks read like the reference drivers:
+
+    lib = pevsl_b200.load()
+    A = pevsl_b200.Matrix.from_csr(n, ia, ja, a)
+    with pevsl_b200.Instance(A) as ev:
+        mu, ecnt = ev.kpmdos(Mdeg=300, damping=1, nvec=60, intv=[a, b, lmin, lmax])
+        ...
+
+There is no CPU fallback: ``load()`` raises if the library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpevsl_b200.so")
+
+RNG_GLIBC = 0
+RNG_GAUSS = 1
+
+# error codes of include/pevsl.h
+PEVSL_NOT_IMPLEMENT = 11
+ERR_CUDA = -1001
+ERR_NOMEM = -1002
+ERR_ARG = -1003
+ERR_NOMATVEC = -1004
+ERR_NONFINITE = -1005
+ERR_EIG = -1006
+
+
+class PevslError(RuntimeError):
+    pass
+
+
+# ---------------------------------------------------------------- structs
+class Csr(C.Structure):
+    _fields_ = [("nrows", C.c_int), ("ncols", C.c_int), ("ia", C.POINTER(C.c_int)),
+                ("ja", C.POINTER(C.c_int)), ("a", C.POINTER(C.c_double))]
+
+
+class Parcsr(C.Structure):
+    _fields_ = [("comm", C.c_int), ("comm_handle", C.c_void_p),
+                ("nrow_global", C.c_int), ("ncol_global", C.c_int),
+                ("nrow_local", C.c_int), ("ncol_local", C.c_int),
+                ("row_starts", C.POINTER(C.c_int)), ("col_starts", C.POINTER(C.c_int)),
+                ("first_row", C.c_int), ("first_col", C.c_int),
+                ("diag", C.POINTER(Csr)), ("offd", C.POINTER(Csr)),
+                ("col_map_offd", C.POINTER(C.c_int))]
+
+
+class Parvec(C.Structure):
+    _fields_ = [("comm", C.c_int), ("n_global", C.c_int), ("n_local", C.c_int),
+                ("n_first", C.c_int), ("data", C.c_void_p)]
+
+
+class Parvecs(C.Structure):
+    _fields_ = [("comm", C.c_int), ("n_global", C.c_int), ("n_local", C.c_int),
+                ("n_first", C.c_int), ("n_vecs", C.c_int), ("ld", C.c_int),
+                ("data", C.c_void_p)]
+
+
+class Polparams(C.Structure):
+    _fields_ = [("max_deg", C.c_int), ("min_deg", C.c_int), ("damping", C.c_int),
+                ("thresh_ext", C.c_double), ("thresh_int", C.c_double),
+                ("intvtol", C.c_double), ("type", C.c_int), ("mu", C.POINTER(C.c_double)),
+                ("cc", C.c_double), ("dd", C.c_double), ("gam", C.c_double),
+                ("bar", C.c_double), ("deg", C.c_int)]
+
+
+class PevslData(C.Structure):
+    _fields_ = [("comm", C.c_int), ("N", C.c_int), ("n", C.c_int), ("nfirst", C.c_int),
+                ("ifGenEv", C.c_int), ("Amv", C.c_void_p), ("Bmv", C.c_void_p),
+                ("Bsol", C.c_void_p), ("LTsol", C.c_void_p), ("stats", C.c_void_p),
+                ("nev_computed", C.c_int), ("eval_computed", C.POINTER(C.c_double)),
+                ("evec_computed", C.c_void_p), ("sigma_mult", C.c_double)]
+
+
+MVFUNC = C.CFUNCTYPE(None, C.c_void_p, C.c_void_p, C.c_void_p)
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+_vp = C.c_void_p
+_D = C.c_double
+_I = C.c_int
+
+# (name, restype, argtypes) of every exported symbol the binding uses; the
+# CPU test suite checks that each one exists in the library.
+SIGNATURES = [
+    ("pEVSL_Start", _I, [_I, C.POINTER(C.POINTER(PevslData))]),
+    ("pEVSL_Finish", _I, [C.POINTER(PevslData)]),
+    ("pEVSL_SetAParcsr", _I, [C.POINTER(PevslData), C.POINTER(Parcsr)]),
+    ("pEVSL_SetAMatvec", _I, [C.POINTER(PevslData), MVFUNC, _vp]),
+    ("pEVSL_SetProbSizes", _I, [C.POINTER(PevslData), _I, _I, _I]),
+    ("pEVSL_SetStdEig", _I, [C.POINTER(PevslData)]),
+    ("pEVSL_SetGenEig", _I, [C.POINTER(PevslData)]),
+    ("pEVSL_SetSigmaMult", _I, [C.POINTER(PevslData), _D]),
+    ("pEVSL_ParcsrCreate", _I, [_I, _I, _ip, _ip, C.POINTER(Parcsr), _I]),
+    ("pEVSL_ParcsrSetup", _I, [C.POINTER(Csr), C.POINTER(Parcsr)]),
+    ("pEVSL_ParcsrFree", None, [C.POINTER(Parcsr)]),
+    ("pEVSL_ParcsrMatvec", None, [C.POINTER(Parcsr), C.POINTER(Parvec), C.POINTER(Parvec)]),
+    ("pEVSL_ParcsrMatvec0", None, [_vp, _vp, _vp]),
+    ("pEVSL_ParcsrNnz", _I, [C.POINTER(Parcsr)]),
+    ("pEVSL_ParcsrGetLocalMat", _I, [C.POINTER(Parcsr), _I, _vp, C.POINTER(Csr), C.c_char]),
+    ("pEVSL_ParvecCreate", None, [_I, _I, _I, _I, C.POINTER(Parvec)]),
+    ("pEVSL_ParvecFree", None, [C.POINTER(Parvec)]),
+    ("pEVSL_ParvecRand", None, [C.POINTER(Parvec)]),
+    ("pEVSL_ParvecDot", None, [C.POINTER(Parvec), C.POINTER(Parvec), _dp]),
+    ("pEVSL_ParvecNrm2", None, [C.POINTER(Parvec), _dp]),
+    ("pEVSL_ParvecSum", None, [C.POINTER(Parvec), _dp]),
+    ("pEVSL_ParvecCopy", None, [C.POINTER(Parvec), C.POINTER(Parvec)]),
+    ("pEVSL_ParvecScal", None, [C.POINTER(Parvec), _D]),
+    ("pEVSL_ParvecAxpy", None, [_D, C.POINTER(Parvec), C.POINTER(Parvec)]),
+    ("pEVSL_ParvecSetZero", None, [C.POINTER(Parvec)]),
+    ("pEVSL_ParvecSetScalar", None, [C.POINTER(Parvec), _D]),
+    ("pEVSL_ParvecsCreate", None, [_I, _I, _I, _I, _I, _I, C.POINTER(Parvecs)]),
+    ("pEVSL_ParvecsFree", None, [C.POINTER(Parvecs)]),
+    ("pEVSL_ParvecsGemv", None, [_D, C.POINTER(Parvecs), _I, _dp, _D, C.POINTER(Parvec)]),
+    ("pEVSL_ParvecsGemtv", None, [_D, C.POINTER(Parvecs), _I, C.POINTER(Parvec), _D, _dp]),
+    ("pEVSL_SetPolDef", None, [C.POINTER(Polparams)]),
+    ("pEVSL_FindPol", _I, [_dp, C.POINTER(Polparams)]),
+    ("pEVSL_FreePol", None, [C.POINTER(Polparams)]),
+    ("pEVSL_Kpmdos", _I, [C.POINTER(PevslData), _I, _I, _I, _dp, _I, _I, _I, _dp, _dp]),
+    ("pEVSL_SpslicerKpm", _I, [_dp, _dp, _I, _dp, _I, _I]),
+    ("pEVSL_LanDosG", _I, [C.POINTER(PevslData), _I, _I, _I, _dp, _dp, _dp, _dp, _I, _I, _I]),
+    ("pEVSL_SpslicerLan", None, [_dp, _dp, _I, _I, _dp]),
+    ("pEVSL_LanTrbounds", _I, [C.POINTER(PevslData), _I, _I, _D, C.POINTER(Parvec), _I, _dp,
+                               _dp, _vp]),
+    ("pEVSL_ChebLanNr", _I, [C.POINTER(PevslData), _dp, _I, _D, C.POINTER(Parvec),
+                             C.POINTER(Polparams), _ip, C.POINTER(_dp),
+                             C.POINTER(C.POINTER(Parvecs)), C.POINTER(_dp), _vp]),
+    ("pEVSL_StatsReset", None, [C.POINTER(PevslData)]),
+    ("pEVSL_Part1d", None, [_I, _I, _ip, _ip, _ip, _I]),
+    ("sort_double", None, [_I, _dp, _ip]),
+    ("linspace", None, [_D, _D, _I, _dp]),
+    ("pEVSL_B200_SetRng", _I, [_I, C.c_uint64]),
+    ("pEVSL_B200_RngDraws", C.c_uint64, []),
+    ("pEVSL_B200_LastIterations", _I, [C.POINTER(PevslData)]),
+    ("pEVSL_B200_LastNconv", _I, [C.POINTER(PevslData)]),
+    ("pEVSL_B200_LaunchCount", C.c_uint64, []),
+    ("pEVSL_B200_PhaseMs", _D, [C.POINTER(PevslData), _I]),
+    ("pEVSL_B200_Memcpy", _I, [_vp, _vp, C.c_size_t]),
+    ("pEVSL_B200_Sync", _I, []),
+    ("pEVSL_B200_LastError", _I, []),
+    ("pEVSL_B200_ChebAv", _I, [C.POINTER(PevslData), C.POINTER(Polparams), _vp, _vp]),
+    ("pEVSL_B200_ReleaseWorkspace", None, []),
+    ("pEVSL_B200_Info", _I, [C.c_char_p, _I]),
+]
+
+
+def load(path: str = LIB_PATH):
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise PevslError(f"{path} is missing: build it with `python -m pevsl_b200.build`")
+    lib = C.CDLL(path)
+    for name, res, args in SIGNATURES:
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _check(code, what):
+    if code != 0:
+        raise PevslError(f"{what} returned {code}")
+
+
+def _ptr(a: np.ndarray, t=_dp):
+    return a.ctypes.data_as(t)
+
+
+def set_rng(mode: int, seed: int) -> None:
+    """Choose the random stream: RNG_GLIBC (the reference's rand()) or
+    RNG_GAUSS (Philox Gaussian on the GPU); restarts the draw counter."""
+    _check(load().pEVSL_B200_SetRng(mode, seed), "pEVSL_B200_SetRng")
+
+
+def launch_count() -> int:
+    return int(load().pEVSL_B200_LaunchCount())
+
+
+def info() -> str:
+    buf = C.create_string_buffer(512)
+    load().pEVSL_B200_Info(buf, 512)
+    return buf.value.decode()
+
+
+# ---------------------------------------------------------------- vectors
+class Vector:
+    """A pevsl_Parvec owned by the library (managed memory)."""
+
+    def __init__(self, n: int, values: np.ndarray | None = None):
+        self.lib = load()
+        self.pv = Parvec()
+        self.lib.pEVSL_ParvecCreate(n, n, 0, 1, C.byref(self.pv))
+        if not self.pv.data:
+            raise PevslError("pEVSL_ParvecCreate failed")
+        self.n = n
+        if values is not None:
+            self.set(values)
+
+    def set(self, values: np.ndarray) -> None:
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        assert v.size == self.n
+        _check(self.lib.pEVSL_B200_Memcpy(self.pv.data, v.ctypes.data, 8 * self.n), "memcpy")
+
+    def get(self) -> np.ndarray:
+        out = np.empty(self.n)
+        _check(self.lib.pEVSL_B200_Memcpy(out.ctypes.data, self.pv.data, 8 * self.n), "memcpy")
+        return out
+
+    def free(self) -> None:
+        if self.pv.data:
+            self.lib.pEVSL_ParvecFree(C.byref(self.pv))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- matrix
+class Matrix:
+    """A pevsl_Parcsr set up from a host CSR (one device CSR on the GPU)."""
+
+    def __init__(self):
+        self.lib = load()
+        self.A = Parcsr()
+        self.n = 0
+        self.nnz = 0
+        self._alive = False
+
+    @classmethod
+    def from_csr(cls, n: int, ia: np.ndarray, ja: np.ndarray, a: np.ndarray) -> "Matrix":
+        m = cls()
+        ia = np.ascontiguousarray(ia, dtype=np.int32)
+        ja = np.ascontiguousarray(ja, dtype=np.int32)
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        csr = Csr(n, n, _ptr(ia, _ip), _ptr(ja, _ip), _ptr(a))
+        _check(m.lib.pEVSL_ParcsrCreate(n, n, None, None, C.byref(m.A), 1), "ParcsrCreate")
+        _check(m.lib.pEVSL_ParcsrSetup(C.byref(csr), C.byref(m.A)), "ParcsrSetup")
+        m.n, m.nnz, m._alive = n, int(ia[-1]), True
+        return m
+
+    def matvec(self, x: np.ndarray) -> np.ndarray:
+        xv, yv = Vector(self.n, x), Vector(self.n)
+        self.lib.pEVSL_ParcsrMatvec(C.byref(self.A), C.byref(xv.pv), C.byref(yv.pv))
+        _check(self.lib.pEVSL_B200_LastError(), "ParcsrMatvec")
+        return yv.get()
+
+    def free(self) -> None:
+        if self._alive:
+            self.lib.pEVSL_ParcsrFree(C.byref(self.A))
+            self._alive = False
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------- filters
+@dataclass
+class Filter:
+    type: int
+    deg: int
+    gam: float
+    bar: float
+    cc: float
+    dd: float
+    mu: np.ndarray
+
+
+def findpol(intv, max_deg=3000, damping=2, thresh_int=0.8, thresh_ext=0.2, deg_in=0):
+    """pEVSL_SetPolDef + the driver overrides + pEVSL_FindPol
+    (TESTS/Lap/LapPLanN.c:214-226).  Returns (code, Filter or None)."""
+    lib = load()
+    pol = Polparams()
+    lib.pEVSL_SetPolDef(C.byref(pol))
+    pol.damping, pol.thresh_int, pol.thresh_ext = damping, thresh_int, thresh_ext
+    pol.max_deg, pol.deg = max_deg, deg_in
+    iv = np.asarray(intv, dtype=np.float64)
+    r = lib.pEVSL_FindPol(_ptr(iv), C.byref(pol))
+    if r:
+        return r, None
+    mu = np.ctypeslib.as_array(pol.mu, shape=(pol.deg + 1,)).copy()
+    f = Filter(pol.type, pol.deg, pol.gam, pol.bar, pol.cc, pol.dd, mu)
+    lib.pEVSL_FreePol(C.byref(pol))
+    return 0, f
+
+
+def _polparams(f: Filter):
+    pol = Polparams()
+    load().pEVSL_SetPolDef(C.byref(pol))
+    mu = np.ascontiguousarray(f.mu, dtype=np.float64)
+    pol.type, pol.deg, pol.gam, pol.bar, pol.cc, pol.dd = f.type, f.deg, f.gam, f.bar, f.cc, f.dd
+    pol.mu = _ptr(mu)
+    return pol, mu
+
+
+def spslicer_kpm(mu, Mdeg, intv, n_int, npts):
+    sli = np.zeros(n_int + 1)
+    mu = np.ascontiguousarray(mu, dtype=np.float64)
+    iv = np.asarray(intv, dtype=np.float64)
+    r = load().pEVSL_SpslicerKpm(_ptr(sli), _ptr(mu), Mdeg, _ptr(iv), n_int, npts)
+    return r, sli
+
+
+def spslicer_lan(xi, yi, n_int):
+    xi = np.ascontiguousarray(xi, dtype=np.float64)
+    yi = np.ascontiguousarray(yi, dtype=np.float64).copy()
+    sli = np.zeros(n_int + 1)
+    load().pEVSL_SpslicerLan(_ptr(xi), _ptr(yi), n_int, len(xi), _ptr(sli))
+    return sli
+
+
+# ---------------------------------------------------------------- instance
+class Instance:
+    """One pEVSL instance (pEVSL_Start ... pEVSL_Finish) bound to a matrix."""
+
+    def __init__(self, A: Matrix | None = None):
+        self.lib = load()
+        self.p = C.POINTER(PevslData)()
+        _check(self.lib.pEVSL_Start(1, C.byref(self.p)), "pEVSL_Start")
+        self.A = A
+        if A is not None:
+            _check(self.lib.pEVSL_SetAParcsr(self.p, C.byref(A.A)), "SetAParcsr")
+
+    @property
+    def n(self) -> int:
+        return self.p.contents.n
+
+    def close(self):
+        if self.p:
+            self.lib.pEVSL_Finish(self.p)
+            self.p = C.POINTER(PevslData)()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def kpmdos(self, Mdeg, damping, nvec, intv):
+        mu = np.zeros(Mdeg + 1)
+        ec = C.c_double()
+        iv = np.asarray(intv, dtype=np.float64)
+        r = self.lib.pEVSL_Kpmdos(self.p, Mdeg, damping, nvec, _ptr(iv), 1, 0, 0, _ptr(mu),
+                                  C.byref(ec))
+        return r, mu, ec.value
+
+    def landos(self, nvec, msteps, npts, intv):
+        xd, yd = np.zeros(npts), np.zeros(npts)
+        ne = C.c_double()
+        iv = np.asarray(intv, dtype=np.float64)
+        r = self.lib.pEVSL_LanDosG(self.p, nvec, msteps, npts, _ptr(xd), _ptr(yd), C.byref(ne),
+                                   _ptr(iv), 1, 0, 0)
+        return r, xd, yd, ne.value
+
+    def lantrbounds(self, lanm, maxit, tol, vinit: np.ndarray, bndtype=1):
+        v = Vector(self.n, vinit)
+        lo, hi = C.c_double(), C.c_double()
+        r = self.lib.pEVSL_LanTrbounds(self.p, lanm, maxit, tol, C.byref(v.pv), bndtype,
+                                       C.byref(lo), C.byref(hi), None)
+        return r, lo.value, hi.value
+
+    def chebav(self, f: Filter, v: np.ndarray) -> np.ndarray:
+        pol, _keep = _polparams(f)
+        vv, yv = Vector(self.n, v), Vector(self.n)
+        _check(self.lib.pEVSL_B200_ChebAv(self.p, C.byref(pol), vv.pv.data, yv.pv.data), "ChebAv")
+        return yv.get()
+
+    def cheblannr(self, intv, maxit, tol, vinit, f: Filter, want_vectors=False):
+        """pEVSL_ChebLanNr; pairs sorted ascending as the drivers do."""
+        pol, _keep = _polparams(f)
+        v = vinit if isinstance(vinit, Vector) else Vector(self.n, vinit)
+        iv = np.asarray(intv, dtype=np.float64)
+        nev = C.c_int()
+        lam, res = _dp(), _dp()
+        W = C.POINTER(Parvecs)()
+        r = self.lib.pEVSL_ChebLanNr(self.p, _ptr(iv), maxit, tol, C.byref(v.pv), C.byref(pol),
+                                     C.byref(nev), C.byref(lam), C.byref(W), C.byref(res), None)
+        out = dict(status=r, nev=nev.value, its=self.lib.pEVSL_B200_LastIterations(self.p),
+                   nconv=self.lib.pEVSL_B200_LastNconv(self.p))
+        m = nev.value
+        libc = C.CDLL(None)
+        libc.free.argtypes = [_vp]
+        if r == 0:
+            lam_a = np.ctypeslib.as_array(lam, shape=(m,)).copy() if m else np.zeros(0)
+            res_a = np.ctypeslib.as_array(res, shape=(m,)).copy() if m else np.zeros(0)
+            order = np.argsort(lam_a, kind="stable")
+            out["lam"], out["res"] = lam_a[order], res_a[order]
+            if want_vectors and m:
+                Wh = np.empty((W.contents.n_vecs, W.contents.ld))
+                _check(self.lib.pEVSL_B200_Memcpy(Wh.ctypes.data, W.contents.data, Wh.nbytes),
+                       "memcpy")
+                out["W"] = Wh[order, : self.n].copy() if m else None
+            if lam:
+                libc.free(C.cast(lam, _vp))
+            if res:
+                libc.free(C.cast(res, _vp))
+            if W:
+                self.lib.pEVSL_ParvecsFree(W)
+                libc.free(C.cast(W, _vp))
+        for k, ph in (("t_iter_ms", 2), ("t_pol_ms", 3), ("t_reorth_ms", 4), ("t_ritz_ms", 5)):
+            out[k] = self.lib.pEVSL_B200_PhaseMs(self.p, ph)
+        return out
+
+
+# ---------------------------------------------------------------- whole run
+@dataclass
+class SliceRun:
+    """Inputs of one spectrum-slicing run (the driver sequence of
+    TESTS/Lap/LapPLanN.c with the bounds step of TESTS/MM/MMPLanN.c)."""
+    a_lo: float
+    b_hi: float
+    nslices: int
+    bounds_mode: int = 0          # 0: lmin/lmax given, 1: pEVSL_LanTrbounds
+    lmin: float = 0.0
+    lmax: float = 12.0
+    lan_lanm: int = 50
+    lan_maxit: int = 200
+    lan_bndtype: int = 1
+    lan_tol: float = 1e-8
+    dos_type: int = 0             # 0: KPM, 1: Lanczos DOS
+    Mdeg: int = 300
+    kpm_damping: int = 1
+    nvec: int = 60
+    landos_msteps: int = 40
+    landos_npts: int = 200
+    pol_damping: int = 2
+    pol_max_deg: int = 3000
+    thresh_int: float = 0.8
+    thresh_ext: float = 0.2
+    tol: float = 1e-8
+    mlan_min: int = 300
+    rng_mode: int = RNG_GLIBC
+    seed: int = 0
+
+
+@dataclass
+class SliceResult:
+    lmin: float
+    lmax: float
+    ecount: float
+    npts: int
+    status: int
+    mu: np.ndarray
+    sli: np.ndarray
+    deg: list = field(default_factory=list)
+    ptype: list = field(default_factory=list)
+    gam: list = field(default_factory=list)
+    bar: list = field(default_factory=list)
+    nev: list = field(default_factory=list)
+    its: list = field(default_factory=list)
+    lam: list = field(default_factory=list)
+    res: list = field(default_factory=list)
+    times: dict = field(default_factory=dict)
+
+
+def solve_interval(A: Matrix, s: SliceRun) -> SliceResult:
+    """Run the whole slicing path through the C API, in the reference
+    drivers' order: start vector, bounds, DOS, slicer, then each slice."""
+    import time
+    lib = load()
+    t_all = time.perf_counter()
+    set_rng(s.rng_mode, s.seed)
+    with Instance(A) as ev:
+        # pEVSL_Start reseeds rand() with srand(0); restart the chosen stream
+        set_rng(s.rng_mode, s.seed)
+        vinit = Vector(A.n)
+        lib.pEVSL_ParvecRand(C.byref(vinit.pv))
+        times = {}
+        t = time.perf_counter()
+        if s.bounds_mode == 1:
+            lo, hi = C.c_double(), C.c_double()
+            r = lib.pEVSL_LanTrbounds(ev.p, s.lan_lanm, s.lan_maxit, s.lan_tol, C.byref(vinit.pv),
+                                      s.lan_bndtype, C.byref(lo), C.byref(hi), None)
+            _check(r, "LanTrbounds")
+            lmin, lmax = lo.value, hi.value
+        else:
+            lmin, lmax = s.lmin, s.lmax
+        times["bounds"] = time.perf_counter() - t
+        intv = [s.a_lo, s.b_hi, lmin, lmax]
+        status = 0
+        t = time.perf_counter()
+        mu = np.zeros(s.Mdeg + 1)
+        if s.dos_type == 0:
+            r, mu, ecount = ev.kpmdos(s.Mdeg, s.kpm_damping, s.nvec, intv)
+            if r:
+                status = 100 + r
+            npts = int(10 * ecount)
+            times["dos"] = time.perf_counter() - t
+            r, sli = spslicer_kpm(mu, s.Mdeg, intv, s.nslices, npts)
+            if r and not status:
+                status = 200 + r
+        else:
+            r, xd, yd, ecount = ev.landos(s.nvec, s.landos_msteps, s.landos_npts, intv)
+            if r:
+                status = 100 + r
+            npts = s.landos_npts
+            times["dos"] = time.perf_counter() - t
+            sli = spslicer_lan(xd, yd, s.nslices)
+        res = SliceResult(lmin, lmax, ecount, npts, status, mu, sli)
+        ev_int = int(1 + ecount / float(s.nslices))
+        t = time.perf_counter()
+        for sl in range(s.nslices):
+            nev = ev_int + 2
+            mlan = min(max(5 * nev, s.mlan_min), A.n)
+            iv = [sli[sl], sli[sl + 1], lmin, lmax]
+            r, f = findpol(iv, s.pol_max_deg, s.pol_damping, s.thresh_int, s.thresh_ext)
+            if r:
+                res.status = res.status or 300 + abs(r)
+                continue
+            out = ev.cheblannr(iv, mlan, s.tol, vinit, f)
+            if out["status"] and not res.status:
+                res.status = 300 + abs(out["status"])
+            res.deg.append(f.deg)
+            res.ptype.append(f.type)
+            res.gam.append(f.gam)
+            res.bar.append(f.bar)
+            res.nev.append(out["nev"])
+            res.its.append(out["its"])
+            res.lam.append(out.get("lam", np.zeros(0)))
+            res.res.append(out.get("res", np.zeros(0)))
+        times["slices"] = time.perf_counter() - t
+        times["total"] = time.perf_counter() - t_all
+        res.times = times
+        vinit.free()
+    return res

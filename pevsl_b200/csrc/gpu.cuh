@@ -1,0 +1,144 @@
+/*
+ * pevsl-b200 device runtime shared by the CUDA modules: the per-process GPU
+ * context (one stream, reduction scratch, device scalars, cached
+ * workspaces), launch accounting, and the host-callable wrappers of the
+ * kernels.  Everything is enqueued on the context stream; wrappers return 0
+ * or PEVSL_ERR_CUDA and never synchronise unless their name says so.
+ */
+#ifndef PEVSL_B200_GPU_CUH
+#define PEVSL_B200_GPU_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace pv {
+
+constexpr int kThreads = 256;      /* block size of the streaming kernels      */
+constexpr int kMaxRedBlocks = 1184; /* 8 x 148 SMs: partial sums per reduction */
+
+/* device scalar slots (doubles) */
+enum Slot {
+  S_ALPHA = 0,
+  S_BETA = 1,
+  S_NRM0 = 2,
+  S_NRM = 3,
+  S_TMP0 = 4,
+  S_TMP1 = 5,
+  S_TMP2 = 6,
+  S_TMP3 = 7,
+  S_COUNT = 64
+};
+/* device int flag slots */
+enum Flag { F_PASS2 = 0, F_COUNT = 16 };
+/* cached workspace slots */
+enum Ws {
+  WS_BASIS = 0, /* Lanczos basis                              */
+  WS_CHEB,      /* three recurrence vectors                   */
+  WS_VEC,       /* misc vectors                               */
+  WS_KPM,       /* KPM blocks                                 */
+  WS_MOM,       /* KPM moments                                */
+  WS_PART,      /* CGS partial products                       */
+  WS_SMALL,     /* small coefficient arrays                   */
+  WS_RITZ,      /* Ritz vectors                               */
+  WS_RITZ2,     /* A * Ritz vectors                           */
+  WS_COUNT
+};
+
+struct Ctx {
+  bool ready = false;
+  int device = 0;
+  int sms = 148;
+  cudaStream_t stream = nullptr;
+  double *red = nullptr;       /* kMaxRedBlocks * 64 partial sums */
+  unsigned *cnt = nullptr;     /* last-block counters, kept at 0  */
+  double *dscal = nullptr;     /* S_COUNT device scalars          */
+  double *hscal = nullptr;     /* pinned mirror of dscal          */
+  int *dflag = nullptr;        /* F_COUNT device flags            */
+  void *ws[WS_COUNT] = {};
+  size_t wsz[WS_COUNT] = {};
+  uint64_t launches = 0;
+  int sticky_error = 0;
+};
+
+Ctx &ctx();
+int ensure();                 /* initialise the context; 0 or PEVSL_ERR_CUDA */
+int fail(cudaError_t e, const char *what);
+int launched(const char *what); /* count a launch and check for errors */
+int sync();
+void *ws(int slot, size_t bytes);
+int memcpy_async(void *dst, const void *src, size_t bytes);
+/* scalar slots: copy device slots [first, first+count) to the pinned mirror
+ * and wait; returns pointer into the mirror or NULL */
+const double *fetch_scalars(int first, int count);
+
+inline unsigned grid_for(long n, int per_thread = 1) {
+  long b = (n + (long)kThreads * per_thread - 1) / ((long)kThreads * per_thread);
+  if (b < 1) b = 1;
+  if (b > kMaxRedBlocks) b = kMaxRedBlocks;
+  return (unsigned)b;
+}
+
+/* ---------------------------------------------------------------- BLAS1 */
+int vfill(double *x, long n, double v);
+int vcopy(const double *x, double *y, long n);
+int vscal(double *x, long n, double a);
+int vaxpy(long n, double a, const double *x, double *y);
+/* y += sign * (*coef) * x, coef in device memory */
+int vaxpy_dev(long n, const double *coef, double sign, const double *x, double *y);
+/* x *= 1 / (*s), s in device memory */
+int vscal_inv_dev(long n, const double *s, double *x);
+/* *out = <x, y> (deterministic); out in device memory */
+int vdot(long n, const double *x, const double *y, double *out);
+/* *out = ||x|| */
+int vnrm2(long n, const double *x, double *out);
+/* *out = sum x */
+int vsum(long n, const double *x, double *out);
+/* y -= (*coef) x  then  *nrm = ||y||  (one pass) */
+int vaxpy_dev_nrm2(long n, const double *coef, const double *x, double *y, double *nrm);
+/* out[c] = <X[:,c], Y[:,c]> for c < m, column-major with leading dims */
+int vdot_cols(long n, int m, const double *X, long ldx, const double *Y, long ldy, double *out);
+/* X[:,c] *= s[c] for c < m (s device) */
+int vscal_cols(long n, int m, double *X, long ldx, const double *s);
+/* Y[:,c] -= lam[c] X[:,c] (lam device) */
+int vaxpy_cols(long n, int m, const double *lam, const double *X, long ldx, double *Y, long ldy);
+
+/* ---------------------------------------------------------------- random */
+/* Philox Gaussian draws m0 .. m0+nv-1 into columns of X: X[i*rs + c*cs]. */
+int rand_gauss(double *X, long n, int nv, long rs, long cs, uint64_t seed, uint64_t m0);
+
+/* ---------------------------------------------------------------- sparse */
+int spmv(const pevsl_devcsr *A, const double *x, double *y);
+/* One degree of the Chebyshev filter recurrence (fused SpMV):
+ *   w = ((A vk - cc vk) * t) - vkm1   (vkm1 may be NULL)
+ *   vkp1 = w;  y = first ? mu0 * vk + muk * w : y + muk * w            */
+int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1,
+              double *y, double cc, double t, double mu0, double muk, int first);
+/* Same recurrence when A x is computed by a user callback: ax = A vk. */
+int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1, double *vkp1,
+                 double *y, double cc, double t, double mu0, double muk, int first);
+/* One KPM degree for s interleaved vectors (row-major n x ld blocks):
+ *   Xkp1 = (A Xk - ctr Xk) sc - Xkm1;   mom[c] = <Xkp1[:,c], V0[:,c]>   */
+int kpm_step(const pevsl_devcsr *A, int s, int ld, const double *Xk, const double *Xkm1,
+             double *Xkp1, const double *V0, double ctr, double sc, double *mom);
+/* Column sums of squares of an interleaved block: out[c] = sum_i X[i*ld+c]^2 */
+int block_colnorm2(long n, int s, int ld, const double *X, double *out);
+/* X[i*ld+c] *= 1/sqrt(nrm2[c]) */
+int block_normalize(long n, int s, int ld, double *X, const double *nrm2);
+
+/* ---------------------------------------------------------------- dense */
+/* w[j] = sum_i V[i + j*ldv] v[i], j < k (two-stage, deterministic); kernels
+ * return early when skip != NULL and *skip == 0 */
+int gemvT(long n, int k, const double *V, long ldv, const double *v, double *w, const int *run);
+/* v -= V w; *nrm = ||v||; if flag: *flag = (*nrm <= eta * *nrm_old), then
+ * *nrm_old = *nrm.  Skipped when run != NULL and *run == 0. */
+int gemv_sub_nrm(long n, int k, const double *V, long ldv, const double *w, double *v,
+                 double *nrm, const int *run, int *flag_out, double *nrm_old, double eta);
+/* U = V(:, 0:k) Y  (n x m, V column-major ldv, Y k x m column-major ldy) */
+int gemm_nn(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy,
+            double *U, long ldu);
+
+}  // namespace pv
+
+#endif

@@ -1,0 +1,850 @@
+/*
+ * The solvers of the slicing path, driven from the host with every vector
+ * operation on the GPU:
+ *
+ *   filter application   pEVSL_ChebAv     SRC/chebpol.c:509-574
+ *   KPM DOS              pEVSL_Kpmdos     SRC/kpmdos.c:36-197
+ *   Lanczos DOS          pEVSL_LanDosG    SRC/landos.c:40-314
+ *   spectrum bounds      pEVSL_LanTrbounds SRC/lantrbnd.c:31-408
+ *   filtered Lanczos     pEVSL_ChebLanNr  SRC/cheblanNr.c:54-448
+ *
+ * The control flow (step counts, tests, breakdown restarts, acceptance) is
+ * the reference's.  The host reads two scalars per Lanczos step (alpha,
+ * beta); everything else stays on the device.  The DGKS second
+ * Gram-Schmidt pass is decided on the device.  When A is the built-in
+ * parcsr, the SpMV is fused into the recurrence kernels; a user matvec
+ * (pEVSL_SetAMatvec) is called with device pointers instead.
+ */
+#include <cuda_runtime.h>
+#include <float.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "gpu.cuh"
+
+using namespace pv;
+
+namespace {
+
+const double kEta = 0.70710678118654752440; /* 1/sqrt(2): DGKS threshold */
+
+/* ------------------------------------------------------------ event timer
+ * Sums the device time of repeated segments (filter applications,
+ * reorthogonalisation) with a small pool of event pairs that is drained
+ * whenever it fills; the pools live for the whole process. */
+struct SegTimer {
+  static constexpr int kPairs = 64;
+  cudaEvent_t ev[2 * kPairs];
+  int used = 0;
+  double acc_ms = 0.0;
+  bool ok = false;
+  void init() {
+    if (!ok) {
+      ok = true;
+      for (int i = 0; i < 2 * kPairs; i++)
+        if (cudaEventCreate(&ev[i]) != cudaSuccess) ok = false;
+    }
+    used = 0;
+    acc_ms = 0.0;
+  }
+  void begin() {
+    if (!ok) return;
+    if (used == kPairs) flush();
+    cudaEventRecord(ev[2 * used], ctx().stream);
+  }
+  void end() {
+    if (!ok) return;
+    cudaEventRecord(ev[2 * used + 1], ctx().stream);
+    used++;
+  }
+  void flush() {
+    if (!ok || used == 0) return;
+    cudaEventSynchronize(ev[2 * used - 1]);
+    for (int i = 0; i < used; i++) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) acc_ms += ms;
+    }
+    used = 0;
+  }
+};
+SegTimer g_t_pol, g_t_orth;
+
+/* matvec through the installed operator: fused kernels use the device CSR
+ * directly; this is for the plain y = A x steps. */
+int apply_A(pevsl_Data *pevsl, const double *x, double *y) {
+  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
+  pevsl->stats->n_mvA++;
+  if (A) return spmv(A, x, y);
+  if (!pevsl->Amv || !pevsl->Amv->func) return PEVSL_ERR_NOMATVEC;
+  if (sync()) return PEVSL_ERR_CUDA;
+  pevsl->Amv->func((double *)x, y, pevsl->Amv->data);
+  return fail(cudaDeviceSynchronize(), "user matvec");
+}
+
+/* y = p((A - cc)/dd) v with mu[0..deg]; w3 holds 3n doubles. */
+int cheb_apply(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, double *y,
+               double *w3, long n) {
+  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
+  const int m = pol->deg;
+  const double cc = pol->cc, dd = pol->dd, t1 = 1.0 / dd, t2 = 2.0 / dd;
+  const double *mu = pol->mu;
+  pevsl->stats->n_polAv++;
+  if (m <= 0) {
+    if (vcopy(v, y, n)) return PEVSL_ERR_CUDA;
+    return vscal(y, n, mu[0]);
+  }
+  if (!A && (!pevsl->Amv || !pevsl->Amv->func)) return PEVSL_ERR_NOMATVEC;
+  double *buf[3] = {w3, w3 + n, w3 + 2 * n};
+  double *ax = A ? nullptr : (double *)ws(WS_VEC, sizeof(double) * (size_t)n);
+  if (!A && !ax) return PEVSL_ERR_NOMEM;
+  const double *vk = v, *vkm1 = nullptr;
+  for (int k = 1; k <= m; k++) {
+    double *vkp1 = buf[(k - 1) % 3];
+    const double t = k == 1 ? t1 : t2;
+    int st;
+    if (A) {
+      st = cheb_step(A, vk, vkm1, vkp1, y, cc, t, mu[0], mu[k], k == 1);
+    } else {
+      st = apply_A(pevsl, vk, ax);
+      if (!st) st = cheb_combine(n, ax, vk, vkm1, vkp1, y, cc, t, mu[0], mu[k], k == 1);
+      pevsl->stats->n_mvA--; /* counted below */
+    }
+    if (st) return st;
+    vkm1 = vk;
+    vk = vkp1;
+  }
+  pevsl->stats->n_mvA += (size_t)m;
+  return 0;
+}
+
+/* One CGS_DGKS (SRC/miscla.c:211-240) of v against V(:, 0:k).  On entry the
+ * device slot S_NRM0 holds ||v||; on exit S_NRM holds the final norm.  The
+ * second pass runs only if the first kept at most 1/sqrt(2) of the norm,
+ * decided on the device. */
+int cgs_dgks(const double *V, long ldv, int k, double *v, long n) {
+  Ctx &c = ctx();
+  double *w = (double *)ws(WS_SMALL, sizeof(double) * (size_t)(k + 1));
+  if (!w) return PEVSL_ERR_NOMEM;
+  int *run2 = c.dflag + F_PASS2;
+  if (gemvT(n, k, V, ldv, v, w, nullptr)) return PEVSL_ERR_CUDA;
+  if (gemv_sub_nrm(n, k, V, ldv, w, v, c.dscal + S_NRM, nullptr, run2, c.dscal + S_NRM0, kEta))
+    return PEVSL_ERR_CUDA;
+  if (gemvT(n, k, V, ldv, v, w, run2)) return PEVSL_ERR_CUDA;
+  return gemv_sub_nrm(n, k, V, ldv, w, v, c.dscal + S_NRM, run2, nullptr, nullptr, kEta);
+}
+
+long round_ld(long n) { return (n + 31) / 32 * 32; }
+
+}  // namespace
+
+extern "C" {
+
+/* y = p(A) v (pEVSL_ChebAv, SRC/chebpol.c:509-574) on device or managed
+ * vectors of length pevsl->n.  Extension entry point: the reference keeps
+ * ChebAv internal. */
+int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y) {
+  if (ensure()) return PEVSL_ERR_CUDA;
+  const long n = pevsl->n;
+  double *w3 = (double *)ws(WS_CHEB, sizeof(double) * 3 * (size_t)n);
+  if (!w3) return PEVSL_ERR_NOMEM;
+  int st = cheb_apply(pevsl, pol, v, y, w3, n);
+  if (!st) st = sync();
+  return st;
+}
+
+/* ================================================================ KPM DOS */
+
+int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *intv, int ngroups,
+                 int groupid, MPI_Comm gl_comm, double *mu, double *ecnt) {
+  const double t0 = pevsl_now();
+  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  if (pevsl_check_intv(intv, stdout) < 0) return -1;
+  const long n = pevsl->n;
+  const double aa = PEVSL_MAX(intv[0], intv[2]), bb = PEVSL_MIN(intv[1], intv[3]);
+  if (intv[0] < intv[2] || intv[1] > intv[3]) {
+    fprintf(stdout, " warning: interval (%e, %e) is adjusted to (%e, %e)\n", intv[0], intv[1],
+            aa, bb);
+  }
+  const double ctr = (intv[3] + intv[2]) / 2.0, wid = (intv[3] - intv[2]) / 2.0;
+  const double beta1 = acos(PEVSL_MAX(-1.0 + DBL_EPSILON, (aa - ctr) / wid));
+  const double beta2 = acos(PEVSL_MIN(1.0 - DBL_EPSILON, (bb - ctr) / wid));
+  double *jac = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1));
+  if (!jac) return PEVSL_ERR_NOMEM;
+  pevsl_dampcf(Mdeg, damping, jac);
+  jac[0] = 1.0;
+  memset(mu, 0, sizeof(double) * (size_t)(Mdeg + 1));
+  double tcnt = 0.0;
+  int vec_start = 0, vec_end = nvec;
+  if (ngroups > 1) pEVSL_Part1d(nvec, ngroups, &groupid, &vec_start, &vec_end, 1);
+  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
+  int st = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0, ctx().stream);
+  if (A) {
+    /* blocks of up to 64 vectors, row-interleaved; one launch per degree */
+    const int smax = 64;
+    for (int m0 = vec_start; m0 < vec_end && !st; m0 += smax) {
+      const int s = vec_end - m0 < smax ? vec_end - m0 : smax;
+      const int ld = s;
+      const size_t blk = (size_t)n * (size_t)ld;
+      double *X = (double *)ws(WS_KPM, sizeof(double) * 4 * blk);
+      double *mom = (double *)ws(WS_MOM, sizeof(double) * (size_t)(Mdeg + 1) * (size_t)s);
+      double *nrm2 = (double *)ws(WS_SMALL, sizeof(double) * 64);
+      double *hmom = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1) * (size_t)s);
+      if (!X || !mom || !nrm2 || !hmom) {
+        free(hmom);
+        st = PEVSL_ERR_NOMEM;
+        break;
+      }
+      double *V0 = X, *B[3] = {X + blk, X + 2 * blk, X + 3 * blk};
+      st = pevsl_rand_block_dev(V0, (int)n, s, ld);
+      if (!st) st = block_colnorm2(n, s, ld, V0, nrm2);
+      if (!st) st = block_normalize(n, s, ld, V0, nrm2);
+      for (int k = 0; k < Mdeg && !st; k++) {
+        const double sc = (k == 0 ? 1.0 : 2.0) / wid;
+        const double *Xk = k == 0 ? V0 : B[(k - 1) % 3];
+        const double *Xkm1 = k == 0 ? nullptr : (k == 1 ? V0 : B[(k - 2) % 3]);
+        st = kpm_step(A, s, ld, Xk, Xkm1, B[k % 3], V0, ctr, sc, mom + (size_t)k * s);
+      }
+      if (!st) st = memcpy_async(hmom, mom, sizeof(double) * (size_t)Mdeg * (size_t)s);
+      if (!st) st = sync();
+      pevsl->stats->n_mvA += (size_t)Mdeg * (size_t)s;
+      /* accumulate exactly as the reference: vector by vector, degree by degree */
+      for (int c = 0; c < s && !st; c++) {
+        mu[0] += jac[0];
+        tcnt -= jac[0] * (beta2 - beta1);
+        for (int k = 0; k < Mdeg; k++) {
+          const int k1 = k + 1;
+          const double t = hmom[(size_t)k * s + c] * 2.0 * jac[k1];
+          mu[k1] += t;
+          tcnt -= t * (sin(k1 * beta2) - sin(k1 * beta1)) / k1;
+        }
+      }
+      free(hmom);
+    }
+  } else {
+    /* user matvec: one vector at a time, as the reference */
+    double *buf = (double *)ws(WS_KPM, sizeof(double) * 4 * (size_t)n);
+    double *hdot = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1));
+    double *ddot_ = (double *)ws(WS_MOM, sizeof(double) * (size_t)(Mdeg + 1));
+    if (!buf || !hdot || !ddot_) st = PEVSL_ERR_NOMEM;
+    for (int m = vec_start; m < vec_end && !st; m++) {
+      double *v = buf, *vkm1 = buf + n, *vk = buf + 2 * n, *vkp1 = buf + 3 * n, *tmp;
+      st = pevsl_rand_vector_dev(v, (int)n);
+      if (!st) st = vnrm2(n, v, ctx().dscal + S_TMP0);
+      const double *h = st ? nullptr : fetch_scalars(S_TMP0, 1);
+      if (!h) {
+        st = st ? st : PEVSL_ERR_CUDA;
+        break;
+      }
+      const double tn = h[0];
+      if (!st) st = vscal(v, n, 1.0 / tn);
+      if (!st) st = vcopy(v, vk, n);
+      if (!st) st = vfill(vkm1, n, 0.0);
+      for (int k = 0; k < Mdeg && !st; k++) {
+        const double sc = (k == 0 ? 1.0 : 2.0) / wid;
+        st = apply_A(pevsl, vk, vkp1);
+        if (!st) st = vaxpy(n, -ctr, vk, vkp1);
+        if (!st) st = vscal(vkp1, n, sc);
+        if (!st) st = vaxpy(n, -1.0, vkm1, vkp1);
+        tmp = vkm1;
+        vkm1 = vk;
+        vk = vkp1;
+        vkp1 = tmp;
+        if (!st) st = vdot(n, vk, v, ddot_ + k);
+      }
+      if (!st) st = memcpy_async(hdot, ddot_, sizeof(double) * (size_t)Mdeg);
+      if (!st) st = sync();
+      if (st) break;
+      mu[0] += jac[0];
+      tcnt -= jac[0] * (beta2 - beta1);
+      for (int k = 0; k < Mdeg; k++) {
+        const int k1 = k + 1;
+        const double t = hdot[k] * 2.0 * jac[k1];
+        mu[k1] += t;
+        tcnt -= t * (sin(k1 * beta2) - sin(k1 * beta1)) / k1;
+      }
+    }
+    free(hdot);
+  }
+  cudaEventRecord(e1, ctx().stream);
+  cudaEventSynchronize(e1);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  pevsl_inst_of(pevsl)->phase_ms[1] = ms;
+  free(jac);
+  if (st) return st;
+  if (ngroups > 1) {
+    double *mu_g = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1));
+    double tcnt_g = 0.0;
+    MPI_Allreduce(mu, mu_g, Mdeg + 1, MPI_DOUBLE, MPI_SUM, gl_comm);
+    MPI_Allreduce(&tcnt, &tcnt_g, 1, MPI_DOUBLE, MPI_SUM, gl_comm);
+    memcpy(mu, mu_g, sizeof(double) * (size_t)(Mdeg + 1));
+    tcnt = tcnt_g;
+    free(mu_g);
+  }
+  const double t = 1.0 / (((double)nvec) * M_PI);
+  for (int k = 0; k <= Mdeg; k++) mu[k] *= t;
+  tcnt *= t * ((double)pevsl->N);
+  *ecnt = tcnt;
+  pevsl->stats->t_dos = pevsl_now() - t0;
+  return 0;
+}
+
+/* ================================================================ Lanczos DOS */
+
+int pEVSL_LanDosG(pevsl_Data *pevsl, const int nvec, int msteps, int npts, double *xdos,
+                  double *ydos, double *neig, double *intv, int ngroups, int groupid,
+                  MPI_Comm gl_comm) {
+  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  const double t0 = pevsl_now();
+  const long n = pevsl->n, ld = round_ld(n);
+  const int maxit = msteps < pevsl->N ? msteps : pevsl->N;
+  double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
+  double *vinit = (double *)ws(WS_VEC, sizeof(double) * (size_t)n);
+  double *y = (double *)calloc((size_t)npts, sizeof(double));
+  int *ind = (int *)malloc(sizeof(int) * (size_t)npts);
+  double *dT = (double *)malloc(sizeof(double) * (size_t)maxit);
+  double *eT = (double *)malloc(sizeof(double) * (size_t)maxit);
+  double *EvalT = (double *)malloc(sizeof(double) * (size_t)maxit);
+  double *EvecT = (double *)malloc(sizeof(double) * (size_t)maxit * (size_t)maxit);
+  int st = (!V || !vinit || !y || !ind || !dT || !eT || !EvalT || !EvecT) ? PEVSL_ERR_NOMEM : 0;
+  const double lm = intv[2], lM = intv[3];
+  const double aa = PEVSL_MAX(intv[0], intv[2]), bb = PEVSL_MIN(intv[1], intv[3]);
+  const int M = PEVSL_MIN(msteps, 30);
+  const double H = (lM - lm) / (M - 1);
+  const double sigma = H / sqrt(8 * log(1.25)) * pevsl->sigma_mult;
+  const double sigma2 = 2 * sigma * sigma;
+  const double width = sigma * sqrt(-2.0 * log(1e-08));
+  if (!st) linspace(aa, bb, npts, xdos);
+  int vec_start = 0, vec_end = nvec;
+  if (ngroups > 1) pEVSL_Part1d(nvec, ngroups, &groupid, &vec_start, &vec_end, 1);
+  Ctx &c = ctx();
+  for (int m = vec_start; m < vec_end && !st; m++) {
+    st = pevsl_rand_vector_dev(vinit, (int)n);
+    if (!st) st = vnrm2(n, vinit, c.dscal + S_TMP0);
+    const double *h = st ? nullptr : fetch_scalars(S_TMP0, 1);
+    if (!h) {
+      st = st ? st : PEVSL_ERR_CUDA;
+      break;
+    }
+    const double tinv = 1.0 / h[0];
+    if (!st) st = vcopy(vinit, V, n);
+    if (!st) st = vscal(V, n, tinv);
+    double wn = 0.0, beta = 0.0;
+    int nwn = 0;
+    for (int k = 0; k < maxit && !st; k++) {
+      double *v = V + (size_t)k * ld, *vnew = V + (size_t)(k + 1) * ld;
+      st = apply_A(pevsl, v, vnew);
+      if (!st && k > 0) st = vaxpy(n, -beta, V + (size_t)(k - 1) * ld, vnew);
+      if (!st) st = vdot(n, v, vnew, c.dscal + S_ALPHA);
+      if (!st) st = vaxpy_dev_nrm2(n, c.dscal + S_ALPHA, v, vnew, c.dscal + S_NRM0);
+      if (!st) st = cgs_dgks(V, ld, k + 1, vnew, n);
+      if (!st) st = memcpy_async(c.hscal + S_ALPHA, c.dscal + S_ALPHA, sizeof(double) * 4);
+      if (!st) st = sync();
+      if (st) break;
+      const double alpha = c.hscal[S_ALPHA];
+      beta = c.hscal[S_NRM];
+      dT[k] = alpha;
+      wn += fabs(alpha) + 2.0 * beta;
+      nwn += 3;
+      if (beta * nwn < orthTol * wn) {
+        st = pevsl_rand_vector_dev(vnew, (int)n);
+        if (!st) st = vnrm2(n, vnew, c.dscal + S_NRM0);
+        if (!st) st = cgs_dgks(V, ld, k + 1, vnew, n);
+        const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
+        if (!hb) {
+          st = st ? st : PEVSL_ERR_CUDA;
+          break;
+        }
+        st = vscal(vnew, n, 1.0 / hb[0]);
+        beta = 0.0;
+      } else {
+        st = vscal(vnew, n, 1.0 / beta);
+      }
+      eT[k] = beta;
+    }
+    if (st) break;
+    if (pevsl_tridiag_eig(maxit, dT, eT, EvalT, EvecT)) {
+      st = PEVSL_ERR_EIG;
+      break;
+    }
+    for (int i = 0; i < maxit; i++) {
+      const double g2 = EvecT[(size_t)i * maxit] * EvecT[(size_t)i * maxit];
+      const double th = EvalT[i];
+      int np = 0;
+      for (int j = 0; j < npts; j++)
+        if (fabs(xdos[j] - th) < width) ind[np++] = j;
+      for (int j = 0; j < np; j++)
+        y[ind[j]] += g2 * exp(-((xdos[ind[j]] - th) * (xdos[ind[j]] - th)) / sigma2);
+    }
+  }
+  if (!st && ngroups > 1) {
+    double *yg = (double *)malloc(sizeof(double) * (size_t)npts);
+    MPI_Allreduce(y, yg, npts, MPI_DOUBLE, MPI_SUM, gl_comm);
+    memcpy(y, yg, sizeof(double) * (size_t)npts);
+    free(yg);
+  }
+  if (!st) {
+    const double scaling = 1.0 / (nvec * sqrt(sigma2 * M_PI));
+    for (int j = 0; j < npts; j++) y[j] *= scaling;
+    memcpy(ydos, y, sizeof(double) * (size_t)npts);
+    pevsl_simpson(xdos, y, npts);
+    *neig = y[npts - 1] * pevsl->N;
+  }
+  free(y);
+  free(ind);
+  free(dT);
+  free(eT);
+  free(EvalT);
+  free(EvecT);
+  pevsl->stats->t_dos = pevsl_now() - t0;
+  return st;
+}
+
+/* ================================================================ bounds */
+
+int pEVSL_LanTrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pevsl_Parvec *vinit,
+                      int bndtype, double *lammin, double *lammax, FILE *fstats) {
+  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  const double t0 = pevsl_now();
+  const int N = pevsl->N;
+  const long n = pevsl->n, ld = round_ld(n);
+  lanm = PEVSL_MIN(lanm, N);
+  const int lanm1 = lanm + 1;
+  if (lanm == N) maxit = PEVSL_MIN(maxit, N);
+  const size_t L = (size_t)lanm1;
+  double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * L);
+  double *R2 = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * 2);
+  double *dY = (double *)ws(WS_RITZ2, sizeof(double) * L * 2 + sizeof(double) * L);
+  double *T = (double *)calloc(L * L, sizeof(double));
+  double *EvecT = (double *)calloc(L * L, sizeof(double));
+  double *Rval = (double *)calloc(L, sizeof(double));
+  double *hY = (double *)malloc(sizeof(double) * L * 2);
+  if (!V || !R2 || !dY || !T || !EvecT || !Rval || !hY) {
+    free(T);
+    free(EvecT);
+    free(Rval);
+    free(hY);
+    return PEVSL_ERR_NOMEM;
+  }
+  double *dS = dY + 2 * L; /* coefficients s of the restart step */
+  Ctx &c = ctx();
+  int st = 0, it = 0, trlen = 0;
+  double lmin = 0.0, lmax = 0.0, s[3] = {0, 0, 0};
+  if (fstats) fprintf(fstats, " LanTR for bounds: dim %d, maxits %d\n", lanm, maxit);
+  st = vcopy(vinit->data, V, n);
+  if (!st) st = vnrm2(n, V, c.dscal + S_TMP0);
+  const double *h0 = st ? nullptr : fetch_scalars(S_TMP0, 1);
+  if (!h0) st = st ? st : PEVSL_ERR_CUDA;
+  if (!st) st = vscal(V, n, 1.0 / h0[0]);
+#define VC(j) (V + (size_t)(j) * ld)
+  while (it < maxit && !st) {
+    double wn = 0.0, beta = 0.0;
+    int nwn = 0;
+    int k = trlen > 0 ? trlen + 1 : 0;
+    if (k + 5 > lanm1) {
+      fprintf(stderr, "Krylov dim too small for this problem. Try a larger dim\n");
+      st = PEVSL_ERR_ARG;
+      break;
+    }
+    if (trlen > 0) {
+      /* thick-restart step: arrowhead column of T (SRC/lantrbnd.c:150-223) */
+      const int k1 = k - 1;
+      double *v = VC(k1), *vnew = VC(k1 + 1);
+      st = apply_A(pevsl, v, vnew);
+      for (int i = 0; i < trlen; i++) {
+        T[i * L + i] = Rval[i];
+        wn += fabs(Rval[i]);
+      }
+      if (!st) st = vdot(n, v, vnew, c.dscal + S_TMP0);
+      const double *hs = st ? nullptr : fetch_scalars(S_TMP0, 1);
+      if (!hs) {
+        st = st ? st : PEVSL_ERR_CUDA;
+        break;
+      }
+      s[k1] = hs[0];
+      if (!st) st = memcpy_async(dS, s, sizeof(double) * (size_t)k);
+      if (!st) st = gemv_sub_nrm(n, k, V, ld, dS, vnew, c.dscal + S_NRM, nullptr, nullptr, nullptr,
+                                 kEta);
+      for (int i = 0; i < k1; i++) {
+        T[trlen * L + i] = s[i];
+        T[i * L + trlen] = s[i];
+        wn += 2.0 * fabs(s[i]);
+      }
+      T[trlen * L + trlen] = s[k1];
+      wn += fabs(s[k1]);
+      const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
+      if (!hb) {
+        st = st ? st : PEVSL_ERR_CUDA;
+        break;
+      }
+      beta = hb[0];
+      wn += 2.0 * beta;
+      nwn += 3 * k;
+      if (beta * nwn < orthTol * wn) {
+        st = pevsl_rand_vector_dev(vnew, (int)n);
+        if (!st) st = vnrm2(n, vnew, c.dscal + S_NRM0);
+        if (!st) st = cgs_dgks(V, ld, k, vnew, n);
+        const double *hb2 = st ? nullptr : fetch_scalars(S_NRM, 1);
+        if (!hb2) {
+          st = st ? st : PEVSL_ERR_CUDA;
+          break;
+        }
+        st = vscal(vnew, n, 1.0 / hb2[0]);
+        beta = 0.0;
+      } else {
+        st = vscal(vnew, n, 1.0 / beta);
+      }
+      T[k1 * L + k] = beta;
+      T[k * L + k1] = beta;
+    }
+    const double *zold = k > 0 ? VC(k - 1) : nullptr;
+    while (k < lanm && it < maxit && !st) {
+      k++;
+      double *v = VC(k - 1), *vnew = VC(k);
+      st = apply_A(pevsl, v, vnew);
+      it++;
+      if (!st && zold) st = vaxpy(n, -beta, zold, vnew);
+      if (!st) st = vdot(n, v, vnew, c.dscal + S_ALPHA);
+      if (!st) st = vaxpy_dev_nrm2(n, c.dscal + S_ALPHA, v, vnew, c.dscal + S_NRM0);
+      if (!st) st = cgs_dgks(V, ld, k, vnew, n);
+      if (!st) st = memcpy_async(c.hscal + S_ALPHA, c.dscal + S_ALPHA, sizeof(double) * 4);
+      if (!st) st = sync();
+      if (st) break;
+      const double alpha = c.hscal[S_ALPHA];
+      beta = c.hscal[S_NRM];
+      T[(k - 1) * L + (k - 1)] = alpha;
+      wn += fabs(alpha) + 2.0 * beta;
+      nwn += 3;
+      zold = v;
+      if (beta * nwn < orthTol * wn) {
+        if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", it, beta);
+        st = pevsl_rand_vector_dev(vnew, (int)n);
+        if (!st) st = vnrm2(n, vnew, c.dscal + S_NRM0);
+        if (!st) st = cgs_dgks(V, ld, k, vnew, n);
+        const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
+        if (!hb) {
+          st = st ? st : PEVSL_ERR_CUDA;
+          break;
+        }
+        st = vscal(vnew, n, 1.0 / hb[0]);
+        beta = 0.0;
+      } else {
+        st = vscal(vnew, n, 1.0 / beta);
+      }
+      T[k * L + (k - 1)] = beta;
+      T[(k - 1) * L + k] = beta;
+    }
+    if (st) break;
+    if (pevsl_dense_symeig(k, T, lanm1, EvecT, lanm1, Rval)) {
+      st = PEVSL_ERR_EIG;
+      break;
+    }
+    s[0] = beta * EvecT[k - 1];
+    s[1] = beta * EvecT[(size_t)(k - 1) * L + (k - 1)];
+    double t1, t2;
+    if (bndtype <= 1) {
+      t1 = fabs(s[0]);
+      t2 = fabs(s[1]);
+    } else {
+      t1 = 2.0 * s[0] * s[0] / (Rval[1] - Rval[0]);
+      t2 = 2.0 * s[1] * s[1] / (Rval[k - 1] - Rval[k - 2]);
+    }
+    lmin = Rval[0] - t1;
+    lmax = Rval[k - 1] + t2;
+    /* the two extreme Ritz vectors become V(:,0:2) */
+    memcpy(hY, EvecT, sizeof(double) * (size_t)k);
+    memcpy(hY + k, EvecT + (size_t)(k - 1) * L, sizeof(double) * (size_t)k);
+    st = memcpy_async(dY, hY, sizeof(double) * 2 * (size_t)k);
+    if (!st) st = gemm_nn(n, k, 2, V, ld, dY, k, R2, ld);
+    if (!st) st = vcopy(R2, VC(0), n);
+    if (!st) st = vcopy(R2 + ld, VC(1), n);
+    trlen = 2;
+    Rval[1] = Rval[k - 1];
+    if (fstats)
+      fprintf(fstats, "it %4d, k %3d: ritz %.15e %.15e, t1,t2 %e %e, res %.15e %.15e\n", it, k,
+              Rval[0], Rval[1], t1, t2, fabs(s[0]), fabs(s[1]));
+    if (t1 + t2 < tol * (fabs(lmin) + fabs(lmax))) break;
+    memset(T, 0, sizeof(double) * L * L);
+    if (!st) st = vcopy(VC(k), VC(trlen), n);
+  }
+#undef VC
+  if (!st) st = sync();
+  *lammin = lmin;
+  *lammax = lmax;
+  free(T);
+  free(EvecT);
+  free(Rval);
+  free(hY);
+  pevsl->stats->t_eigbounds += pevsl_now() - t0;
+  pevsl_inst_of(pevsl)->phase_ms[0] = 1e3 * (pevsl_now() - t0);
+  return st;
+}
+
+/* ================================================================ filtered Lanczos */
+
+int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
+                    pevsl_Polparams *pol, int *nevOut, double **lamo, pevsl_Parvecs **Wo,
+                    double **reso, FILE *fstats) {
+  const double tall = pevsl_now();
+  pevsl_inst *inst = pevsl_inst_of(pevsl);
+  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  const int N = pevsl->N;
+  const long n = pevsl->n, ld = round_ld(n);
+  maxit = PEVSL_MIN(N, maxit);
+  const double bar = pol->bar, gamB = pol->gam;
+  if (pevsl_check_intv(intv, fstats) < 0) {
+    *nevOut = 0;
+    *lamo = nullptr;
+    *Wo = nullptr;
+    *reso = nullptr;
+    return 0;
+  }
+  const double aa = intv[0], bb = intv[1];
+  if (fstats) {
+    fprintf(fstats, " intv:[%e, %e, %e, %e]\n", intv[0], intv[1], intv[2], intv[3]);
+    fprintf(fstats, " ** Cheb Poly of deg = %d, gam = %.15e, bar: %.15e\n", pol->deg, gamB, bar);
+  }
+  if (gamB > 1.0 || gamB < -1.0) {
+    fprintf(stdout, "gamB error %.15e\n", gamB);
+    return -1;
+  }
+  if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
+  Ctx &c = ctx();
+  double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
+  double *w3 = (double *)ws(WS_CHEB, sizeof(double) * 3 * (size_t)n);
+  double *vrand = (double *)ws(WS_VEC, sizeof(double) * (size_t)n);
+  double *dT = (double *)malloc(sizeof(double) * (size_t)maxit);
+  double *eT = (double *)malloc(sizeof(double) * (size_t)maxit);
+  double *EvalT = (double *)malloc(sizeof(double) * (size_t)maxit);
+  if (!V || !w3 || !vrand || !dT || !eT || !EvalT) {
+    free(dT);
+    free(eT);
+    free(EvalT);
+    return PEVSL_ERR_NOMEM;
+  }
+  /* the user-matvec path of cheb_apply uses WS_VEC itself: keep vrand apart */
+  if (!pevsl_builtin_A(pevsl)) {
+    vrand = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)n);
+    if (!vrand) return PEVSL_ERR_NOMEM;
+  }
+  SegTimer &t_pol = g_t_pol, &t_orth = g_t_orth;
+  t_pol.init();
+  t_orth.init();
+  cudaEvent_t e_all0, e_all1, e_r0;
+  cudaEventCreate(&e_all0);
+  cudaEventCreate(&e_all1);
+  cudaEventCreate(&e_r0);
+  cudaEventRecord(e_all0, c.stream);
+#define VC(j) (V + (size_t)(j) * ld)
+  int st = 0, k, kdim = 0, count = 0, nconv = 0;
+  /* filter the start vector and normalise it (SRC/cheblanNr.c:164-194) */
+  t_pol.begin();
+  st = cheb_apply(pevsl, pol, vinit->data, VC(0), w3, n);
+  t_pol.end();
+  if (!st) st = vnrm2(n, VC(0), c.dscal + S_TMP0);
+  const double *h0 = st ? nullptr : fetch_scalars(S_TMP0, 1);
+  if (!h0) st = st ? st : PEVSL_ERR_CUDA;
+  if (!st) st = vscal(VC(0), n, 1.0 / h0[0]);
+  double wn = 0.0, tr0 = 0.0, tr1, alpha, beta = 0.0;
+  int nwn = 0;
+  for (k = 0; k < maxit && !st; k++) {
+    double *z = VC(k), *znew = VC(k + 1);
+    t_pol.begin();
+    st = cheb_apply(pevsl, pol, z, znew, w3, n);
+    t_pol.end();
+    if (!st && k > 0) st = vaxpy(n, -beta, VC(k - 1), znew);
+    if (!st) st = vdot(n, z, znew, c.dscal + S_ALPHA);
+    t_orth.begin();
+    if (!st) st = vaxpy_dev_nrm2(n, c.dscal + S_ALPHA, z, znew, c.dscal + S_NRM0);
+    if (!st) st = cgs_dgks(V, ld, k + 1, znew, n);
+    t_orth.end();
+    if (!st) st = memcpy_async(c.hscal + S_ALPHA, c.dscal + S_ALPHA, sizeof(double) * 4);
+    if (!st) st = sync();
+    if (st) break;
+    alpha = c.hscal[S_ALPHA];
+    beta = c.hscal[S_NRM];
+    if (!isfinite(alpha) || !isfinite(beta)) {
+      st = PEVSL_ERR_NONFINITE;
+      break;
+    }
+    dT[k] = alpha;
+    wn += fabs(alpha);
+    wn += 2.0 * beta;
+    nwn += 3;
+    if (beta * nwn < orthTol * wn) {
+      /* lucky breakdown: restart from a new filtered random vector
+       * (SRC/cheblanNr.c:248-281) */
+      if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
+      st = pevsl_rand_vector_dev(vrand, (int)n);
+      t_pol.begin();
+      if (!st) st = cheb_apply(pevsl, pol, vrand, znew, w3, n);
+      t_pol.end();
+      if (!st) st = vnrm2(n, znew, c.dscal + S_NRM0);
+      if (!st) st = cgs_dgks(V, ld, k + 1, znew, n);
+      const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
+      if (!hb) {
+        st = st ? st : PEVSL_ERR_CUDA;
+        break;
+      }
+      st = vscal(znew, n, 1.0 / hb[0]);
+      beta = 0.0;
+    } else {
+      st = vscal(znew, n, 1.0 / beta);
+    }
+    eT[k] = beta;
+    if ((k < 30 || (k - 30) % 20 != 0) && k != maxit - 1) continue;
+    /* restricted-trace convergence test (SRC/cheblanNr.c:293-332) */
+    kdim = k + 1;
+    const double te = pevsl_now();
+    if (pevsl_tridiag_eig(kdim, dT, eT, EvalT, nullptr)) {
+      st = PEVSL_ERR_EIG;
+      break;
+    }
+    pevsl->stats->t_eig += pevsl_now() - te;
+    count = kdim;
+    tr1 = 0;
+    nconv = 0;
+    for (int i = 0; i < count; i++) {
+      if (EvalT[i] + 5 * DBL_EPSILON >= bar) {
+        tr1 += EvalT[i];
+        nconv++;
+      }
+    }
+    if (fstats) fprintf(fstats, "  k %4d:   nconv %4d  tr1 %21.15e\n", k, nconv, tr1);
+    if (fabs(tr1 - tr0) < 2e-12 || fabs(tr1) + fabs(tr0) < 1e-10) break;
+    tr0 = tr1;
+  }
+  if (!st && k >= maxit && fstats)
+    fprintf(fstats, "The max number of iterations [%d] has been reached. The eigenvalues computed "
+                    "may not have converged\n", maxit);
+  inst->last_its = kdim;
+  inst->last_nconv = nconv;
+  /* ---------------- Ritz pairs for Ritz values of p(A) >= bar ---------- */
+  int nev = 0;
+  double *Lam = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
+  double *res = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
+  pevsl_Parvecs *Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
+  if (!Lam || !res || !Rvec) st = st ? st : PEVSL_ERR_NOMEM;
+  cudaEventRecord(e_r0, c.stream);
+  const double tr_start = pevsl_now();
+  if (!st) {
+    pEVSL_ParvecsDuplParvec(vinit, nconv, (int)n, Rvec);
+    if (nconv > 0 && !Rvec->data) st = PEVSL_ERR_NOMEM;
+  }
+  int nsel = 0;
+  int *sel = nullptr;
+  if (!st && kdim > 0) {
+    const double te = pevsl_now();
+    /* eigenvalues again (the last test may predate the last step) */
+    st = pevsl_tridiag_eig(kdim, dT, eT, EvalT, nullptr) ? PEVSL_ERR_EIG : 0;
+    sel = (int *)malloc(sizeof(int) * (size_t)kdim);
+    for (int i = 0; i < count && !st; i++)
+      if (EvalT[i] >= bar) sel[nsel++] = i;
+    double *Y = nullptr;
+    if (!st && nsel > 0) {
+      Y = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)nsel);
+      st = Y ? pevsl_tridiag_eig_sel(kdim, dT, eT, EvalT, nsel, sel, Y) : PEVSL_ERR_NOMEM;
+      if (st) st = PEVSL_ERR_EIG;
+    }
+    pevsl->stats->t_eig += pevsl_now() - te;
+    if (!st && nsel > 0) {
+      /* U = V(:,0:kdim) Y, normalise, W = A U, lambda = <W,U>, residuals */
+      double *U = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * (size_t)nsel);
+      double *W = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)ld * (size_t)nsel);
+      double *dY = (double *)ws(WS_PART, sizeof(double) * (size_t)kdim * (size_t)nsel);
+      double *dv = (double *)ws(WS_MOM, sizeof(double) * 3 * (size_t)nsel);
+      double *hv = (double *)malloc(sizeof(double) * 3 * (size_t)nsel);
+      if (!U || !W || !dY || !dv || !hv) st = PEVSL_ERR_NOMEM;
+      if (!st) st = memcpy_async(dY, Y, sizeof(double) * (size_t)kdim * (size_t)nsel);
+      if (!st) st = gemm_nn(n, kdim, nsel, V, ld, dY, kdim, U, ld);
+      if (!st) st = vdot_cols(n, nsel, U, ld, U, ld, dv);
+      if (!st) st = memcpy_async(hv, dv, sizeof(double) * (size_t)nsel);
+      if (!st) st = sync();
+      for (int j = 0; j < nsel && !st; j++) {
+        const double t = sqrt(hv[j]);
+        if (t == 0.0) {
+          st = 2; /* zero eigenvector (SRC/cheblanNr.c:377-379) */
+          break;
+        }
+        hv[nsel + j] = 1.0 / t;
+      }
+      if (!st) st = memcpy_async(dv + nsel, hv + nsel, sizeof(double) * (size_t)nsel);
+      if (!st) st = vscal_cols(n, nsel, U, ld, dv + nsel);
+      for (int j = 0; j < nsel && !st; j++) st = apply_A(pevsl, U + (size_t)j * ld, W + (size_t)j * ld);
+      if (!st) st = vdot_cols(n, nsel, W, ld, U, ld, dv);
+      if (!st) st = vaxpy_cols(n, nsel, dv, U, ld, W, ld);
+      if (!st) st = vdot_cols(n, nsel, W, ld, W, ld, dv + 2 * nsel);
+      if (!st) st = memcpy_async(hv, dv, sizeof(double) * 3 * (size_t)nsel);
+      if (!st) st = sync();
+      for (int j = 0; j < nsel && !st; j++) {
+        const double lam = hv[j];
+        if (lam < aa - DBL_EPSILON || lam > bb + DBL_EPSILON) continue;
+        const double r0 = sqrt(hv[2 * nsel + j]);
+        if (r0 < tol) {
+          Lam[nev] = lam;
+          res[nev] = r0;
+          st = vcopy(U + (size_t)j * ld, Rvec->data + (size_t)nev * Rvec->ld, n);
+          nev++;
+        }
+      }
+      free(hv);
+    }
+    free(Y);
+  }
+  free(sel);
+  if (!st) st = sync();
+#undef VC
+  cudaEventRecord(e_all1, c.stream);
+  cudaEventSynchronize(e_all1);
+  t_pol.flush();
+  t_orth.flush();
+  float ms_all = 0.f, ms_ritz = 0.f;
+  cudaEventElapsedTime(&ms_all, e_all0, e_all1);
+  cudaEventElapsedTime(&ms_ritz, e_r0, e_all1);
+  inst->phase_ms[2] = ms_all;
+  inst->phase_ms[3] = t_pol.acc_ms;
+  inst->phase_ms[4] = t_orth.acc_ms;
+  inst->phase_ms[5] = ms_ritz;
+  pevsl->stats->t_polAv += 1e-3 * t_pol.acc_ms;
+  pevsl->stats->t_reorth += 1e-3 * t_orth.acc_ms;
+  cudaEventDestroy(e_all0);
+  cudaEventDestroy(e_all1);
+  cudaEventDestroy(e_r0);
+  free(dT);
+  free(eT);
+  free(EvalT);
+  if (st) {
+    free(Lam);
+    free(res);
+    if (Rvec) {
+      pEVSL_ParvecsFree(Rvec);
+      free(Rvec);
+    }
+    *nevOut = 0;
+    *lamo = nullptr;
+    *Wo = nullptr;
+    *reso = nullptr;
+    return st;
+  }
+  *nevOut = nev;
+  *lamo = Lam;
+  *Wo = Rvec;
+  *reso = res;
+  pevsl->stats->t_ritz = pevsl_now() - tr_start;
+  pevsl->stats->t_iter = pevsl_now() - tall;
+  return 0;
+}
+
+}  // extern "C"

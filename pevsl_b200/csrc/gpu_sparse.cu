@@ -1,0 +1,505 @@
+/*
+ * Sparse matrix on the GPU: the parcsr API (SRC/parcsr.c, SRC/parcsrmv.c)
+ * collapsed onto one device CSR, the CSR SpMV, and the two fused hot kernels
+ * of the path:
+ *
+ *  - cheb_step: one degree of the Chebyshev filter recurrence of
+ *    pEVSL_ChebAv (SRC/chebpol.c:538-568) with the SpMV fused in, so that a
+ *    degree reads A, v_k, v_{k-1}, y and writes v_{k+1}, y once;
+ *  - kpm_step: one degree of the KPM recurrence of pEVSL_Kpmdos
+ *    (SRC/kpmdos.c:129-156) for a block of s random vectors at once, with the
+ *    moment dot products fused in, so that A is read once per degree for all
+ *    vectors.
+ *
+ * Layout: CSR with int32 row pointers / column indices and fp64 values; a
+ * row is handled by a group of L lanes (L = 1..32, a power of two picked from
+ * the mean row length) that read the row's entries contiguously and reduce
+ * with warp shuffles.  KPM blocks are row-interleaved (row i of all s vectors
+ * contiguous), so the gather of x[col] is one coalesced 8*s-byte segment.
+ */
+#include <ctype.h>
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "gpu.cuh"
+
+namespace pv {
+
+template <int L>
+__device__ __forceinline__ unsigned group_mask() {
+  if constexpr (L == 32) {
+    return 0xffffffffu;
+  } else {
+    const unsigned lane = threadIdx.x & 31u;
+    return ((1u << L) - 1u) << (lane & ~(unsigned)(L - 1));
+  }
+}
+
+template <int L>
+__device__ __forceinline__ double group_sum(double v, unsigned mask) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o);
+  return v;
+}
+
+/* r = sum_{j in row} a[j] x[ja[j]], spread over the L lanes of the group */
+template <int L>
+__device__ __forceinline__ double row_dot(int row, const int *__restrict__ ia,
+                                          const int *__restrict__ ja, const double *__restrict__ a,
+                                          const double *__restrict__ x, int lane) {
+  const int s = ia[row], e = ia[row + 1];
+  double r = 0.0;
+  for (int j = s + lane; j < e; j += L) r = fma(a[j], __ldg(x + ja[j]), r);
+  return r;
+}
+
+template <int L>
+__global__ void __launch_bounds__(kThreads) k_spmv(int n, const int *__restrict__ ia,
+                                                   const int *__restrict__ ja,
+                                                   const double *__restrict__ a,
+                                                   const double *__restrict__ x,
+                                                   double *__restrict__ y) {
+  const long gt = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int row = (int)(gt / L), lane = (int)(threadIdx.x & (L - 1));
+  if (row >= n) return; /* the whole group leaves together */
+  const unsigned mask = group_mask<L>();
+  const double r = group_sum<L>(row_dot<L>(row, ia, ja, a, x, lane), mask);
+  if (lane == 0) y[row] = r;
+}
+
+template <int L>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb_step(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                const double *__restrict__ a, const double *__restrict__ vk,
+                const double *__restrict__ vkm1, double *__restrict__ vkp1, double *__restrict__ y,
+                double cc, double t, double mu0, double muk, int first) {
+  const long gt = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  const int row = (int)(gt / L), lane = (int)(threadIdx.x & (L - 1));
+  if (row >= n) return;
+  const unsigned mask = group_mask<L>();
+  const double r = group_sum<L>(row_dot<L>(row, ia, ja, a, vk, lane), mask);
+  if (lane == 0) {
+    const double x = vk[row];
+    double w = (r - cc * x) * t;
+    if (vkm1) w -= vkm1[row];
+    vkp1[row] = w;
+    y[row] = first ? mu0 * x + muk * w : y[row] + muk * w;
+  }
+}
+
+__global__ void k_cheb_combine(long n, const double *__restrict__ ax, const double *__restrict__ vk,
+                               const double *__restrict__ vkm1, double *__restrict__ vkp1,
+                               double *__restrict__ y, double cc, double t, double mu0, double muk,
+                               int first) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double x = vk[i];
+    double w = (ax[i] - cc * x) * t;
+    if (vkm1) w -= vkm1[i];
+    vkp1[i] = w;
+    y[i] = first ? mu0 * x + muk * w : y[i] + muk * w;
+  }
+}
+
+/* KPM degree for s <= 32*CPL interleaved vectors; one warp per row (grid
+ * stride), lane c handles columns c, c+32, ...  Moments: per-block partial
+ * sums in partials[block*s + c], the last block adds them in block order. */
+template <int CPL>
+__global__ void __launch_bounds__(kThreads)
+    k_kpm_step(int n, int s, int ld, const int *__restrict__ ia, const int *__restrict__ ja,
+               const double *__restrict__ a, const double *__restrict__ Xk,
+               const double *__restrict__ Xkm1, double *__restrict__ Xkp1,
+               const double *__restrict__ V0, double ctr, double sc, double *partials,
+               unsigned *counter, double *mom) {
+  __shared__ double acc_sh[kThreads / 32][32 * CPL];
+  __shared__ bool am_last;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  double acc[CPL];
+#pragma unroll
+  for (int q = 0; q < CPL; q++) acc[q] = 0.0;
+  for (int row = blockIdx.x * wpb + wib; row < n; row += gridDim.x * wpb) {
+    double r[CPL];
+#pragma unroll
+    for (int q = 0; q < CPL; q++) r[q] = 0.0;
+    const int e = ia[row + 1];
+    for (int j = ia[row]; j < e; j++) {
+      const double aj = a[j];
+      const double *xr = Xk + (size_t)ja[j] * ld;
+#pragma unroll
+      for (int q = 0; q < CPL; q++) {
+        const int c = lane + 32 * q;
+        if (c < s) r[q] = fma(aj, xr[c], r[q]);
+      }
+    }
+    const size_t base = (size_t)row * ld;
+#pragma unroll
+    for (int q = 0; q < CPL; q++) {
+      const int c = lane + 32 * q;
+      if (c < s) {
+        double w = (r[q] - ctr * Xk[base + c]) * sc;
+        if (Xkm1) w -= Xkm1[base + c];
+        Xkp1[base + c] = w;
+        acc[q] = fma(w, V0[base + c], acc[q]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < CPL; q++) acc_sh[wib][lane + 32 * q] = acc[q];
+  __syncthreads();
+  for (int c = threadIdx.x; c < s; c += blockDim.x) {
+    double t = 0.0;
+    for (int w = 0; w < wpb; w++) t += acc_sh[w][c];
+    partials[(size_t)blockIdx.x * s + c] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  for (int c = threadIdx.x; c < s; c += blockDim.x) {
+    double t = 0.0;
+    for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(partials + (size_t)b * s + c);
+    mom[c] = t;
+  }
+  if (threadIdx.x == 0) *counter = 0;
+}
+
+/* out[c] = sum_i X[i*ld + c]^2: per-block partials, last block adds them */
+__global__ void k_block_colnorm2(long n, int s, int ld, const double *__restrict__ X,
+                                 double *partials, unsigned *counter, double *out) {
+  __shared__ double acc_sh[kThreads / 32][64];
+  __shared__ bool am_last;
+  const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
+  double acc[2] = {0.0, 0.0};
+  for (long row = blockIdx.x * wpb + wib; row < n; row += (long)gridDim.x * wpb) {
+    for (int q = 0; q < 2; q++) {
+      const int c = lane + 32 * q;
+      if (c < s) {
+        const double v = X[row * ld + c];
+        acc[q] = fma(v, v, acc[q]);
+      }
+    }
+  }
+  acc_sh[wib][lane] = acc[0];
+  acc_sh[wib][lane + 32] = acc[1];
+  __syncthreads();
+  for (int c = threadIdx.x; c < s; c += blockDim.x) {
+    double t = 0.0;
+    for (int w = 0; w < wpb; w++) t += acc_sh[w][c];
+    partials[(size_t)blockIdx.x * s + c] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  for (int c = threadIdx.x; c < s; c += blockDim.x) {
+    double t = 0.0;
+    for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(partials + (size_t)b * s + c);
+    out[c] = t;
+  }
+  if (threadIdx.x == 0) *counter = 0;
+}
+
+__global__ void k_block_normalize(long n, int s, int ld, double *X, const double *nrm2) {
+  const long tot = n * (long)ld;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot; i += (long)gridDim.x * blockDim.x) {
+    const int c = (int)(i % ld);
+    if (c < s) X[i] *= 1.0 / sqrt(nrm2[c]);
+  }
+}
+
+#define PV_LANE_SWITCH(KERNEL, LANES, N, ...)                                                     \
+  do {                                                                                           \
+    const long _rows_per_block = kThreads / (LANES);                                             \
+    const unsigned _g = (unsigned)(((N) + _rows_per_block - 1) / _rows_per_block);              \
+    switch (LANES) {                                                                             \
+      case 1: KERNEL<1><<<_g, kThreads, 0, ctx().stream>>>(__VA_ARGS__); break;                  \
+      case 2: KERNEL<2><<<_g, kThreads, 0, ctx().stream>>>(__VA_ARGS__); break;                  \
+      case 4: KERNEL<4><<<_g, kThreads, 0, ctx().stream>>>(__VA_ARGS__); break;                  \
+      case 8: KERNEL<8><<<_g, kThreads, 0, ctx().stream>>>(__VA_ARGS__); break;                  \
+      case 16: KERNEL<16><<<_g, kThreads, 0, ctx().stream>>>(__VA_ARGS__); break;                \
+      default: KERNEL<32><<<_g, kThreads, 0, ctx().stream>>>(__VA_ARGS__); break;                \
+    }                                                                                            \
+  } while (0)
+
+int spmv(const pevsl_devcsr *A, const double *x, double *y) {
+  if (A->nrows <= 0) return 0;
+  PV_LANE_SWITCH(k_spmv, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, x, y);
+  return launched("spmv");
+}
+
+int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1, double *y,
+              double cc, double t, double mu0, double muk, int first) {
+  if (A->nrows <= 0) return 0;
+  PV_LANE_SWITCH(k_cheb_step, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y,
+                 cc, t, mu0, muk, first);
+  return launched("cheb_step");
+}
+
+int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1, double *vkp1,
+                 double *y, double cc, double t, double mu0, double muk, int first) {
+  if (n <= 0) return 0;
+  k_cheb_combine<<<grid_for(n, 4), kThreads, 0, ctx().stream>>>(n, ax, vk, vkm1, vkp1, y, cc, t,
+                                                                 mu0, muk, first);
+  return launched("cheb_combine");
+}
+
+static unsigned warp_row_grid(long n) {
+  const long wpb = kThreads / 32;
+  long g = (n + wpb - 1) / wpb;
+  if (g > kMaxRedBlocks) g = kMaxRedBlocks;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+int kpm_step(const pevsl_devcsr *A, int s, int ld, const double *Xk, const double *Xkm1,
+             double *Xkp1, const double *V0, double ctr, double sc, double *mom) {
+  if (s < 1 || s > 64) return PEVSL_ERR_ARG;
+  const unsigned g = warp_row_grid(A->nrows);
+  if (s <= 32) {
+    k_kpm_step<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, s, ld, A->ia, A->ja, A->a, Xk, Xkm1,
+                                                    Xkp1, V0, ctr, sc, ctx().red, ctx().cnt, mom);
+  } else {
+    k_kpm_step<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, s, ld, A->ia, A->ja, A->a, Xk, Xkm1,
+                                                    Xkp1, V0, ctr, sc, ctx().red, ctx().cnt, mom);
+  }
+  return launched("kpm_step");
+}
+
+int block_colnorm2(long n, int s, int ld, const double *X, double *out) {
+  if (s < 1 || s > 64) return PEVSL_ERR_ARG;
+  k_block_colnorm2<<<warp_row_grid(n), kThreads, 0, ctx().stream>>>(n, s, ld, X, ctx().red,
+                                                                     ctx().cnt, out);
+  return launched("block_colnorm2");
+}
+
+int block_normalize(long n, int s, int ld, double *X, const double *nrm2) {
+  k_block_normalize<<<grid_for(n * ld, 4), kThreads, 0, ctx().stream>>>(n, s, ld, X, nrm2);
+  return launched("block_normalize");
+}
+
+}  // namespace pv
+
+/* ================================================================ parcsr API */
+using namespace pv;
+
+static int choose_lanes(double avg) {
+  int L = 1;
+  while (L < 32 && L < avg) L <<= 1;
+  return L;
+}
+
+static void *alloc_managed(size_t bytes) {
+  void *p = nullptr;
+  if (fail(cudaMallocManaged(&p, bytes ? bytes : 16, cudaMemAttachGlobal), "cudaMallocManaged"))
+    return nullptr;
+  return p;
+}
+
+extern "C" {
+
+pevsl_devcsr *pevsl_devcsr_of(const pevsl_Parcsr *A) {
+  if (!A || !A->comm_handle) return nullptr;
+  pevsl_devcsr *d = (pevsl_devcsr *)A->comm_handle;
+  return d->magic == PEVSL_DEVCSR_MAGIC ? d : nullptr;
+}
+
+pevsl_devcsr *pevsl_builtin_A(pevsl_Data *pevsl) {
+  if (!pevsl->Amv || pevsl->Amv->func != pEVSL_ParcsrMatvec0) return nullptr;
+  return pevsl_devcsr_of((const pevsl_Parcsr *)pevsl->Amv->data);
+}
+
+/* Sizes only; with one process the local block is the whole matrix unless
+ * explicit starts say otherwise (SRC/parcsr.c:24-63). */
+int pEVSL_ParcsrCreate(int nrow, int ncol, int *row_starts, int *col_starts, pevsl_Parcsr *A,
+                       MPI_Comm comm) {
+  memset(A, 0, sizeof(*A));
+  A->comm = comm;
+  A->nrow_global = nrow;
+  A->ncol_global = ncol;
+  A->nrow_local = row_starts ? row_starts[1] - row_starts[0] : nrow;
+  A->ncol_local = col_starts ? col_starts[1] - col_starts[0] : ncol;
+  A->first_row = row_starts ? row_starts[0] : 0;
+  A->first_col = col_starts ? col_starts[0] : 0;
+  if (row_starts) {
+    A->row_starts = (int *)malloc(2 * sizeof(int));
+    memcpy(A->row_starts, row_starts, 2 * sizeof(int));
+  }
+  if (col_starts) {
+    A->col_starts = (int *)malloc(2 * sizeof(int));
+    memcpy(A->col_starts, col_starts, 2 * sizeof(int));
+  }
+  return 0;
+}
+
+/* Upload the caller's host CSR (the local rows, global column indices) as
+ * one device CSR (SRC/parcsr.c:70-283 without the split and halo plan). */
+int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
+  if (ensure()) return PEVSL_ERR_CUDA;
+  const int nr = A->nrow_local;
+  if (!Ai || Ai->nrows != nr || nr < 0) return PEVSL_ERR_ARG;
+  const long long nnz = Ai->ia[nr];
+  pevsl_devcsr *d = (pevsl_devcsr *)calloc(1, sizeof(pevsl_devcsr));
+  if (!d) return PEVSL_ERR_NOMEM;
+  d->magic = PEVSL_DEVCSR_MAGIC;
+  d->nrows = nr;
+  d->ncols = A->ncol_global;
+  d->nnz = nnz;
+  int maxr = 0;
+  for (int i = 0; i < nr; i++) {
+    const int r = Ai->ia[i + 1] - Ai->ia[i];
+    if (r > maxr) maxr = r;
+  }
+  d->max_row_nnz = maxr;
+  d->avg_row_nnz = nr ? (double)nnz / nr : 0.0;
+  d->lanes = choose_lanes(d->avg_row_nnz);
+  const char *lenv = getenv("PEVSL_B200_LANES");
+  if (lenv) {
+    const int L = atoi(lenv);
+    if (L == 1 || L == 2 || L == 4 || L == 8 || L == 16 || L == 32) d->lanes = L;
+  }
+  d->ia = (int *)alloc_managed(sizeof(int) * (size_t)(nr + 1));
+  d->ja = (int *)alloc_managed(sizeof(int) * (size_t)nnz);
+  d->a = (double *)alloc_managed(sizeof(double) * (size_t)nnz);
+  if (!d->ia || !d->ja || !d->a) {
+    cudaFree(d->ia);
+    cudaFree(d->ja);
+    cudaFree(d->a);
+    free(d);
+    return PEVSL_ERR_NOMEM;
+  }
+  {
+    /* keep the matrix resident in HBM (advice is optional: errors ignored) */
+    const int dev = ctx().device;
+    cudaMemAdvise(d->ia, sizeof(int) * (size_t)(nr + 1), cudaMemAdviseSetPreferredLocation, dev);
+    cudaMemAdvise(d->ja, sizeof(int) * (size_t)nnz, cudaMemAdviseSetPreferredLocation, dev);
+    cudaMemAdvise(d->a, sizeof(double) * (size_t)nnz, cudaMemAdviseSetPreferredLocation, dev);
+    cudaGetLastError();
+  }
+  int st = memcpy_async(d->ia, Ai->ia, sizeof(int) * (size_t)(nr + 1));
+  if (!st) st = memcpy_async(d->ja, Ai->ja, sizeof(int) * (size_t)nnz);
+  if (!st) st = memcpy_async(d->a, Ai->a, sizeof(double) * (size_t)nnz);
+  if (!st) st = sync();
+  if (st) return st;
+  A->comm_handle = (commHandle *)d;
+  A->diag = (pevsl_Csr *)calloc(1, sizeof(pevsl_Csr));
+  A->offd = (pevsl_Csr *)calloc(1, sizeof(pevsl_Csr));
+  A->diag->nrows = nr;
+  A->diag->ncols = A->ncol_global;
+  A->diag->ia = d->ia;
+  A->diag->ja = d->ja;
+  A->diag->a = d->a;
+  /* an empty off-diagonal block: PEVSL_CSRNNZ(offd) reads ia[0] == 0 */
+  A->offd->ia = (int *)calloc(1, sizeof(int));
+  return 0;
+}
+
+void pEVSL_ParcsrFree(pevsl_Parcsr *A) {
+  pevsl_devcsr *d = pevsl_devcsr_of(A);
+  if (d) {
+    cudaStreamSynchronize(ctx().stream);
+    cudaFree(d->ia);
+    cudaFree(d->ja);
+    cudaFree(d->a);
+    if (d->a32) cudaFree(d->a32);
+    d->magic = 0;
+    free(d);
+  }
+  A->comm_handle = nullptr;
+  free(A->row_starts);
+  free(A->col_starts);
+  A->row_starts = A->col_starts = nullptr;
+  if (A->diag) free(A->diag);
+  if (A->offd) {
+    free(A->offd->ia);
+    free(A->offd);
+  }
+  A->diag = A->offd = nullptr;
+  free(A->col_map_offd);
+  A->col_map_offd = nullptr;
+}
+
+/* Local rows as host COO and/or CSR with global columns, optionally only
+ * the lower ('L') or upper ('U') triangle, 0- or 1-based
+ * (SRC/parcsr.c:319-401). */
+int pEVSL_ParcsrGetLocalMat(pevsl_Parcsr *A, int idx, pevsl_Coo *coo, pevsl_Csr *csr, char stype) {
+  pevsl_devcsr *d = pevsl_devcsr_of(A);
+  if (!d) return PEVSL_ERR_ARG;
+  stype = (char)toupper((unsigned char)stype);
+  if (stype != 'L' && stype != 'U') stype = 'A';
+  const int nr = d->nrows;
+  const long long nnz = d->nnz;
+  int *ia = (int *)malloc(sizeof(int) * (size_t)(nr + 1));
+  int *ja = (int *)malloc(sizeof(int) * (size_t)(nnz ? nnz : 1));
+  double *a = (double *)malloc(sizeof(double) * (size_t)(nnz ? nnz : 1));
+  if (!ia || !ja || !a) {
+    free(ia);
+    free(ja);
+    free(a);
+    return PEVSL_ERR_NOMEM;
+  }
+  int st = memcpy_async(ia, d->ia, sizeof(int) * (size_t)(nr + 1));
+  if (!st) st = memcpy_async(ja, d->ja, sizeof(int) * (size_t)nnz);
+  if (!st) st = memcpy_async(a, d->a, sizeof(double) * (size_t)nnz);
+  if (!st) st = sync();
+  if (st) {
+    free(ia);
+    free(ja);
+    free(a);
+    return st;
+  }
+  pevsl_Csr loc;
+  pEVSL_CsrResize(nr, A->ncol_global, (int)nnz, &loc);
+  int k = 0;
+  loc.ia[0] = 0;
+  for (int i = 0; i < nr; i++) {
+    const int grow = i + A->first_row;
+    for (int j = ia[i]; j < ia[i + 1]; j++) {
+      const int gcol = ja[j];
+      if (stype == 'A' || (stype == 'L' && grow >= gcol) || (stype == 'U' && grow <= gcol)) {
+        loc.ja[k] = gcol;
+        loc.a[k] = a[j];
+        k++;
+      }
+    }
+    loc.ia[i + 1] = k;
+  }
+  free(ia);
+  free(ja);
+  free(a);
+  pEVSL_SortRow(&loc);
+  if (coo) pEVSL_CsrToCoo(&loc, idx, coo);
+  if (csr) {
+    if (idx) {
+      for (int j = 0; j < loc.ia[nr]; j++) loc.ja[j]++;
+      for (int i = 0; i <= nr; i++) loc.ia[i]++;
+    }
+    *csr = loc;
+  } else {
+    pEVSL_FreeCsr(&loc);
+  }
+  return 0;
+}
+
+int pEVSL_ParcsrNnz(pevsl_Parcsr *A) {
+  pevsl_devcsr *d = pevsl_devcsr_of(A);
+  return d ? (int)d->nnz : 0;
+}
+
+int pEVSL_ParcsrLocalNnz(pevsl_Parcsr *A) { return pEVSL_ParcsrNnz(A); }
+
+void pEVSL_ParcsrMatvec0(double *x, double *y, void *data) {
+  pevsl_devcsr *d = pevsl_devcsr_of((const pevsl_Parcsr *)data);
+  if (!d || ensure()) return;
+  if (!spmv(d, x, y)) sync();
+}
+
+void pEVSL_ParcsrMatvec(pevsl_Parcsr *A, pevsl_Parvec *x, pevsl_Parvec *y) {
+  pEVSL_ParcsrMatvec0(x->data, y->data, (void *)A);
+}
+
+}  // extern "C"

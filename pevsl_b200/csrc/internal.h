@@ -1,0 +1,86 @@
+/*
+ * pevsl-b200 internal interfaces shared by the host C modules and the CUDA
+ * modules.  Not installed; callers use include/pevsl.h and pevsl_b200.h.
+ */
+#ifndef PEVSL_B200_INTERNAL_H
+#define PEVSL_B200_INTERNAL_H
+
+#include <stdint.h>
+
+#include "pevsl.h"
+#include "pevsl_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ instance
+ * pEVSL_Start allocates this block; the caller sees &inst->pub. */
+typedef struct pevsl_inst {
+  pevsl_Data pub; /* first member: pevsl_Data* <-> pevsl_inst* */
+  pevsl_Stat stat;
+  pevsl_Matvec amv, bmv;
+  pevsl_Bsol bsol;
+  pevsl_Ltsol ltsol;
+  int last_its, last_nconv;
+  double phase_ms[8];
+} pevsl_inst;
+
+static inline pevsl_inst *pevsl_inst_of(pevsl_Data *d) { return (pevsl_inst *)d; }
+
+/* ------------------------------------------------------------------ device CSR
+ * pevsl_Parcsr.comm_handle points at this block after pEVSL_ParcsrSetup; its
+ * first member is a zeroed commHandle so the pointer type stays valid. */
+#define PEVSL_DEVCSR_MAGIC 0x42323030u /* "B200" */
+typedef struct pevsl_devcsr {
+  commHandle zero_handle;
+  uint32_t magic;
+  int nrows, ncols;
+  long long nnz;
+  int *ia;    /* device, nrows+1 */
+  int *ja;    /* device, nnz     */
+  double *a;  /* device, nnz     */
+  float *a32; /* device fp32 copy, made on first use */
+  int max_row_nnz;
+  double avg_row_nnz;
+  int lanes; /* threads per row in the row-group SpMV kernels */
+} pevsl_devcsr;
+
+/* The device matrix behind a Parcsr, or NULL if it was never set up here. */
+pevsl_devcsr *pevsl_devcsr_of(const pevsl_Parcsr *A);
+
+/* The built-in matrix of an instance when Amv is the parcsr callback, else
+ * NULL (a user matvec is installed). */
+pevsl_devcsr *pevsl_builtin_A(pevsl_Data *pevsl);
+
+/* ------------------------------------------------------------------ host helpers
+ * (host C modules) */
+double pevsl_now(void);
+int pevsl_check_intv(const double *intv, FILE *fstats);
+void pevsl_dampcf(int m, int damping, double *jac);
+void pevsl_chebxPltd(int m, const double *mu, int npts, const double *xi, double *yi);
+/* eigen-decomposition of a symmetric tridiagonal matrix; Z may be NULL */
+int pevsl_tridiag_eig(int n, const double *d, const double *e, double *w, double *Z);
+/* eigenvalues (ascending) + eigenvectors of the eigenvalues with ascending
+ * indices sel[0..nsel) into Zsel (n x nsel, column major) */
+int pevsl_tridiag_eig_sel(int n, const double *d, const double *e, double *w, int nsel,
+                          const int *sel, double *Zsel);
+/* eigen-decomposition of a dense symmetric matrix (column major) */
+int pevsl_dense_symeig(int n, const double *A, int lda, double *Q, int ldq, double *lam);
+void pevsl_simpson(const double *xi, double *yi, int npts);
+
+/* RNG state (host side; rng.cu owns the device generator) */
+int pevsl_rng_mode(void);
+uint64_t pevsl_rng_seed(void);
+uint64_t pevsl_rng_take(uint64_t ndraws); /* returns first draw index */
+/* Fill n doubles at dev (device/managed) with the next random vector. */
+int pevsl_rand_vector_dev(double *dev, int n);
+/* Fill nv column-interleaved vectors X[i*ld + c], c < nv, with the next nv
+ * draws (draw order = column order), row-interleaved layout. */
+int pevsl_rand_block_dev(double *X, int n, int nv, int ld);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -137,6 +137,26 @@ def main():
         ref, (12, 12, 12), RunSpec(0.5, 2.5, 3, dos_type=1, nvec=10, rng_mode=1, seed=2))
     dump("pipelines.json", runs)
 
+    # 7. Lucky breakdown and restart (SRC/cheblanNr.c:248-281): a diagonal
+    #    matrix with 10 distinct eigenvalues of multiplicity 40; the Krylov
+    #    space exhausts after a few steps and every restart draws a new
+    #    random vector from the glibc stream.
+    n = 400
+    d = np.repeat(np.arange(1.0, 11.0), 40)
+    ia = np.arange(n + 1, dtype=np.int32)
+    ja = np.arange(n, dtype=np.int32)
+    from checkers import Csr
+    D = Csr(n, ia, ja, d.copy())
+    intv = [3.5, 5.5, 0.5, 10.5]
+    _, pol = ref.findpol(intv)
+    ref.set_rng(0, 9)
+    v0 = np.cos(np.arange(n, dtype=np.float64) * 0.37)
+    out = ref.cheblannr(D, intv, 300, 1e-8, v0, pol)
+    dump("breakdown_case.json", dict(n=n, diag="repeat(1..10, 40)", intv=intv, maxit=300,
+                                     tol=1e-8, v0="cos(0.37 i)", seed=9, deg=pol["deg"],
+                                     status=out["status"], nev=out["nev"], its=out["its"],
+                                     lam=fl(out["lam"]), res=fl(out["res"])))
+
 
 if __name__ == "__main__":
     main()

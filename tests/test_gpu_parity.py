@@ -1,0 +1,348 @@
+"""Parity of the CUDA path with the oracle and the reference's golden outputs.
+
+Every test calls the product through its C-ABI (libpevsl_b200.so via
+pevsl_b200) and checks it against the plain-C oracle on the same inputs
+and/or the fixtures generated from the reference.  Tolerances (FP64 path):
+
+  SpMV                     1e-14 relative (summation order only)
+  random vectors           glibc stream exact; Philox Gaussian 1e-14 relative
+                           (device log/sincos vs host libm)
+  KPM moments / ecount     1e-12 relative;  npts identical
+  slice endpoints          1e-12 relative;  filter degree/type identical
+  filter application       1e-11 relative
+  bounds (LanTrbounds)     1e-10 relative
+  eigenvalues              1e-10 relative;  per-slice counts identical
+  residuals                ||Ax - lam x|| < tol = 1e-8 and ||Ax - lam x||/|lam| <= 1e-8
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import pevsl_b200 as pv
+from checkers import Csr, RunSpec, exact_eig_lap, laplacian
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def dev_matrix(A: Csr) -> pv.Matrix:
+    return pv.Matrix.from_csr(A.n, A.ia, A.ja, A.a)
+
+
+def random_csr(n, per_row, seed, sym=False):
+    rng = np.random.default_rng(seed)
+    rows = []
+    for i in range(n):
+        k = int(per_row[i]) if hasattr(per_row, "__len__") else per_row
+        cols = np.sort(rng.choice(n, size=min(k, n), replace=False))
+        rows.append(cols)
+    ia = np.zeros(n + 1, np.int32)
+    ia[1:] = np.cumsum([len(r) for r in rows])
+    ja = np.concatenate(rows).astype(np.int32)
+    a = rng.standard_normal(len(ja))
+    return Csr(n, ia, ja, a)
+
+
+# ---------------------------------------------------------------- SpMV
+def test_matvec_golden(gpu):
+    for key, case in golden("matvec_sin.json").items():
+        A = laplacian(*case["grid"])
+        M = dev_matrix(A)
+        y = M.matvec(np.sin(np.arange(A.n, dtype=np.float64)))
+        assert rel(y, case["y"]) <= 1e-14, key
+
+
+@pytest.mark.parametrize("per_row", [1, 3, 7, 13, 29, 70, "ragged"])
+def test_spmv_lane_widths(gpu, oracle, per_row):
+    """Rows of 1..70 entries select every lane width (1..32 threads per row);
+    'ragged' mixes empty rows and long rows."""
+    n = 3001
+    if per_row == "ragged":
+        rng = np.random.default_rng(5)
+        pr = rng.integers(0, 120, size=n)
+        pr[::7] = 0
+        A = random_csr(n, pr, 1)
+    else:
+        A = random_csr(n, per_row, per_row)
+    x = np.random.default_rng(2).standard_normal(n)
+    y = dev_matrix(A).matvec(x)
+    ref = oracle.matvec(A, x)
+    assert np.max(np.abs(y - ref)) <= 1e-14 * max(1.0, np.max(np.abs(ref))) * 8
+
+
+def test_spmv_empty_and_tiny(gpu, oracle):
+    for n in (1, 2, 33):
+        A = laplacian(n, 1, 1) if n > 1 else Csr(1, np.array([0, 1], np.int32),
+                                                 np.array([0], np.int32), np.array([2.5]))
+        x = np.linspace(-1, 1, n)
+        assert rel(dev_matrix(A).matvec(x), oracle.matvec(A, x)) <= 1e-15
+
+
+# ---------------------------------------------------------------- vectors / RNG
+def test_parvec_blas(gpu):
+    lib = pv.load()
+    n = 100003
+    rng = np.random.default_rng(0)
+    xa, ya = rng.standard_normal(n), rng.standard_normal(n)
+    x, y = pv.Vector(n, xa), pv.Vector(n, ya)
+    t = C.c_double()
+    lib.pEVSL_ParvecDot(C.byref(x.pv), C.byref(y.pv), C.byref(t))
+    assert abs(t.value - xa @ ya) <= 1e-12 * np.sqrt(n)
+    lib.pEVSL_ParvecNrm2(C.byref(x.pv), C.byref(t))
+    assert abs(t.value - np.linalg.norm(xa)) <= 1e-13 * np.linalg.norm(xa)
+    lib.pEVSL_ParvecSum(C.byref(x.pv), C.byref(t))
+    assert abs(t.value - xa.sum()) <= 1e-11
+    lib.pEVSL_ParvecAxpy(0.5, C.byref(x.pv), C.byref(y.pv))
+    assert rel(y.get(), ya + 0.5 * xa) <= 1e-15
+    lib.pEVSL_ParvecScal(C.byref(y.pv), -2.0)
+    assert rel(y.get(), -2.0 * (ya + 0.5 * xa)) <= 1e-15
+    lib.pEVSL_ParvecCopy(C.byref(x.pv), C.byref(y.pv))
+    assert np.array_equal(y.get(), xa)
+    lib.pEVSL_ParvecSetScalar(C.byref(y.pv), 3.0)
+    assert np.all(y.get() == 3.0)
+    lib.pEVSL_ParvecSetZero(C.byref(y.pv))
+    assert np.all(y.get() == 0.0)
+    # managed memory: the host reads the data pointer directly, as
+    # TESTS0/Matvec/test1.c does
+    host = np.ctypeslib.as_array(C.cast(x.pv.data, C.POINTER(C.c_double)), shape=(n,))
+    assert np.array_equal(host, xa)
+    assert lib.pEVSL_B200_LastError() == 0
+
+
+def test_parvecs_gemv_gemtv(gpu):
+    lib = pv.load()
+    n, k = 5000, 37
+    rng = np.random.default_rng(1)
+    Vh = rng.standard_normal((k, n))
+    X = pv.Parvecs()
+    lib.pEVSL_ParvecsCreate(n, k, n, n, 0, 1, C.byref(X))
+    lib.pEVSL_B200_Memcpy(X.data, Vh.ctypes.data, Vh.nbytes)
+    v = pv.Vector(n, rng.standard_normal(n))
+    w = np.zeros(k)
+    lib.pEVSL_ParvecsGemtv(1.0, C.byref(X), k, C.byref(v.pv), 0.0,
+                           w.ctypes.data_as(C.POINTER(C.c_double)))
+    assert rel(w, Vh @ v.get()) <= 1e-13
+    coef = rng.standard_normal(k)
+    y0 = v.get()
+    lib.pEVSL_ParvecsGemv(-1.0, C.byref(X), k, coef.ctypes.data_as(C.POINTER(C.c_double)), 1.0,
+                          C.byref(v.pv))
+    assert rel(v.get(), y0 - Vh.T @ coef) <= 1e-13
+    lib.pEVSL_ParvecsFree(C.byref(X))
+
+
+def test_rng_glibc_stream_matches_reference_formula(gpu, oracle):
+    lib = pv.load()
+    n = 7777
+    pv.set_rng(pv.RNG_GLIBC, 5)
+    v = pv.Vector(n)
+    lib.pEVSL_ParvecRand(C.byref(v.pv))
+    got = v.get()
+    oracle.lib.orc_set_rng(0, C.c_uint64(5))
+    exp = np.zeros(n)
+    oracle.lib.orc_rand_vector(exp.ctypes.data_as(C.c_void_p), n)
+    assert np.array_equal(got, exp)
+    assert np.all(np.abs(got) <= 1.0)
+
+
+def test_rng_gauss_matches_oracle(gpu, oracle):
+    lib = pv.load()
+    n = 10001
+    pv.set_rng(pv.RNG_GAUSS, 1234)
+    oracle.lib.orc_set_rng(1, C.c_uint64(1234))
+    for draw in range(3):
+        v = pv.Vector(n)
+        lib.pEVSL_ParvecRand(C.byref(v.pv))
+        exp = np.zeros(n)
+        oracle.lib.orc_rand_vector(exp.ctypes.data_as(C.c_void_p), n)
+        assert np.max(np.abs(v.get() - exp)) <= 1e-14 * np.max(np.abs(exp)), draw
+    assert int(lib.pEVSL_B200_RngDraws()) == 3
+    assert abs(exp.mean()) < 0.05 and abs(exp.std() - 1.0) < 0.05
+
+
+# ---------------------------------------------------------------- KPM, filter
+@pytest.mark.parametrize("mode", ["glibc", "gauss"])
+def test_kpm_golden(gpu, mode):
+    g = golden("lap20_kpm.json")
+    case = g["cases"][mode]
+    A = dev_matrix(laplacian(*g["grid"]))
+    with pv.Instance(A) as ev:
+        pv.set_rng(0 if mode == "glibc" else 1, g["seed"])
+        r, mu, ec = ev.kpmdos(g["Mdeg"], g["damping"], g["nvec"], g["intv"])
+    assert r == 0
+    assert rel(mu, case["mu"]) <= 1e-12
+    assert abs(ec - case["ecount"]) <= 1e-10 * abs(case["ecount"])
+    assert int(10 * ec) == case["npts"]
+    r, sli = pv.spslicer_kpm(mu, g["Mdeg"], g["intv"], 5, int(10 * ec))
+    assert r == 0 and rel(sli, case["sli"]) <= 1e-12
+
+
+def test_kpm_more_than_one_block(gpu, oracle):
+    """nvec = 150 runs as blocks of 64 + 64 + 22 vectors."""
+    A = laplacian(9, 10, 11)
+    intv = [1.0, 3.0, 0.0, 12.0]
+    with pv.Instance(dev_matrix(A)) as ev:
+        pv.set_rng(pv.RNG_GAUSS, 77)
+        r, mu, ec = ev.kpmdos(60, 2, 150, intv)
+    oracle.set_rng(1, 77)
+    _, mu_o, ec_o = oracle.kpmdos(A, 60, 2, 150, intv)
+    assert r == 0 and rel(mu, mu_o) <= 1e-12 and abs(ec - ec_o) <= 1e-10 * abs(ec_o)
+
+
+def test_chebav_matches_oracle(gpu, oracle):
+    A = laplacian(20, 20, 20)
+    for intv in ([0.6, 0.7482233502538076, 0.0, 12.0], [0.0, 0.5, 0.0, 12.0], [11.0, 12.0, 0, 12]):
+        r, f = pv.findpol(intv)
+        v = np.cos(np.arange(A.n) * 0.1)
+        with pv.Instance(dev_matrix(A)) as ev:
+            y = ev.chebav(f, v)
+        yo = oracle.chebav(A, dict(deg=f.deg, cc=f.cc, dd=f.dd, mu=f.mu), v)
+        assert rel(y, yo) <= 1e-11, intv
+
+
+# ---------------------------------------------------------------- Lanczos pieces
+def test_lantrbounds_golden(gpu):
+    g = golden("lanczos_cases.json")
+    A = dev_matrix(laplacian(*g["grid"]))
+    b = g["lantrbounds"]
+    v0 = np.cos(np.arange(A.n, dtype=np.float64))
+    for bt, c in b["cases"].items():
+        with pv.Instance(A) as ev:
+            pv.set_rng(pv.RNG_GAUSS, 3)
+            r, lo, hi = ev.lantrbounds(b["lanm"], b["maxit"], b["tol"], v0, int(bt))
+        assert r == c["status"] == 0
+        assert abs(lo - c["lmin"]) <= 1e-10 * max(1, abs(c["lmin"]))
+        assert abs(hi - c["lmax"]) <= 1e-10 * abs(c["lmax"])
+
+
+def test_landos_golden(gpu):
+    g = golden("lanczos_cases.json")
+    d = g["landos"]
+    A = dev_matrix(laplacian(*g["grid"]))
+    with pv.Instance(A) as ev:
+        pv.set_rng(pv.RNG_GAUSS, d["seed"])
+        r, xd, yd, ne = ev.landos(d["nvec"], d["msteps"], d["npts"], d["intv"])
+    assert r == 0
+    assert rel(xd, d["xdos"]) <= 1e-15
+    assert rel(yd, d["ydos"]) <= 1e-10
+    assert abs(ne - d["neig"]) <= 1e-10 * abs(d["neig"])
+    assert rel(pv.spslicer_lan(xd, yd, 4), d["sli4"]) <= 1e-12
+
+
+def test_cheblannr_slice_matches_oracle(gpu, oracle):
+    A = laplacian(20, 20, 20)
+    intv = [0.6, 0.7482233502538076, 0.0, 12.0]
+    r, f = pv.findpol(intv)
+    v0 = np.sin(np.arange(A.n) * 0.7)
+    with pv.Instance(dev_matrix(A)) as ev:
+        out = ev.cheblannr(intv, 300, 1e-8, v0, f, want_vectors=True)
+    ref = oracle.cheblannr(A, intv, 300, 1e-8, v0, dict(deg=f.deg, type=f.type, gam=f.gam,
+                                                         bar=f.bar, cc=f.cc, dd=f.dd, mu=f.mu))
+    assert out["status"] == 0
+    assert out["nev"] == ref["nev"] == 21 and out["its"] == ref["its"]
+    assert rel(out["lam"], ref["lam"]) <= 1e-10
+    assert np.all(out["res"] < 1e-8)
+    # eigenvectors: residuals recomputed on the host from the returned vectors
+    W = out["W"]
+    for lam, w in zip(out["lam"], W):
+        r = oracle.matvec(A, w) - lam * w
+        assert np.linalg.norm(r) / abs(lam) <= 1e-8 and abs(np.linalg.norm(w) - 1) < 1e-12
+
+
+def test_breakdown_restart_golden(gpu):
+    g = golden("breakdown_case.json")
+    n = g["n"]
+    D = Csr(n, np.arange(n + 1, dtype=np.int32), np.arange(n, dtype=np.int32),
+            np.repeat(np.arange(1.0, 11.0), 40))
+    r, f = pv.findpol(g["intv"])
+    assert f.deg == g["deg"]
+    with pv.Instance(dev_matrix(D)) as ev:
+        pv.set_rng(pv.RNG_GLIBC, g["seed"])
+        out = ev.cheblannr(g["intv"], g["maxit"], g["tol"], np.cos(np.arange(n) * 0.37), f)
+    assert (out["status"], out["nev"], out["its"]) == (g["status"], g["nev"], g["its"])
+    assert rel(out["lam"], g["lam"]) <= 1e-10
+
+
+# ---------------------------------------------------------------- whole runs
+def check_pipeline(r: pv.SliceResult, g, grid):
+    assert r.status == g["status"] == 0
+    assert abs(r.lmin - g["lmin"]) <= 1e-10 * max(1, abs(g["lmin"]))
+    assert abs(r.lmax - g["lmax"]) <= 1e-10 * abs(g["lmax"])
+    assert abs(r.ecount - g["ecount"]) <= 1e-10 * abs(g["ecount"])
+    assert r.npts == g["npts"]
+    assert rel(r.sli, g["sli"]) <= 1e-12
+    assert r.deg == g["deg"] and r.ptype == g["ptype"]
+    assert r.nev == g["nev"], (r.nev, g["nev"])
+    assert r.its == g["its"]
+    for sl in range(len(g["nev"])):
+        lam = r.lam[sl]
+        assert rel(lam, g["lam"][sl]) <= 1e-10
+        assert np.all(r.res[sl] < g["spec"]["tol"])
+        assert np.all(r.res[sl] / np.abs(lam) <= 1e-8)
+        ex = exact_eig_lap(*grid, g["sli"][sl], g["sli"][sl + 1])
+        assert len(ex) == len(lam) and np.max(np.abs(lam - ex)) <= 1e-12
+
+
+@pytest.mark.parametrize("name", ["lap10_kpm_gauss", "lap30x30_kpm_glibc", "lap12_landos_gauss",
+                                  "lap20_readme_glibc", "lap20_lantr_gauss"])
+def test_pipeline_golden(gpu, name):
+    g = golden("pipelines.json")[name]
+    A = dev_matrix(laplacian(*g["grid"]))
+    r = pv.solve_interval(A, pv.SliceRun(**g["spec"]))
+    check_pipeline(r, g, g["grid"])
+
+
+# ---------------------------------------------------------------- error paths
+def test_error_codes(gpu):
+    A = dev_matrix(laplacian(6, 6, 6))
+    with pv.Instance(A) as ev:
+        r, _, _ = ev.kpmdos(20, 1, 2, [1.0, 0.5, 0.0, 12.0])
+        assert r == -1
+        r, _, _ = ev.kpmdos(20, 1, 2, [13.0, 14.0, 0.0, 12.0])
+        assert r == -1
+        r, f = pv.findpol([1.0, 2.0, 0.0, 12.0])
+        out = ev.cheblannr([2.0, 1.0, 0.0, 12.0], 50, 1e-8, np.ones(A.n), f)
+        assert out["status"] == 0 and out["nev"] == 0
+        bad = pv.Filter(f.type, f.deg, 1.5, f.bar, f.cc, f.dd, f.mu)
+        out = ev.cheblannr([1.0, 2.0, 0.0, 12.0], 50, 1e-8, np.ones(A.n), bad)
+        assert out["status"] == -1
+        v = np.ones(A.n)
+        v[3] = np.nan
+        out = ev.cheblannr([1.0, 2.0, 0.0, 12.0], 50, 1e-8, v, f)
+        assert out["status"] == pv.ERR_NONFINITE
+    assert pv.findpol([1.0, 0.5, 0.0, 12.0])[0] == -1
+    assert pv.spslicer_kpm(np.ones(11), 10, [3.0, 1.0, 0, 12], 3, 40)[0] == -1
+
+
+def test_user_matvec_callback(gpu):
+    """pEVSL_SetAMatvec with a callback that receives device pointers; the
+    unfused path must give the fused path's results."""
+    lib = pv.load()
+    A = laplacian(12, 12, 12)
+    M = dev_matrix(A)
+    intv = [1.0, 1.6, 0.0, 12.0]
+    r, f = pv.findpol(intv)
+    v0 = np.cos(np.arange(A.n) * 0.3)
+
+    @pv.MVFUNC
+    def mv(x, y, data):
+        lib.pEVSL_ParcsrMatvec0(x, y, C.addressof(M.A))
+
+    with pv.Instance(M) as ev:
+        fused = ev.cheblannr(intv, 300, 1e-8, v0, f)
+        pv.set_rng(pv.RNG_GAUSS, 4)
+        _, mu_f, ec_f = ev.kpmdos(40, 1, 8, intv)
+    with pv.Instance(None) as ev:
+        lib.pEVSL_SetProbSizes(ev.p, A.n, A.n, 0)
+        lib.pEVSL_SetAMatvec(ev.p, mv, None)
+        cb = ev.cheblannr(intv, 300, 1e-8, v0, f)
+        pv.set_rng(pv.RNG_GAUSS, 4)
+        _, mu_c, ec_c = ev.kpmdos(40, 1, 8, intv)
+    assert cb["status"] == 0 and cb["nev"] == fused["nev"] and cb["its"] == fused["its"]
+    assert rel(cb["lam"], fused["lam"]) <= 1e-10
+    assert rel(mu_c, mu_f) <= 1e-12 and abs(ec_c - ec_f) <= 1e-10 * abs(ec_f)

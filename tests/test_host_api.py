@@ -1,0 +1,123 @@
+"""CPU tests of the product library's host code and C-ABI (no GPU needed).
+
+* every function declared in include/*.h is exported by libpevsl_b200.so;
+* the host-side parts of the path — filter design (pEVSL_FindPol), the KPM
+  and Lanczos slicers, partition/sort helpers — reproduce the reference's
+  golden outputs.  These run on the host in the product as in the
+  reference, so they are tested here without a GPU.  Tolerance: filter
+  degree/type and return codes exact, gam/bar/coefficients/endpoints 1e-12.
+"""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import pevsl_b200 as pv
+from conftest import ROOT, golden
+
+
+def rel(a, b):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def declared_functions():
+    names = set()
+    for h in ("pevsl.h", "pevsl_b200.h"):
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        kept, cont = [], False
+        for line in text.splitlines():
+            if cont or line.lstrip().startswith("#"):
+                cont = line.rstrip().endswith("\\")
+                continue
+            kept.append(line)
+        text = "\n".join(kept)
+        text = re.sub(r"typedef[^;]*;", "", text)
+        for m in re.finditer(r"\b([A-Za-z_][A-Za-z0-9_]*)\s*\([^;{}]*\)\s*;", text):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "return", "sizeof", "typedef"):
+                names.add(name)
+    # typedef'd callback types are not functions
+    return sorted(n for n in names if n not in ("SVFuncC", "SVFunc", "MVFunc"))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    out = os.popen("nm -D --defined-only " + pv.LIB_PATH).read()
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = [n for n in declared_functions() if n not in exported]
+    assert not missing, missing
+    assert len(declared_functions()) > 60
+
+
+def test_binding_signatures_resolve(lib):
+    for name, _, _ in pv.SIGNATURES:
+        assert hasattr(lib, name), name
+
+
+def test_findpol_matches_reference_golden(lib):
+    for c in golden("findpol_cases.json")["cases"]:
+        r, f = pv.findpol(c["intv"], **c["kw"])
+        assert r == c["status"], c
+        if r == 0:
+            assert (f.type, f.deg) == (c["type"], c["deg"]), c
+            assert abs(f.gam - c["gam"]) <= 1e-12 and abs(f.bar - c["bar"]) <= 1e-12, c
+            assert rel(f.mu, c["mu"]) <= 1e-12
+            assert f.cc == c["cc"] and f.dd == c["dd"]
+
+
+@pytest.mark.parametrize("mode", ["glibc", "gauss"])
+def test_slicer_and_filters_on_reference_moments(lib, mode):
+    g = golden("lap20_kpm.json")
+    case = g["cases"][mode]
+    r, sli = pv.spslicer_kpm(case["mu"], g["Mdeg"], g["intv"], 5, case["npts"])
+    assert r == case["slicer_status"]
+    assert rel(sli, case["sli"]) <= 1e-12
+    for p in case["pols"]:
+        r, f = pv.findpol(p["intv"])
+        assert r == 0 and f.deg == p["deg"] and f.type == p["type"]
+        assert abs(f.gam - p["gam"]) <= 1e-12 and abs(f.bar - p["bar"]) <= 1e-12
+        assert rel(f.mu, p["mu"]) <= 1e-12
+
+
+def test_slicer_edge_cases(lib):
+    g = golden("spslicer_cases.json")
+    for c in g["cases"]:
+        iv = c.get("intv", g["intv"])
+        r, sli = pv.spslicer_kpm(g["mu"], g["Mdeg"], iv, c["n_int"], c["npts"])
+        assert r == c["status"], c
+        if "sli" in c:
+            assert rel(sli, c["sli"]) <= 1e-12
+
+
+def test_lanczos_slicer_on_reference_dos(lib):
+    d = golden("lanczos_cases.json")["landos"]
+    sli = pv.spslicer_lan(d["xdos"], d["ydos"], 4)
+    assert rel(sli, d["sli4"]) <= 1e-12
+
+
+def test_part1d_and_sort(lib):
+    # SRC/utils.c:124-127: 9 -> [3,2,2,2], 10 -> [3,3,2,2], 11 -> [3,3,3,2]
+    for length, sizes in ((9, [3, 2, 2, 2]), (10, [3, 3, 2, 2]), (11, [3, 3, 3, 2])):
+        got = []
+        for p in range(4):
+            idx, j1, j2 = C.c_int(p), C.c_int(), C.c_int()
+            lib.pEVSL_Part1d(length, 4, C.byref(idx), C.byref(j1), C.byref(j2), 1)
+            got.append(j2.value - j1.value)
+        assert got == sizes
+        start = 0
+        for p, sz in enumerate(sizes):
+            for item in range(start, start + sz):
+                idx, j1, j2 = C.c_int(), C.c_int(item), C.c_int()
+                lib.pEVSL_Part1d(length, 4, C.byref(idx), C.byref(j1), C.byref(j2), 2)
+                assert idx.value == p and j2.value == sz
+            start += sz
+    v = np.array([3.0, -1.0, 2.0, 2.0, 0.5])
+    ind = np.zeros(5, np.int32)
+    lib.sort_double(5, v.ctypes.data_as(C.POINTER(C.c_double)), ind.ctypes.data_as(C.POINTER(C.c_int)))
+    assert list(v) == [-1.0, 0.5, 2.0, 2.0, 3.0] and ind[0] == 1 and ind[4] == 0
+    x = np.zeros(7)
+    lib.linspace(0.25, 1.75, 7, x.ctypes.data_as(C.POINTER(C.c_double)))
+    assert x[0] == 0.25 and x[-1] == 1.75 and abs(x[3] - 1.0) < 1e-16
