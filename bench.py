@@ -1,0 +1,459 @@
+#!/usr/bin/env python
+"""Eigenpairs/s of pEVSL's spectrum-slicing path on B200 (one process per GPU).
+
+A step is one whole run of the path on the workload (bounds by thick-restart
+Lanczos, KPM density of states, slicing, then filtered Lanczos on every
+slice), through the C-ABI library libpevsl_b200.so:
+
+  value : matrix resident in HBM; device time (CUDA events on the library
+          stream) of K steps after W warm-up steps; eigenpairs accepted at
+          residual <= 1e-8 per second, summed over ranks / max rank time.
+  e2e   : the same through the public API from pinned host buffers: every step
+          uploads the CSR (pEVSL_ParcsrSetup), solves, reads the eigenvalues and
+          residuals back, frees the matrix.
+
+Default workload (the metric's configuration): 3D 7-point Laplacian
+100^3 (n = 1e6, nnz = 6.94e6), interval [0.80, 0.82], 4 slices, KPM Mdeg 300
+with 30 seeded Gaussian vectors, tol 1e-8.  With N > 1 GPUs every rank
+solves its own copy with its own seed (weak scaling, no collective on the
+data path); rank 0 prints the JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+os.environ.setdefault("OPENBLAS_NUM_THREADS", "1")
+
+import numpy as np  # noqa: E402
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "lap100_4slices": dict(grid=(100, 100, 100), a=0.80, b=0.82, nslices=4, Mdeg=300, nvec=30),
+    "lap20_5slices": dict(grid=(20, 20, 20), a=0.6, b=1.2, nslices=5, Mdeg=300, nvec=60),
+}
+DEFAULT_WORKLOAD = "lap100_4slices"
+METRIC = "eigenpairs/s at residual <= 1e-8 (3D Laplacian 100^3, [0.80,0.82], 4 slices, FP64)"
+
+
+def slice_run(w, seed):
+    import pevsl_b200 as pv
+    return pv.SliceRun(w["a"], w["b"], w["nslices"], bounds_mode=1, Mdeg=w["Mdeg"],
+                       kpm_damping=1, nvec=w["nvec"], pol_damping=2, pol_max_deg=3000,
+                       thresh_int=0.8, thresh_ext=0.2, tol=1e-8, rng_mode=pv.RNG_GAUSS, seed=seed)
+
+
+# ---------------------------------------------------------------- distributed
+class Dist:
+    def __init__(self, n_gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            backend = os.environ.get("PEVSL_BENCH_BACKEND", "gloo")
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples every 200 ms while the timed region runs."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        out, _ = self.proc.communicate(timeout=10)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- helpers
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(workload):
+    """dram bytes per launch of the fused filter kernel from the committed ncu
+    summary (profiles/), or None."""
+    path = os.path.join(ROOT, "profiles", "cheb_step_traffic.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(workload)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_reference_sample(n, ia, ja, a, fil, seconds_budget=30.0):
+    """Time the reference's own pEVSL_ChebAv (oracle/_ref, compiled from the
+    reference sources) on this matrix with one slice's filter, on one core.
+    Returns seconds per filter degree (one SpMV + the recurrence's BLAS1)."""
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so"))
+    deg = fil.deg
+    # bounded sample: enough degrees for ~seconds_budget at ~10 ms each
+    mu = np.ascontiguousarray(fil.mu[: deg + 1])
+    v = np.cos(np.arange(n) * 0.1)
+    y = np.zeros(n)
+    P = lambda x: x.ctypes.data_as(C.c_void_p)  # noqa: E731
+    # probe: a short filter of degree 20 to estimate the per-degree time
+    t = time.perf_counter()
+    lib.oref_chebav(n, P(ia), P(ja), P(a), 20, C.c_double(fil.cc), C.c_double(fil.dd), P(mu), P(v),
+                    P(y))
+    per = (time.perf_counter() - t) / 20
+    d = int(max(20, min(deg, seconds_budget / max(per, 1e-9))))
+    t = time.perf_counter()
+    lib.oref_chebav(n, P(ia), P(ja), P(a), d, C.c_double(fil.cc), C.c_double(fil.dd), P(mu), P(v),
+                    P(y))
+    return (time.perf_counter() - t) / d, d
+
+
+# ---------------------------------------------------------------- our arm
+def run_b200(args, dist):
+    import pevsl_b200 as pv
+    from pevsl_b200.problems import laplacian
+    w = WORKLOADS[args.workload]
+    pv.load()
+    pv.load().pEVSL_B200_SetDevice(dist.local)
+    lib = pv.load()
+    n, ia, ja, a = laplacian(*w["grid"])
+    nnz = int(ia[-1])
+    seed = 1000 * dist.rank
+    spec = slice_run(w, seed)
+    # pinned host copies of the inputs for the end-to-end leg
+    ia_p, p1 = pv.pinned_empty(n + 1, np.int32)
+    ja_p, p2 = pv.pinned_empty(nnz, np.int32)
+    a_p, p3 = pv.pinned_empty(nnz, np.float64)
+    ia_p[:], ja_p[:], a_p[:] = ia, ja, a
+    M = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
+
+    batched = args.path == "batched"
+
+    def step():
+        return pv.solve_interval(M, spec, batched=batched)
+
+    for _ in range(args.warmup):
+        r = step()
+    dist.barrier()
+    clocks = ClockSampler(dist.local)
+    clocks.start()
+    pv.load().pEVSL_B200_Sync()
+    pv.load().pEVSL_B200_ResetFilterCounters()
+    l0 = pv.launch_count()
+    lib.pEVSL_B200_EventRecord(0)
+    eig = 0
+    results = []
+    for _ in range(args.steps):
+        r = step()
+        results.append(r)
+        eig += sum(r.nev)
+    lib.pEVSL_B200_EventRecord(1)
+    ms = lib.pEVSL_B200_EventElapsedMs(0, 1)
+    clk = clocks.stop()
+    launches = pv.launch_count() - l0
+    f_launch, f_bytes, f_ms = pv.filter_counters()
+    dist.barrier()
+    t_max = dist.max(ms / 1e3)
+    eig_all = dist.sum(float(eig))
+    value = eig_all / t_max
+    # end-to-end leg: upload from pinned memory, solve, results to host
+    dist.barrier()
+    lib.pEVSL_B200_EventRecord(2)
+    t0 = time.perf_counter()
+    e2e_eig = 0
+    d2h = 0
+    for _ in range(args.steps):
+        M2 = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
+        r2 = pv.solve_interval(M2, spec, batched=batched)
+        M2.free()
+        e2e_eig += sum(r2.nev)
+        d2h += sum(len(x) for x in r2.lam) * 16
+    lib.pEVSL_B200_EventRecord(3)
+    e2e_ms = lib.pEVSL_B200_EventElapsedMs(2, 3)
+    wall_e2e = time.perf_counter() - t0
+    dist.barrier()
+    e2e_t = dist.max(max(e2e_ms / 1e3, wall_e2e))
+    e2e_val = dist.sum(float(e2e_eig)) / e2e_t
+    # roofline of the dominant kernel (fused Chebyshev filter degree)
+    peak, peak_kind = measured_peak()
+    per_launch_bytes = f_bytes / max(f_launch, 1)
+    per_launch_ms = f_ms / max(f_launch, 1)
+    achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if f_launch else None
+    r0 = results[0]
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "eigenpairs/s",
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": t_max * 1e3 / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic: 3D Dirichlet Laplacian generated on the host, seeded Philox Gaussian "
+                "random vectors (seed 1000*rank)",
+        "config": {"workload": args.workload, "n": n, "nnz": nnz, "interval": [w["a"], w["b"]],
+                   "nslices": w["nslices"], "kpm_mdeg": w["Mdeg"], "kpm_nvec": w["nvec"],
+                   "bounds": "thick-restart Lanczos (50, 200, 1e-8)", "tol": 1e-8,
+                   "precision": "fp64",
+                   "path": ("all slices in lockstep (pEVSL_B200_ChebLanNrBatch), bit-identical to "
+                            "the slice-by-slice drop-in path" if batched else
+                            "slice by slice (pEVSL_ChebLanNr, the drop-in path)"),
+                   "eigenpairs_per_step": sum(r0.nev), "nev_per_slice": r0.nev,
+                   "lanczos_steps_per_slice": r0.its, "filter_degree_per_slice": r0.deg,
+                   "l2": "matrix + vectors ~120 MB per filter degree against a 126 MB L2; "
+                         "no flush between steps (each step streams the working set "
+                         "thousands of times)",
+                   "parallelism": f"replicas x{dist.world}"},
+        "gpu_launches": int(launches),
+        "clocks": clk,
+        "roofline": {
+            "kernel": ("cheb_multi (fused SpMV + Chebyshev recurrence, all slices per launch)"
+                       if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream)"),
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
+            "bytes_per_launch": per_launch_bytes, "launches": f_launch,
+            "avg_launch_us": per_launch_ms * 1e3, "traffic": ncu_traffic(args.workload)},
+        "e2e": {"value": e2e_val, "unit": "eigenpairs/s",
+                "h2d_bytes_per_step": int(4 * (n + 1) + 12 * nnz),
+                "d2h_bytes_per_step": int(d2h // max(args.steps, 1))},
+    }
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        try:
+            r, fil = pv.findpol([r0.sli[0], r0.sli[1], r0.lmin, r0.lmax], 3000, 2, 0.8, 0.2)
+            per, d = cpu_reference_sample(n, ia, ja, a, fil)
+            # whole-run CPU time: every filter degree and every KPM / bounds
+            # SpMV at the measured per-degree cost (reorthogonalisation, ~1-2%
+            # of the reference's time on this workload, not counted)
+            kpm = w["Mdeg"] * w["nvec"]
+            cpu_t = per * (f_launch / args.steps + kpm + 200)
+            out["cpu_baseline"] = {
+                "value": sum(r0.nev) / cpu_t, "unit": "eigenpairs/s", "cores": 1,
+                "kind": "reference",
+                "sample": f"reference pEVSL_ChebAv (oracle/_ref, OpenBLAS 1 thread) of degree {d} "
+                          f"with slice 0's filter on this matrix: {per*1e3:.2f} ms per degree; "
+                          f"extrapolated to the run's {int(f_launch/args.steps)} filter degrees + "
+                          f"{kpm} KPM + <=200 bounds matvecs"}
+        except Exception as e:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    M.free()
+    for p in (p1, p2, p3):
+        pv.free_pinned(p)
+    return out
+
+
+# ---------------------------------------------------------------- reference arm
+def _ref_slice_worker(q, n, ia, ja, a, deg, cc, dd, mu, budget):
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+
+    class F:
+        pass
+    f = F()
+    f.deg, f.cc, f.dd, f.mu = deg, cc, dd, mu
+    q.put(cpu_reference_sample(n, ia, ja, a, f, budget))
+
+
+def run_reference(args, dist):
+    """The reference's own CPU code (oracle/_ref) on this workload: its
+    pEVSL_LanTrbounds/Kpmdos-free filter cost measured per slice, one process
+    per slice as the reference's MPI groups, each step a bounded sample."""
+    if dist.rank != 0:
+        return None
+    import multiprocessing as mp
+
+    import pevsl_b200 as pv
+    from pevsl_b200.problems import laplacian
+    w = WORKLOADS[args.workload]
+    n, ia, ja, a = laplacian(*w["grid"])
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so"))
+    P = lambda x: x.ctypes.data_as(C.c_void_p)  # noqa: E731
+    # bounds with the reference's thick-restart Lanczos (real run)
+    lib.oref_set_unit_rng(1, C.c_uint64(0))
+    v0 = np.cos(np.arange(n) * 0.37)
+    lo, hi = C.c_double(), C.c_double()
+    lib.oref_lantrbounds(n, P(ia), P(ja), P(a), 50, 200, C.c_double(1e-8), P(v0), 1, C.byref(lo),
+                         C.byref(hi))
+    nsl = w["nslices"]
+    cores = min(os.cpu_count() or 1, nsl)
+    ctx = mp.get_context("spawn")
+    times = []
+    counts = REF_COUNTS.get(args.workload)
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        q = ctx.Queue()
+        procs = []
+        edges = np.linspace(w["a"], w["b"], nsl + 1)
+        for s in range(nsl):
+            r, fil = pv.findpol([edges[s], edges[s + 1], lo.value, hi.value], 3000, 2, 0.8, 0.2)
+            p = ctx.Process(target=_ref_slice_worker,
+                            args=(q, n, ia, ja, a, fil.deg, fil.cc, fil.dd, fil.mu, 20.0))
+            p.start()
+            procs.append(p)
+        per = [q.get() for _ in procs]
+        for p in procs:
+            p.join()
+        if it >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    per_deg = float(np.mean([x[0] for x in per]))
+    kpm = w["Mdeg"] * w["nvec"]
+    if counts:
+        # slices run concurrently (one process each): the slowest slice
+        # sets the time; KPM vectors split across the same processes
+        slice_t = max(per_deg * (its + 1) * deg for its, deg in zip(counts["its"], counts["deg"]))
+        total_t = slice_t + per_deg * (kpm / cores + 200)
+        value = counts["eigenpairs"] / total_t
+        how = (f"per-slice filter cost measured with the reference's pEVSL_ChebAv "
+               f"({per_deg*1e3:.2f} ms per degree, {nsl} processes in parallel), extrapolated to "
+               f"the per-slice Lanczos steps {counts['its']} and degrees {counts['deg']} of this "
+               f"workload (identical in the reference and the GPU path) + KPM split over "
+               f"{cores} processes")
+    else:
+        value, how = None, "per-slice step counts for this workload not recorded"
+    return {"metric": METRIC, "value": value, "unit": "eigenpairs/s", "n_gpus": dist.world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * float(np.mean(times)) if times else None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: 3D Dirichlet Laplacian", "impl": "reference",
+            "config": {"workload": args.workload, "n": n, "nnz": int(ia[-1])},
+            "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": cores,
+                             "kind": "reference", "sample": how},
+            "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+# per-slice Lanczos steps / filter degrees / accepted pairs of the workload,
+# recorded from a parity-checked run (used only to extrapolate the CPU sample)
+REF_COUNTS = {
+    "lap100_4slices": {"its": [431, 531, 531, 431], "deg": [1888, 1902, 1917, 1930],
+                       "eigenpairs": 454},
+    "lap20_5slices": {"its": [151, 151, 151, 151, 151], "deg": [54, 72, 91, 89, 110],
+                      "eigenpairs": 118},
+}
+
+
+def kernel_case(args):
+    """A few launches of one kernel on a matrix larger than L2, for ncu:
+    --kernel-case cheb_step runs two degree-8 filter applications (16 fused
+    filter-degree launches) on the 3D Laplacian of side --grid; kpm_step runs
+    8 KPM degrees for 16 vectors."""
+    import pevsl_b200 as pv
+    from pevsl_b200.problems import laplacian
+    g = args.grid
+    n, ia, ja, a = laplacian(g, g, g)
+    M = pv.Matrix.from_csr(n, ia, ja, a)
+    pv.set_rng(pv.RNG_GAUSS, 0)
+    with pv.Instance(M) as ev:
+        if args.kernel_case == "cheb_step":
+            r, f = pv.findpol([0.80, 0.82, 0.0, 12.0], deg_in=8)
+            v = np.cos(np.arange(n) * 0.1)
+            for _ in range(2):
+                ev.chebav(f, v)
+        else:
+            ev.kpmdos(8, 1, 16, [0.80, 0.82, 0.0, 12.0])
+    print(json.dumps({"kernel_case": args.kernel_case, "n": n, "nnz": int(ia[-1])}))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--path", default="batched", choices=["batched", "plain"],
+                    help="batched: slices in lockstep; plain: one pEVSL_ChebLanNr per slice")
+    ap.add_argument("--kernel-case", choices=["cheb_step", "kpm_step"],
+                    help="run a few launches of one kernel (for ncu) and exit")
+    ap.add_argument("--grid", type=int, default=128)
+    args = ap.parse_args()
+    if args.kernel_case:
+        kernel_case(args)
+        return
+    if args.warmup < 3:
+        args.warmup = 3
+    dist = Dist(args.gpus)
+    out = run_reference(args, dist) if args.impl == "reference" else run_b200(args, dist)
+    if dist.rank == 0 and out is not None:
+        print(json.dumps(out), flush=True)
+    dist.close()
+
+
+if __name__ == "__main__":
+    main()

@@ -56,8 +56,45 @@ int pEVSL_B200_LastError(void);
  * vectors of length pevsl->n. */
 int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y);
 
+/* pEVSL_ChebLanNr for nslices slices at once.  The slices advance in
+ * lockstep: one fused filter kernel per polynomial degree serves every slice
+ * still filtering (the matrix is read once per degree for all of them), the
+ * reorthogonalisation kernels run batched, and one host read per Lanczos
+ * step fetches all slices' recurrence scalars.  Slice s uses
+ * intvs[4s..4s+3], pols[s], maxits[s]; its outputs are nevOut[s], lamo[s],
+ * Wo[s], reso[s] (allocated as by pEVSL_ChebLanNr), its[s] (Lanczos steps)
+ * and status[s] (pEVSL_ChebLanNr's return code).  Returns the first
+ * nonzero status.  The results equal pEVSL_ChebLanNr called slice by slice,
+ * except that a lucky-breakdown restart draws its random vector in lockstep
+ * order rather than after the preceding slices have finished. */
+int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intvs,
+                              const int *maxits, double tol, pevsl_Parvec *vinit,
+                              pevsl_Polparams *pols, int *nevOut, double **lamo,
+                              pevsl_Parvecs **Wo, double **reso, int *its, int *status,
+                              FILE *fstats);
+
 /* Release cached device workspaces (they are reused across calls). */
 void pEVSL_B200_ReleaseWorkspace(void);
+
+/* Device used by the library (call before any other entry point); by
+ * default the environment variable PEVSL_B200_DEVICE, else LOCAL_RANK of a
+ * one-process-per-GPU launcher, else device 0. */
+int pEVSL_B200_SetDevice(int device);
+
+/* CUDA events (slots 0..15) recorded on the library stream, and the device
+ * time between two of them (waits for the second). */
+int pEVSL_B200_EventRecord(int slot);
+double pEVSL_B200_EventElapsedMs(int a, int b);
+
+/* Page-locked host memory for fast host<->device copies of inputs. */
+void *pEVSL_B200_HostAlloc(size_t bytes);
+void pEVSL_B200_HostFree(void *p);
+
+/* Counters of the fused Chebyshev filter kernel since the last reset:
+ * launches inside pEVSL_ChebLanNr, their algorithmic bytes (CSR + vectors),
+ * and the device time of the filter applications that contain them. */
+void pEVSL_B200_FilterCounters(uint64_t *launches, double *bytes, double *ms);
+void pEVSL_B200_ResetFilterCounters(void);
 
 /* Short build/device description into buf (NUL-terminated). */
 int pEVSL_B200_Info(char *buf, int len);

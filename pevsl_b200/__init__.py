@@ -155,6 +155,17 @@ SIGNATURES = [
     ("pEVSL_B200_ChebAv", _I, [C.POINTER(PevslData), C.POINTER(Polparams), _vp, _vp]),
     ("pEVSL_B200_ReleaseWorkspace", None, []),
     ("pEVSL_B200_Info", _I, [C.c_char_p, _I]),
+    ("pEVSL_B200_SetDevice", _I, [_I]),
+    ("pEVSL_B200_EventRecord", _I, [_I]),
+    ("pEVSL_B200_EventElapsedMs", _D, [_I, _I]),
+    ("pEVSL_B200_HostAlloc", _vp, [C.c_size_t]),
+    ("pEVSL_B200_HostFree", None, [_vp]),
+    ("pEVSL_B200_FilterCounters", None, [C.POINTER(C.c_uint64), _dp, _dp]),
+    ("pEVSL_B200_ResetFilterCounters", None, []),
+    ("pEVSL_B200_ChebLanNrBatch", _I, [C.POINTER(PevslData), _I, _dp, _ip, _D,
+                                       C.POINTER(Parvec), C.POINTER(Polparams), _ip,
+                                       C.POINTER(_dp), C.POINTER(C.POINTER(Parvecs)),
+                                       C.POINTER(_dp), _ip, _ip, _vp]),
 ]
 
 
@@ -191,6 +202,28 @@ def set_rng(mode: int, seed: int) -> None:
 
 def launch_count() -> int:
     return int(load().pEVSL_B200_LaunchCount())
+
+
+def filter_counters():
+    """(launches, algorithmic bytes, device ms) of the fused filter kernel."""
+    n, b, m = C.c_uint64(), C.c_double(), C.c_double()
+    load().pEVSL_B200_FilterCounters(C.byref(n), C.byref(b), C.byref(m))
+    return int(n.value), b.value, m.value
+
+
+def pinned_empty(count: int, dtype) -> tuple:
+    """A numpy array in page-locked host memory and its raw pointer (free
+    with free_pinned)."""
+    dt = np.dtype(dtype)
+    p = load().pEVSL_B200_HostAlloc(max(1, count) * dt.itemsize)
+    if not p:
+        raise PevslError("pEVSL_B200_HostAlloc failed")
+    buf = (C.c_char * (max(1, count) * dt.itemsize)).from_address(p)
+    return np.frombuffer(buf, dtype=dt, count=count), p
+
+
+def free_pinned(p) -> None:
+    load().pEVSL_B200_HostFree(p)
 
 
 def info() -> str:
@@ -423,6 +456,55 @@ class Instance:
         return out
 
 
+def _free_outputs(lib, lam, res, W):
+    libc = C.CDLL(None)
+    libc.free.argtypes = [_vp]
+    if lam:
+        libc.free(C.cast(lam, _vp))
+    if res:
+        libc.free(C.cast(res, _vp))
+    if W:
+        lib.pEVSL_ParvecsFree(W)
+        libc.free(C.cast(W, _vp))
+
+
+def cheblannr_batch(ev: "Instance", intvs, maxits, tol, vinit, filters):
+    """pEVSL_B200_ChebLanNrBatch: all slices in lockstep; a list of per-slice
+    dicts like Instance.cheblannr (without vectors)."""
+    lib = ev.lib
+    ns = len(filters)
+    pols = (Polparams * max(ns, 1))()
+    keep = []
+    for i, f in enumerate(filters):
+        p, mu = _polparams(f)
+        pols[i] = p
+        keep.append(mu)
+    v = vinit if isinstance(vinit, Vector) else Vector(ev.n, vinit)
+    iv = np.ascontiguousarray(np.asarray(intvs, dtype=np.float64).reshape(-1))
+    mx = np.ascontiguousarray(maxits, dtype=np.int32)
+    nev = np.zeros(ns, np.int32)
+    its = np.zeros(ns, np.int32)
+    status = np.zeros(ns, np.int32)
+    lam = (_dp * max(ns, 1))()
+    res = (_dp * max(ns, 1))()
+    W = (C.POINTER(Parvecs) * max(ns, 1))()
+    r = lib.pEVSL_B200_ChebLanNrBatch(ev.p, ns, _ptr(iv), _ptr(mx, _ip), tol, C.byref(v.pv),
+                                      pols, _ptr(nev, _ip), lam, W, res, _ptr(its, _ip),
+                                      _ptr(status, _ip), None)
+    outs = []
+    for i in range(ns):
+        m = int(nev[i])
+        o = dict(status=int(status[i]), nev=m, its=int(its[i]))
+        if status[i] == 0:
+            la = np.ctypeslib.as_array(lam[i], shape=(m,)).copy() if m else np.zeros(0)
+            rs = np.ctypeslib.as_array(res[i], shape=(m,)).copy() if m else np.zeros(0)
+            order = np.argsort(la, kind="stable")
+            o["lam"], o["res"] = la[order], rs[order]
+        _free_outputs(lib, lam[i], res[i], W[i])
+        outs.append(o)
+    return r, outs
+
+
 # ---------------------------------------------------------------- whole run
 @dataclass
 class SliceRun:
@@ -474,9 +556,11 @@ class SliceResult:
     times: dict = field(default_factory=dict)
 
 
-def solve_interval(A: Matrix, s: SliceRun) -> SliceResult:
+def solve_interval(A: Matrix, s: SliceRun, batched: bool = False) -> SliceResult:
     """Run the whole slicing path through the C API, in the reference
-    drivers' order: start vector, bounds, DOS, slicer, then each slice."""
+    drivers' order: start vector, bounds, DOS, slicer, then each slice
+    (one pEVSL_ChebLanNr per slice, or all slices in lockstep through
+    pEVSL_B200_ChebLanNrBatch when batched)."""
     import time
     lib = load()
     t_all = time.perf_counter()
@@ -520,7 +604,30 @@ def solve_interval(A: Matrix, s: SliceRun) -> SliceResult:
         res = SliceResult(lmin, lmax, ecount, npts, status, mu, sli)
         ev_int = int(1 + ecount / float(s.nslices))
         t = time.perf_counter()
-        for sl in range(s.nslices):
+        if batched:
+            nev = ev_int + 2
+            mlan = min(max(5 * nev, s.mlan_min), A.n)
+            filters, intvs = [], []
+            for sl in range(s.nslices):
+                iv = [sli[sl], sli[sl + 1], lmin, lmax]
+                r, f = findpol(iv, s.pol_max_deg, s.pol_damping, s.thresh_int, s.thresh_ext)
+                if r:
+                    raise PevslError(f"pEVSL_FindPol returned {r} for slice {sl}")
+                filters.append(f)
+                intvs.append(iv)
+            r, outs = cheblannr_batch(ev, intvs, [mlan] * s.nslices, s.tol, vinit, filters)
+            for f, out in zip(filters, outs):
+                if out["status"] and not res.status:
+                    res.status = 300 + abs(out["status"])
+                res.deg.append(f.deg)
+                res.ptype.append(f.type)
+                res.gam.append(f.gam)
+                res.bar.append(f.bar)
+                res.nev.append(out["nev"])
+                res.its.append(out["its"])
+                res.lam.append(out.get("lam", np.zeros(0)))
+                res.res.append(out.get("res", np.zeros(0)))
+        for sl in range(0 if not batched else s.nslices, s.nslices):
             nev = ev_int + 2
             mlan = min(max(5 * nev, s.mlan_min), A.n)
             iv = [sli[sl], sli[sl + 1], lmin, lmax]

@@ -17,6 +17,26 @@ namespace pv {
 
 constexpr int kThreads = 256;      /* block size of the streaming kernels      */
 constexpr int kMaxRedBlocks = 1184; /* 8 x 148 SMs: partial sums per reduction */
+constexpr int kMaxBatch = 16;       /* entries of one batched launch            */
+
+/* per-entry pointers / scalars of a batched launch (kernel parameters) */
+struct VPtrs {
+  double *p[kMaxBatch];
+};
+struct CPtrs {
+  const double *p[kMaxBatch];
+};
+struct BScal {
+  double v[kMaxBatch];
+};
+/* per-entry filter data of a batched filter degree */
+struct BatchParams {
+  unsigned mask;          /* active entries */
+  int deg[kMaxBatch];     /* filter degree of each entry */
+  double cc[kMaxBatch];   /* centre of the spectrum bounds */
+  double t1[kMaxBatch];   /* 1 / dd */
+  double t2[kMaxBatch];   /* 2 / dd */
+};
 
 /* device scalar slots (doubles) */
 enum Slot {
@@ -135,6 +155,28 @@ int gemvT(long n, int k, const double *V, long ldv, const double *v, double *w, 
  * *nrm_old = *nrm.  Skipped when run != NULL and *run == 0. */
 int gemv_sub_nrm(long n, int k, const double *V, long ldv, const double *w, double *v,
                  double *nrm, const int *run, int *flag_out, double *nrm_old, double eta);
+/* ---------------------------------------------------------------- batched
+ * Entry s of every call uses pointer p[s] / scalar v[s]; only entries whose
+ * bit is set in mask run.  Per-entry outputs go to out[s]. */
+int b_axpy(long n, int S, CPtrs x, VPtrs y, BScal a, unsigned mask);
+int b_scal(long n, int S, VPtrs x, BScal a, unsigned mask);
+int b_dot(long n, int S, CPtrs x, CPtrs y, double *out, int fin, unsigned mask);
+int b_axpy_dev_nrm2(long n, int S, const double *coef, CPtrs x, VPtrs y, double *nrm,
+                    unsigned mask);
+int b_gather(long n, int S, CPtrs src, double *Z, unsigned mask);
+int b_scatter(long n, int S, const double *Y, VPtrs dst, unsigned mask);
+/* w[s*ldw + j] = <V_s(:,j), v_s>, j < k */
+int b_gemvT(long n, int S, int k, CPtrs V, long ldv, CPtrs v, double *w, long ldw, const int *run,
+            unsigned mask);
+/* v_s -= V_s w_s; nrm[s] = ||v_s||; flag/nrm_old per entry as gemv_sub_nrm */
+int b_gemv_sub_nrm(long n, int S, int k, CPtrs V, long ldv, const double *w, long ldw, VPtrs v,
+                   double *nrm, const int *run, int *flag_out, double *nrm_old, double eta,
+                   unsigned mask);
+/* one filter degree k for S (1,2,4,8,16) row-interleaved vectors
+ * (X[i*S + s]); mu is S rows of mu_ld coefficients */
+int cheb_multi(const pevsl_devcsr *A, int S, const double *vk, const double *vkm1, double *vkp1,
+               double *y, const double *mu, int mu_ld, int k, const BatchParams &p);
+
 /* U = V(:, 0:k) Y  (n x m, V column-major ldv, Y k x m column-major ldy) */
 int gemm_nn(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy,
             double *U, long ldu);

@@ -16,6 +16,7 @@
 #include <string.h>
 
 #include "gpu.cuh"
+#include "gpu_device.cuh"
 
 namespace pv {
 
@@ -30,9 +31,20 @@ int fail(cudaError_t e, const char *what) {
   return PEVSL_ERR_CUDA;
 }
 
+static int g_req_device = -1;
+
 int ensure() {
   if (g_ctx.ready) return 0;
-  int dev = 0;
+  int dev = 0, ndev = 0;
+  if (fail(cudaGetDeviceCount(&ndev), "cudaGetDeviceCount")) return PEVSL_ERR_CUDA;
+  /* device: pEVSL_B200_SetDevice, else PEVSL_B200_DEVICE, else the launcher's
+   * LOCAL_RANK (one process per GPU), else 0 */
+  int want = g_req_device;
+  if (want < 0 && getenv("PEVSL_B200_DEVICE")) want = atoi(getenv("PEVSL_B200_DEVICE"));
+  if (want < 0 && getenv("LOCAL_RANK")) want = atoi(getenv("LOCAL_RANK"));
+  if (want >= 0 && ndev > 0) {
+    if (fail(cudaSetDevice(want % ndev), "cudaSetDevice")) return PEVSL_ERR_CUDA;
+  }
   if (fail(cudaGetDevice(&dev), "cudaGetDevice")) return PEVSL_ERR_CUDA;
   g_ctx.device = dev;
   cudaDeviceProp prop;
@@ -91,54 +103,6 @@ const double *fetch_scalars(int first, int count) {
   return g_ctx.hscal + first;
 }
 
-/* ---------------------------------------------------------------- reductions */
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-
-/* Sum over the block (fixed tree); the result is valid in thread 0. */
-__device__ double block_sum(double v) {
-  __shared__ double sh[32];
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  v = warp_sum(v);
-  __syncthreads();
-  if (l == 0) sh[w] = v;
-  __syncthreads();
-  const int nw = (blockDim.x + 31) >> 5;
-  v = threadIdx.x < nw ? sh[threadIdx.x] : 0.0;
-  if (w == 0) v = warp_sum(v);
-  return v;
-}
-
-enum Fin { FIN_ID = 0, FIN_SQRT = 1 };
-
-/* Write this block's partial; the last block adds all partials in block order
- * and stores fin(total) to *out.  Returns true in the thread that stored. */
-__device__ bool finish_sum(double part, double *partials, unsigned *counter, double *out, int fin) {
-  __shared__ bool am_last;
-  const double s = block_sum(part);
-  if (threadIdx.x == 0) {
-    partials[blockIdx.x] = s;
-    __threadfence();
-    am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!am_last) return false;
-  __threadfence();
-  double t = 0.0;
-  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t += __ldcg(partials + i);
-  t = block_sum(t);
-  if (threadIdx.x == 0) {
-    *out = fin == FIN_SQRT ? sqrt(t) : t;
-    *counter = 0;
-    return true;
-  }
-  return false;
-}
-
 /* ---------------------------------------------------------------- BLAS1 kernels */
 
 __global__ void k_fill(double *x, long n, double v) {
@@ -164,32 +128,14 @@ __global__ void k_scal_inv_dev(long n, const double *s, double *x) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     x[i] *= a;
 }
-__global__ void k_dot(long n, const double *__restrict__ x, const double *__restrict__ y,
-                      double *partials, unsigned *counter, double *out, int fin) {
-  double s = 0.0;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    s += x[i] * y[i];
-  finish_sum(s, partials, counter, out, fin);
-}
 __global__ void k_sum(long n, const double *__restrict__ x, double *partials, unsigned *counter,
                       double *out) {
   double s = 0.0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     s += x[i];
-  finish_sum(s, partials, counter, out, FIN_ID);
-}
-/* y -= (*coef) x, then ||y|| */
-__global__ void k_axpy_dev_nrm2(long n, const double *coef, const double *__restrict__ x,
-                                double *__restrict__ y, double *partials, unsigned *counter,
-                                double *nrm) {
-  const double a = -*coef;
-  double s = 0.0;
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const double v = y[i] + a * x[i];
-    y[i] = v;
-    s += v * v;
-  }
-  finish_sum(s, partials, counter, nrm, FIN_SQRT);
+  bool last;
+  const double t = grid_sum(s, partials, counter, FIN_ID, &last);
+  if (last && threadIdx.x == 0) *out = t;
 }
 
 /* per-column dot products: grid (bx, m); partials [m][bx] */
@@ -201,9 +147,10 @@ __global__ void k_dot_cols(long n, const double *__restrict__ X, long ldx,
   double s = 0.0;
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
     s += x[i] * y[i];
-  /* finish_sum over the blocks of this column */
+  /* grid reduction over the blocks of this column */
   __shared__ bool am_last;
-  const double b = block_sum(s);
+  __shared__ double sh[32];
+  const double b = block_sum(s, sh);
   if (threadIdx.x == 0) {
     partials[(size_t)c * gridDim.x + blockIdx.x] = b;
     __threadfence();
@@ -215,7 +162,7 @@ __global__ void k_dot_cols(long n, const double *__restrict__ X, long ldx,
   double t = 0.0;
   for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x)
     t += __ldcg(partials + (size_t)c * gridDim.x + i);
-  t = block_sum(t);
+  t = block_sum(t, sh);
   if (threadIdx.x == 0) {
     out[c] = t;
     counters[c] = 0;
@@ -267,22 +214,9 @@ int vscal_inv_dev(long n, const double *s, double *x) {
   k_scal_inv_dev<<<grid_for(n, 4), kThreads, 0, g_ctx.stream>>>(n, s, x);
   return launched("scal_inv_dev");
 }
-int vdot(long n, const double *x, const double *y, double *out) {
-  k_dot<<<grid_for(n, 4), kThreads, 0, g_ctx.stream>>>(n, x, y, g_ctx.red, g_ctx.cnt, out, FIN_ID);
-  return launched("dot");
-}
-int vnrm2(long n, const double *x, double *out) {
-  k_dot<<<grid_for(n, 4), kThreads, 0, g_ctx.stream>>>(n, x, x, g_ctx.red, g_ctx.cnt, out, FIN_SQRT);
-  return launched("nrm2");
-}
 int vsum(long n, const double *x, double *out) {
   k_sum<<<grid_for(n, 4), kThreads, 0, g_ctx.stream>>>(n, x, g_ctx.red, g_ctx.cnt, out);
   return launched("sum");
-}
-int vaxpy_dev_nrm2(long n, const double *coef, const double *x, double *y, double *nrm) {
-  k_axpy_dev_nrm2<<<grid_for(n, 4), kThreads, 0, g_ctx.stream>>>(n, coef, x, y, g_ctx.red,
-                                                                   g_ctx.cnt, nrm);
-  return launched("axpy_dev_nrm2");
 }
 
 static unsigned col_blocks(long n) {
@@ -451,6 +385,44 @@ int pEVSL_B200_Memcpy(void *dst, const void *src, size_t bytes) {
   if (ensure()) return PEVSL_ERR_CUDA;
   if (memcpy_async(dst, src, bytes)) return PEVSL_ERR_CUDA;
   return sync();
+}
+
+int pEVSL_B200_SetDevice(int device) {
+  if (g_ctx.ready) return g_ctx.device == device ? 0 : PEVSL_ERR_ARG;
+  g_req_device = device;
+  return ensure();
+}
+
+/* Events on the library stream, for timing a region of library work. */
+static cudaEvent_t g_user_ev[16];
+static bool g_user_ev_ok = false;
+
+int pEVSL_B200_EventRecord(int slot) {
+  if (ensure() || slot < 0 || slot >= 16) return PEVSL_ERR_ARG;
+  if (!g_user_ev_ok) {
+    for (int i = 0; i < 16; i++)
+      if (fail(cudaEventCreate(&g_user_ev[i]), "cudaEventCreate")) return PEVSL_ERR_CUDA;
+    g_user_ev_ok = true;
+  }
+  return fail(cudaEventRecord(g_user_ev[slot], g_ctx.stream), "cudaEventRecord");
+}
+
+double pEVSL_B200_EventElapsedMs(int a, int b) {
+  if (!g_user_ev_ok || a < 0 || a >= 16 || b < 0 || b >= 16) return -1.0;
+  if (fail(cudaEventSynchronize(g_user_ev[b]), "cudaEventSynchronize")) return -1.0;
+  float ms = 0.f;
+  if (fail(cudaEventElapsedTime(&ms, g_user_ev[a], g_user_ev[b]), "cudaEventElapsedTime")) return -1.0;
+  return (double)ms;
+}
+
+void *pEVSL_B200_HostAlloc(size_t bytes) {
+  void *p = nullptr;
+  if (ensure() || fail(cudaMallocHost(&p, bytes ? bytes : 1), "cudaMallocHost")) return nullptr;
+  return p;
+}
+
+void pEVSL_B200_HostFree(void *p) {
+  if (p) cudaFreeHost(p);
 }
 
 /* Wait for all work queued by the library. */

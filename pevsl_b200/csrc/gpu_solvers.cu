@@ -23,6 +23,7 @@
 #include <string.h>
 
 #include "gpu.cuh"
+#include "gpu_device.cuh"
 
 using namespace pv;
 
@@ -71,6 +72,20 @@ struct SegTimer {
 };
 SegTimer g_t_pol, g_t_orth;
 
+/* process-wide counters of the fused filter kernel (pEVSL_B200_FilterCounters) */
+uint64_t g_filter_launches = 0;
+double g_filter_bytes = 0.0;
+double g_filter_ms = 0.0;
+
+/* algorithmic HBM bytes of one fused filter degree: the CSR (int32 column
+ * indices, fp64 values, int32 row pointers) plus v_k read once, and
+ * v_{k-1}, y read / v_{k+1}, y written (first degree: no v_{k-1}, y only
+ * written) */
+double cheb_step_bytes(const pevsl_devcsr *A, int first) {
+  const double n = A->nrows;
+  return 12.0 * (double)A->nnz + 4.0 * (n + 1) + (first ? 24.0 : 40.0) * n;
+}
+
 /* matvec through the installed operator: fused kernels use the device CSR
  * directly; this is for the plain y = A x steps. */
 int apply_A(pevsl_Data *pevsl, const double *x, double *y) {
@@ -106,6 +121,8 @@ int cheb_apply(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, d
     int st;
     if (A) {
       st = cheb_step(A, vk, vkm1, vkp1, y, cc, t, mu[0], mu[k], k == 1);
+      g_filter_launches++;
+      g_filter_bytes += cheb_step_bytes(A, k == 1);
     } else {
       st = apply_A(pevsl, vk, ax);
       if (!st) st = cheb_combine(n, ax, vk, vkm1, vkp1, y, cc, t, mu[0], mu[k], k == 1);
@@ -140,6 +157,22 @@ long round_ld(long n) { return (n + 31) / 32 * 32; }
 }  // namespace
 
 extern "C" {
+
+/* Filter-kernel counters since the last reset: launches of the fused
+ * Chebyshev degree kernel inside pEVSL_ChebLanNr, their algorithmic bytes,
+ * and the device time of the filter applications that contain them (CUDA
+ * events around each application, so launch gaps are included). */
+void pEVSL_B200_FilterCounters(uint64_t *launches, double *bytes, double *ms) {
+  if (launches) *launches = g_filter_launches;
+  if (bytes) *bytes = g_filter_bytes;
+  if (ms) *ms = g_filter_ms;
+}
+
+void pEVSL_B200_ResetFilterCounters(void) {
+  g_filter_launches = 0;
+  g_filter_bytes = 0.0;
+  g_filter_ms = 0.0;
+}
 
 /* y = p(A) v (pEVSL_ChebAv, SRC/chebpol.c:509-574) on device or managed
  * vectors of length pevsl->n.  Extension entry point: the reference keeps
@@ -591,260 +624,501 @@ int pEVSL_LanTrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pevsl_
   return st;
 }
 
-/* ================================================================ filtered Lanczos */
+/* ================================================================ filtered Lanczos
+ * pEVSL_ChebLanNr (SRC/cheblanNr.c:54-448) for a batch of slices that
+ * advance in lockstep: at every Lanczos step one fused filter kernel per
+ * degree serves all slices (the matrix is read once per degree), the
+ * Gram-Schmidt kernels run batched, and one host read fetches every slice's
+ * alpha and beta.  Each slice keeps its own basis, tridiagonal matrix,
+ * convergence test and stop; a single slice is a batch of one and follows
+ * exactly the reference's sequence of operations. */
+
+struct SliceState {
+  /* inputs */
+  double intv[4];
+  const pevsl_Polparams *pol;
+  int maxit;
+  /* state */
+  double *V;      /* basis, ld x (maxit+1) */
+  double *dT, *eT, *EvalT;
+  double wn, tr0, beta;
+  int nwn, kdim, count, nconv;
+  int active, done;
+  /* outputs */
+  int status, nev, its;
+  double *Lam, *res;
+  pevsl_Parvecs *Rvec;
+};
+
+static int next_pow2(int s) {
+  int p = 1;
+  while (p < s) p <<= 1;
+  return p;
+}
+
+/* Ritz pairs of one finished slice (SRC/cheblanNr.c:339-413): eigenvectors
+ * of T only for Ritz values >= bar, U = V Y, normalise, W = A U, Rayleigh
+ * quotients, interval check, residuals, acceptance below tol. */
+static int ritz_extract(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, long n, long ld,
+                        double tol) {
+  Ctx &c = ctx();
+  const int kdim = S->kdim, nconv = S->nconv, count = S->count;
+  const double bar = S->pol->bar, aa = S->intv[0], bb = S->intv[1];
+  S->Lam = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
+  S->res = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
+  S->Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
+  if (!S->Lam || !S->res || !S->Rvec) return PEVSL_ERR_NOMEM;
+  pEVSL_ParvecsDuplParvec(vinit, nconv, (int)n, S->Rvec);
+  if (nconv > 0 && !S->Rvec->data) return PEVSL_ERR_NOMEM;
+  S->nev = 0;
+  if (kdim <= 0) return 0;
+  int st = 0, nsel = 0;
+  const double te = pevsl_now();
+  /* eigenvalues again: the last convergence test may predate the last step */
+  if (pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) return PEVSL_ERR_EIG;
+  int *sel = (int *)malloc(sizeof(int) * (size_t)kdim);
+  if (!sel) return PEVSL_ERR_NOMEM;
+  for (int i = 0; i < count; i++)
+    if (S->EvalT[i] >= bar) sel[nsel++] = i;
+  double *Y = nullptr;
+  if (nsel > 0) {
+    Y = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)nsel);
+    st = Y ? pevsl_tridiag_eig_sel(kdim, S->dT, S->eT, S->EvalT, nsel, sel, Y) : PEVSL_ERR_NOMEM;
+    if (st) st = PEVSL_ERR_EIG;
+  }
+  pevsl->stats->t_eig += pevsl_now() - te;
+  if (!st && nsel > 0) {
+    double *U = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * (size_t)nsel);
+    double *W = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)ld * (size_t)nsel);
+    double *dY = (double *)ws(WS_PART, sizeof(double) * (size_t)kdim * (size_t)nsel);
+    double *dv = (double *)ws(WS_MOM, sizeof(double) * 3 * (size_t)nsel);
+    double *hv = (double *)malloc(sizeof(double) * 3 * (size_t)nsel);
+    if (!U || !W || !dY || !dv || !hv) st = PEVSL_ERR_NOMEM;
+    if (!st) st = memcpy_async(dY, Y, sizeof(double) * (size_t)kdim * (size_t)nsel);
+    if (!st) st = gemm_nn(n, kdim, nsel, S->V, ld, dY, kdim, U, ld);
+    if (!st) st = vdot_cols(n, nsel, U, ld, U, ld, dv);
+    if (!st) st = memcpy_async(hv, dv, sizeof(double) * (size_t)nsel);
+    if (!st) st = sync();
+    for (int j = 0; j < nsel && !st; j++) {
+      const double t = sqrt(hv[j]);
+      if (t == 0.0) {
+        st = 2; /* zero eigenvector (SRC/cheblanNr.c:377-379) */
+        break;
+      }
+      hv[nsel + j] = 1.0 / t;
+    }
+    if (!st) st = memcpy_async(dv + nsel, hv + nsel, sizeof(double) * (size_t)nsel);
+    if (!st) st = vscal_cols(n, nsel, U, ld, dv + nsel);
+    for (int j = 0; j < nsel && !st; j++) st = apply_A(pevsl, U + (size_t)j * ld, W + (size_t)j * ld);
+    if (!st) st = vdot_cols(n, nsel, W, ld, U, ld, dv);
+    if (!st) st = vaxpy_cols(n, nsel, dv, U, ld, W, ld);
+    if (!st) st = vdot_cols(n, nsel, W, ld, W, ld, dv + 2 * nsel);
+    if (!st) st = memcpy_async(hv, dv, sizeof(double) * 3 * (size_t)nsel);
+    if (!st) st = sync();
+    for (int j = 0; j < nsel && !st; j++) {
+      const double lam = hv[j];
+      if (lam < aa - DBL_EPSILON || lam > bb + DBL_EPSILON) continue;
+      const double r0 = sqrt(hv[2 * nsel + j]);
+      if (r0 < tol) {
+        S->Lam[S->nev] = lam;
+        S->res[S->nev] = r0;
+        st = vcopy(U + (size_t)j * ld, S->Rvec->data + (size_t)S->nev * S->Rvec->ld, n);
+        S->nev++;
+      }
+    }
+    free(hv);
+  }
+  free(Y);
+  free(sel);
+  if (!st) st = sync();
+  return st;
+}
+
+static void free_slice_outputs(SliceState *S) {
+  free(S->Lam);
+  free(S->res);
+  if (S->Rvec) {
+    pEVSL_ParvecsFree(S->Rvec);
+    free(S->Rvec);
+  }
+  S->Lam = S->res = nullptr;
+  S->Rvec = nullptr;
+}
+
+/* Lockstep filtered Lanczos over ns <= kMaxBatch slices sharing vinit. */
+static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol,
+                           pevsl_Parvec *vinit, FILE *fstats) {
+  Ctx &c = ctx();
+  const int N = pevsl->N;
+  const long n = pevsl->n, ld = round_ld(n);
+  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
+  const int Sp = next_pow2(ns);
+  const bool interleaved = A && Sp > 1;
+  unsigned act = 0;
+  size_t basis_cols = 0;
+  int mu_ld = 1;
+  for (int s = 0; s < ns; s++) {
+    SliceState *S = &SL[s];
+    S->maxit = PEVSL_MIN(N, S->maxit);
+    S->status = 0;
+    S->nev = 0;
+    S->its = 0;
+    if (pevsl_check_intv(S->intv, fstats) < 0) {
+      S->done = 1; /* invalid interval: no pairs, status 0 (SRC/cheblanNr.c:96-100) */
+      continue;
+    }
+    if (fstats) {
+      fprintf(fstats, " intv:[%e, %e, %e, %e]\n", S->intv[0], S->intv[1], S->intv[2], S->intv[3]);
+      fprintf(fstats, " ** Cheb Poly of deg = %d, gam = %.15e, bar: %.15e\n", S->pol->deg,
+              S->pol->gam, S->pol->bar);
+    }
+    if (S->pol->gam > 1.0 || S->pol->gam < -1.0) {
+      fprintf(stdout, "gamB error %.15e\n", S->pol->gam);
+      S->status = -1;
+      S->done = 1;
+      continue;
+    }
+    if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
+    act |= 1u << s;
+    basis_cols += (size_t)S->maxit + 1;
+    mu_ld = PEVSL_MAX(mu_ld, S->pol->deg + 1);
+  }
+  if (!act) return 0;
+  /* bases of all active slices in one workspace */
+  double *Vall = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * basis_cols);
+  const size_t ilv = (size_t)n * (size_t)Sp; /* one interleaved block */
+  double *w3 = (double *)ws(WS_CHEB, sizeof(double) * (interleaved ? 5 * ilv : 3 * (size_t)n));
+  double *vrand = (double *)ws(A ? WS_VEC : WS_RITZ2, sizeof(double) * (size_t)n);
+  double *mu_all = interleaved ? (double *)ws(WS_MOM, sizeof(double) * (size_t)Sp * mu_ld) : nullptr;
+  if (!Vall || !w3 || !vrand || (interleaved && !mu_all)) return PEVSL_ERR_NOMEM;
+  int st = 0;
+  size_t off = 0;
+  BatchParams bp{};
+  for (int s = 0; s < ns; s++) {
+    SliceState *S = &SL[s];
+    if (!((act >> s) & 1u)) continue;
+    S->V = Vall + off * (size_t)ld;
+    off += (size_t)S->maxit + 1;
+    S->dT = (double *)malloc(sizeof(double) * (size_t)S->maxit);
+    S->eT = (double *)malloc(sizeof(double) * (size_t)S->maxit);
+    S->EvalT = (double *)malloc(sizeof(double) * (size_t)S->maxit);
+    if (!S->dT || !S->eT || !S->EvalT) return PEVSL_ERR_NOMEM;
+    S->wn = S->tr0 = S->beta = 0.0;
+    S->nwn = S->kdim = S->count = S->nconv = 0;
+    if (interleaved) {
+      st = memcpy_async(mu_all + (size_t)s * mu_ld, S->pol->mu, sizeof(double) * (S->pol->deg + 1));
+      bp.deg[s] = S->pol->deg;
+      bp.cc[s] = S->pol->cc;
+      bp.t1[s] = 1.0 / S->pol->dd;
+      bp.t2[s] = 2.0 / S->pol->dd;
+      if (st) return st;
+    }
+  }
+  SegTimer &t_pol = g_t_pol, &t_orth = g_t_orth;
+  /* y_s = p_s(A) x_s for the slices in mask: x_s = V_s(:,k) (or xin for
+   * all), y_s = V_s(:,k+1) (or column 0) */
+  auto filter = [&](unsigned mask, int kin, const double *xin, int kout) -> int {
+    t_pol.begin();
+    int r = 0;
+    if (!interleaved) {
+      for (int s = 0; s < ns && !r; s++)
+        if ((mask >> s) & 1u)
+          r = cheb_apply(pevsl, SL[s].pol, xin ? xin : SL[s].V + (size_t)kin * ld,
+                         SL[s].V + (size_t)kout * ld, w3, n);
+    } else {
+      double *Z = w3, *Y = w3 + ilv, *buf[3] = {w3 + 2 * ilv, w3 + 3 * ilv, w3 + 4 * ilv};
+      CPtrs src{};
+      VPtrs dst{};
+      int maxdeg = 0;
+      for (int s = 0; s < ns; s++) {
+        src.p[s] = xin ? xin : SL[s].V + (size_t)kin * ld;
+        dst.p[s] = SL[s].V + (size_t)kout * ld;
+        if ((mask >> s) & 1u) maxdeg = PEVSL_MAX(maxdeg, SL[s].pol->deg);
+      }
+      r = b_gather(n, Sp, src, Z, mask);
+      bp.mask = mask;
+      const double *vk = Z, *vkm1 = nullptr;
+      for (int k = 1; k <= maxdeg && !r; k++) {
+        double *vkp1 = buf[(k - 1) % 3];
+        r = cheb_multi(A, Sp, vk, vkm1, vkp1, Y, mu_all, mu_ld, k, bp);
+        /* one read of the matrix serves every slice still filtering */
+        g_filter_launches++;
+        g_filter_bytes += 12.0 * (double)A->nnz + 4.0 * (A->nrows + 1.0);
+        for (int s = 0; s < ns; s++)
+          if (((mask >> s) & 1u) && k <= SL[s].pol->deg)
+            g_filter_bytes += (k == 1 ? 24.0 : 40.0) * (double)A->nrows;
+        vkm1 = vk;
+        vk = vkp1;
+      }
+      if (!r) r = b_scatter(n, Sp, Y, dst, mask);
+      for (int s = 0; s < ns; s++)
+        if ((mask >> s) & 1u) {
+          pevsl->stats->n_polAv++;
+          pevsl->stats->n_mvA += (size_t)SL[s].pol->deg;
+        }
+    }
+    t_pol.end();
+    return r;
+  };
+  cudaEvent_t e_all0, e_all1;
+  cudaEventCreate(&e_all0);
+  cudaEventCreate(&e_all1);
+  cudaEventRecord(e_all0, c.stream);
+  /* filter the start vector, normalise (SRC/cheblanNr.c:164-194) */
+  st = filter(act, 0, vinit->data, 0);
+  {
+    CPtrs x{};
+    for (int s = 0; s < ns; s++) x.p[s] = SL[s].V;
+    if (!st) st = b_dot(n, ns, x, x, c.dscal + 16, FIN_SQRT, act);
+    const double *h = st ? nullptr : fetch_scalars(16, ns);
+    if (!h) st = st ? st : PEVSL_ERR_CUDA;
+    BScal inv{};
+    VPtrs y{};
+    for (int s = 0; s < ns && !st; s++) {
+      inv.v[s] = 1.0 / h[s];
+      y.p[s] = SL[s].V;
+    }
+    if (!st) st = b_scal(n, ns, y, inv, act);
+  }
+  double *dA = c.dscal + 16, *dN0 = c.dscal + 32, *dN = c.dscal + 48;
+  int *dF = c.dflag;
+  double *dW = (double *)ws(WS_SMALL, sizeof(double) * kMaxBatch * (size_t)(off + 1));
+  if (!dW) st = PEVSL_ERR_NOMEM;
+  int k;
+  for (k = 0; act && !st; k++) {
+    CPtrs vprev{}, vk{}, vks{}, Vc{};
+    VPtrs vnew{};
+    BScal mb{};
+    for (int s = 0; s < ns; s++) {
+      if (!((act >> s) & 1u)) continue;
+      SliceState *S = &SL[s];
+      vk.p[s] = S->V + (size_t)k * ld;
+      vnew.p[s] = S->V + (size_t)(k + 1) * ld;
+      vks.p[s] = vnew.p[s];
+      Vc.p[s] = S->V;
+      if (k > 0) vprev.p[s] = S->V + (size_t)(k - 1) * ld;
+      mb.v[s] = -S->beta;
+    }
+    st = filter(act, k, nullptr, k + 1);
+    if (!st && k > 0) st = b_axpy(n, ns, vprev, vnew, mb, act);
+    if (!st) st = b_dot(n, ns, vk, vks, dA, FIN_ID, act);
+    t_orth.begin();
+    if (!st) st = b_axpy_dev_nrm2(n, ns, dA, vk, vnew, dN0, act);
+    /* CGS_DGKS: pass 1, then pass 2 where the first kept <= 1/sqrt(2) */
+    if (!st) st = b_gemvT(n, ns, k + 1, Vc, ld, vks, dW, k + 1, nullptr, act);
+    if (!st) st = b_gemv_sub_nrm(n, ns, k + 1, Vc, ld, dW, k + 1, vnew, dN, nullptr, dF, dN0, kEta, act);
+    if (!st) st = b_gemvT(n, ns, k + 1, Vc, ld, vks, dW, k + 1, dF, act);
+    if (!st) st = b_gemv_sub_nrm(n, ns, k + 1, Vc, ld, dW, k + 1, vnew, dN, dF, nullptr, nullptr, kEta, act);
+    t_orth.end();
+    if (!st) st = memcpy_async(c.hscal + 16, c.dscal + 16, sizeof(double) * 48);
+    if (!st) st = sync();
+    if (st) break;
+    t_pol.flush();
+    t_orth.flush();
+    BScal inv{};
+    VPtrs sc{};
+    unsigned scal_mask = 0;
+    for (int s = 0; s < ns && !st; s++) {
+      if (!((act >> s) & 1u)) continue;
+      SliceState *S = &SL[s];
+      const double alpha = c.hscal[16 + s];
+      double beta = c.hscal[48 + s];
+      if (!isfinite(alpha) || !isfinite(beta)) {
+        S->status = PEVSL_ERR_NONFINITE;
+        S->done = 1;
+        act &= ~(1u << s);
+        continue;
+      }
+      S->dT[k] = alpha;
+      S->wn += fabs(alpha);
+      S->wn += 2.0 * beta;
+      S->nwn += 3;
+      double *znew = S->V + (size_t)(k + 1) * ld;
+      if (beta * S->nwn < orthTol * S->wn) {
+        /* lucky breakdown: restart from a new filtered random vector
+         * (SRC/cheblanNr.c:248-281) */
+        if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
+        st = pevsl_rand_vector_dev(vrand, (int)n);
+        t_pol.begin();
+        if (!st) st = cheb_apply(pevsl, S->pol, vrand, znew, w3 + (interleaved ? 2 * ilv : 0), n);
+        t_pol.end();
+        if (!st) st = vnrm2(n, znew, c.dscal + S_NRM0);
+        if (!st) st = cgs_dgks(S->V, ld, k + 1, znew, n);
+        const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
+        if (!hb) {
+          st = st ? st : PEVSL_ERR_CUDA;
+          break;
+        }
+        st = vscal(znew, n, 1.0 / hb[0]);
+        beta = 0.0;
+      } else {
+        inv.v[s] = 1.0 / beta;
+        sc.p[s] = znew;
+        scal_mask |= 1u << s;
+      }
+      S->beta = beta;
+      S->eT[k] = beta;
+    }
+    if (!st && scal_mask) st = b_scal(n, ns, sc, inv, scal_mask);
+    if (st) break;
+    /* restricted-trace convergence test (SRC/cheblanNr.c:293-332) */
+    for (int s = 0; s < ns; s++) {
+      if (!((act >> s) & 1u)) continue;
+      SliceState *S = &SL[s];
+      if ((k < 30 || (k - 30) % 20 != 0) && k != S->maxit - 1) continue;
+      S->kdim = k + 1;
+      const double te = pevsl_now();
+      if (pevsl_tridiag_eig(S->kdim, S->dT, S->eT, S->EvalT, nullptr)) {
+        st = PEVSL_ERR_EIG;
+        break;
+      }
+      pevsl->stats->t_eig += pevsl_now() - te;
+      S->count = S->kdim;
+      double tr1 = 0.0;
+      S->nconv = 0;
+      for (int i = 0; i < S->count; i++) {
+        if (S->EvalT[i] + 5 * DBL_EPSILON >= S->pol->bar) {
+          tr1 += S->EvalT[i];
+          S->nconv++;
+        }
+      }
+      if (fstats) fprintf(fstats, "  k %4d:   nconv %4d  tr1 %21.15e\n", k, S->nconv, tr1);
+      const bool conv = fabs(tr1 - S->tr0) < 2e-12 || fabs(tr1) + fabs(S->tr0) < 1e-10;
+      S->tr0 = tr1;
+      if (conv || k == S->maxit - 1) {
+        if (!conv && fstats)
+          fprintf(fstats, "The max number of iterations [%d] has been reached. The eigenvalues "
+                          "computed may not have converged\n", S->maxit);
+        act &= ~(1u << s);
+      }
+    }
+  }
+  cudaEventRecord(e_all1, c.stream);
+  const double tr_start = pevsl_now();
+  for (int s = 0; s < ns && !st; s++) {
+    SliceState *S = &SL[s];
+    if (S->done || S->status) continue;
+    S->its = S->kdim;
+    const int rs = ritz_extract(pevsl, S, vinit, n, ld, tol);
+    if (rs) S->status = rs;
+  }
+  pevsl->stats->t_ritz = pevsl_now() - tr_start;
+  cudaEventSynchronize(e_all1);
+  t_pol.flush();
+  t_orth.flush();
+  float ms_all = 0.f;
+  cudaEventElapsedTime(&ms_all, e_all0, e_all1);
+  cudaEventDestroy(e_all0);
+  cudaEventDestroy(e_all1);
+  pevsl_inst *inst = pevsl_inst_of(pevsl);
+  inst->phase_ms[2] = ms_all;
+  inst->phase_ms[3] = t_pol.acc_ms;
+  inst->phase_ms[4] = t_orth.acc_ms;
+  if (A) g_filter_ms += t_pol.acc_ms;
+  pevsl->stats->t_polAv += 1e-3 * t_pol.acc_ms;
+  pevsl->stats->t_reorth += 1e-3 * t_orth.acc_ms;
+  for (int s = 0; s < ns; s++) {
+    free(SL[s].dT);
+    free(SL[s].eT);
+    free(SL[s].EvalT);
+    SL[s].dT = SL[s].eT = SL[s].EvalT = nullptr;
+  }
+  return st;
+}
 
 int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
                     pevsl_Polparams *pol, int *nevOut, double **lamo, pevsl_Parvecs **Wo,
                     double **reso, FILE *fstats) {
   const double tall = pevsl_now();
-  pevsl_inst *inst = pevsl_inst_of(pevsl);
+  *nevOut = 0;
+  *lamo = nullptr;
+  *Wo = nullptr;
+  *reso = nullptr;
   if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   if (ensure()) return PEVSL_ERR_CUDA;
-  const int N = pevsl->N;
-  const long n = pevsl->n, ld = round_ld(n);
-  maxit = PEVSL_MIN(N, maxit);
-  const double bar = pol->bar, gamB = pol->gam;
-  if (pevsl_check_intv(intv, fstats) < 0) {
-    *nevOut = 0;
-    *lamo = nullptr;
-    *Wo = nullptr;
-    *reso = nullptr;
-    return 0;
-  }
-  const double aa = intv[0], bb = intv[1];
-  if (fstats) {
-    fprintf(fstats, " intv:[%e, %e, %e, %e]\n", intv[0], intv[1], intv[2], intv[3]);
-    fprintf(fstats, " ** Cheb Poly of deg = %d, gam = %.15e, bar: %.15e\n", pol->deg, gamB, bar);
-  }
-  if (gamB > 1.0 || gamB < -1.0) {
-    fprintf(stdout, "gamB error %.15e\n", gamB);
-    return -1;
-  }
-  if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
-  Ctx &c = ctx();
-  double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
-  double *w3 = (double *)ws(WS_CHEB, sizeof(double) * 3 * (size_t)n);
-  double *vrand = (double *)ws(WS_VEC, sizeof(double) * (size_t)n);
-  double *dT = (double *)malloc(sizeof(double) * (size_t)maxit);
-  double *eT = (double *)malloc(sizeof(double) * (size_t)maxit);
-  double *EvalT = (double *)malloc(sizeof(double) * (size_t)maxit);
-  if (!V || !w3 || !vrand || !dT || !eT || !EvalT) {
-    free(dT);
-    free(eT);
-    free(EvalT);
-    return PEVSL_ERR_NOMEM;
-  }
-  /* the user-matvec path of cheb_apply uses WS_VEC itself: keep vrand apart */
-  if (!pevsl_builtin_A(pevsl)) {
-    vrand = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)n);
-    if (!vrand) return PEVSL_ERR_NOMEM;
-  }
-  SegTimer &t_pol = g_t_pol, &t_orth = g_t_orth;
-  t_pol.init();
-  t_orth.init();
-  cudaEvent_t e_all0, e_all1, e_r0;
-  cudaEventCreate(&e_all0);
-  cudaEventCreate(&e_all1);
-  cudaEventCreate(&e_r0);
-  cudaEventRecord(e_all0, c.stream);
-#define VC(j) (V + (size_t)(j) * ld)
-  int st = 0, k, kdim = 0, count = 0, nconv = 0;
-  /* filter the start vector and normalise it (SRC/cheblanNr.c:164-194) */
-  t_pol.begin();
-  st = cheb_apply(pevsl, pol, vinit->data, VC(0), w3, n);
-  t_pol.end();
-  if (!st) st = vnrm2(n, VC(0), c.dscal + S_TMP0);
-  const double *h0 = st ? nullptr : fetch_scalars(S_TMP0, 1);
-  if (!h0) st = st ? st : PEVSL_ERR_CUDA;
-  if (!st) st = vscal(VC(0), n, 1.0 / h0[0]);
-  double wn = 0.0, tr0 = 0.0, tr1, alpha, beta = 0.0;
-  int nwn = 0;
-  for (k = 0; k < maxit && !st; k++) {
-    double *z = VC(k), *znew = VC(k + 1);
-    t_pol.begin();
-    st = cheb_apply(pevsl, pol, z, znew, w3, n);
-    t_pol.end();
-    if (!st && k > 0) st = vaxpy(n, -beta, VC(k - 1), znew);
-    if (!st) st = vdot(n, z, znew, c.dscal + S_ALPHA);
-    t_orth.begin();
-    if (!st) st = vaxpy_dev_nrm2(n, c.dscal + S_ALPHA, z, znew, c.dscal + S_NRM0);
-    if (!st) st = cgs_dgks(V, ld, k + 1, znew, n);
-    t_orth.end();
-    if (!st) st = memcpy_async(c.hscal + S_ALPHA, c.dscal + S_ALPHA, sizeof(double) * 4);
-    if (!st) st = sync();
-    if (st) break;
-    alpha = c.hscal[S_ALPHA];
-    beta = c.hscal[S_NRM];
-    if (!isfinite(alpha) || !isfinite(beta)) {
-      st = PEVSL_ERR_NONFINITE;
-      break;
-    }
-    dT[k] = alpha;
-    wn += fabs(alpha);
-    wn += 2.0 * beta;
-    nwn += 3;
-    if (beta * nwn < orthTol * wn) {
-      /* lucky breakdown: restart from a new filtered random vector
-       * (SRC/cheblanNr.c:248-281) */
-      if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
-      st = pevsl_rand_vector_dev(vrand, (int)n);
-      t_pol.begin();
-      if (!st) st = cheb_apply(pevsl, pol, vrand, znew, w3, n);
-      t_pol.end();
-      if (!st) st = vnrm2(n, znew, c.dscal + S_NRM0);
-      if (!st) st = cgs_dgks(V, ld, k + 1, znew, n);
-      const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
-      if (!hb) {
-        st = st ? st : PEVSL_ERR_CUDA;
-        break;
-      }
-      st = vscal(znew, n, 1.0 / hb[0]);
-      beta = 0.0;
-    } else {
-      st = vscal(znew, n, 1.0 / beta);
-    }
-    eT[k] = beta;
-    if ((k < 30 || (k - 30) % 20 != 0) && k != maxit - 1) continue;
-    /* restricted-trace convergence test (SRC/cheblanNr.c:293-332) */
-    kdim = k + 1;
-    const double te = pevsl_now();
-    if (pevsl_tridiag_eig(kdim, dT, eT, EvalT, nullptr)) {
-      st = PEVSL_ERR_EIG;
-      break;
-    }
-    pevsl->stats->t_eig += pevsl_now() - te;
-    count = kdim;
-    tr1 = 0;
-    nconv = 0;
-    for (int i = 0; i < count; i++) {
-      if (EvalT[i] + 5 * DBL_EPSILON >= bar) {
-        tr1 += EvalT[i];
-        nconv++;
-      }
-    }
-    if (fstats) fprintf(fstats, "  k %4d:   nconv %4d  tr1 %21.15e\n", k, nconv, tr1);
-    if (fabs(tr1 - tr0) < 2e-12 || fabs(tr1) + fabs(tr0) < 1e-10) break;
-    tr0 = tr1;
-  }
-  if (!st && k >= maxit && fstats)
-    fprintf(fstats, "The max number of iterations [%d] has been reached. The eigenvalues computed "
-                    "may not have converged\n", maxit);
-  inst->last_its = kdim;
-  inst->last_nconv = nconv;
-  /* ---------------- Ritz pairs for Ritz values of p(A) >= bar ---------- */
-  int nev = 0;
-  double *Lam = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
-  double *res = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
-  pevsl_Parvecs *Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
-  if (!Lam || !res || !Rvec) st = st ? st : PEVSL_ERR_NOMEM;
-  cudaEventRecord(e_r0, c.stream);
-  const double tr_start = pevsl_now();
-  if (!st) {
-    pEVSL_ParvecsDuplParvec(vinit, nconv, (int)n, Rvec);
-    if (nconv > 0 && !Rvec->data) st = PEVSL_ERR_NOMEM;
-  }
-  int nsel = 0;
-  int *sel = nullptr;
-  if (!st && kdim > 0) {
-    const double te = pevsl_now();
-    /* eigenvalues again (the last test may predate the last step) */
-    st = pevsl_tridiag_eig(kdim, dT, eT, EvalT, nullptr) ? PEVSL_ERR_EIG : 0;
-    sel = (int *)malloc(sizeof(int) * (size_t)kdim);
-    for (int i = 0; i < count && !st; i++)
-      if (EvalT[i] >= bar) sel[nsel++] = i;
-    double *Y = nullptr;
-    if (!st && nsel > 0) {
-      Y = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)nsel);
-      st = Y ? pevsl_tridiag_eig_sel(kdim, dT, eT, EvalT, nsel, sel, Y) : PEVSL_ERR_NOMEM;
-      if (st) st = PEVSL_ERR_EIG;
-    }
-    pevsl->stats->t_eig += pevsl_now() - te;
-    if (!st && nsel > 0) {
-      /* U = V(:,0:kdim) Y, normalise, W = A U, lambda = <W,U>, residuals */
-      double *U = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * (size_t)nsel);
-      double *W = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)ld * (size_t)nsel);
-      double *dY = (double *)ws(WS_PART, sizeof(double) * (size_t)kdim * (size_t)nsel);
-      double *dv = (double *)ws(WS_MOM, sizeof(double) * 3 * (size_t)nsel);
-      double *hv = (double *)malloc(sizeof(double) * 3 * (size_t)nsel);
-      if (!U || !W || !dY || !dv || !hv) st = PEVSL_ERR_NOMEM;
-      if (!st) st = memcpy_async(dY, Y, sizeof(double) * (size_t)kdim * (size_t)nsel);
-      if (!st) st = gemm_nn(n, kdim, nsel, V, ld, dY, kdim, U, ld);
-      if (!st) st = vdot_cols(n, nsel, U, ld, U, ld, dv);
-      if (!st) st = memcpy_async(hv, dv, sizeof(double) * (size_t)nsel);
-      if (!st) st = sync();
-      for (int j = 0; j < nsel && !st; j++) {
-        const double t = sqrt(hv[j]);
-        if (t == 0.0) {
-          st = 2; /* zero eigenvector (SRC/cheblanNr.c:377-379) */
-          break;
-        }
-        hv[nsel + j] = 1.0 / t;
-      }
-      if (!st) st = memcpy_async(dv + nsel, hv + nsel, sizeof(double) * (size_t)nsel);
-      if (!st) st = vscal_cols(n, nsel, U, ld, dv + nsel);
-      for (int j = 0; j < nsel && !st; j++) st = apply_A(pevsl, U + (size_t)j * ld, W + (size_t)j * ld);
-      if (!st) st = vdot_cols(n, nsel, W, ld, U, ld, dv);
-      if (!st) st = vaxpy_cols(n, nsel, dv, U, ld, W, ld);
-      if (!st) st = vdot_cols(n, nsel, W, ld, W, ld, dv + 2 * nsel);
-      if (!st) st = memcpy_async(hv, dv, sizeof(double) * 3 * (size_t)nsel);
-      if (!st) st = sync();
-      for (int j = 0; j < nsel && !st; j++) {
-        const double lam = hv[j];
-        if (lam < aa - DBL_EPSILON || lam > bb + DBL_EPSILON) continue;
-        const double r0 = sqrt(hv[2 * nsel + j]);
-        if (r0 < tol) {
-          Lam[nev] = lam;
-          res[nev] = r0;
-          st = vcopy(U + (size_t)j * ld, Rvec->data + (size_t)nev * Rvec->ld, n);
-          nev++;
-        }
-      }
-      free(hv);
-    }
-    free(Y);
-  }
-  free(sel);
-  if (!st) st = sync();
-#undef VC
-  cudaEventRecord(e_all1, c.stream);
-  cudaEventSynchronize(e_all1);
-  t_pol.flush();
-  t_orth.flush();
-  float ms_all = 0.f, ms_ritz = 0.f;
-  cudaEventElapsedTime(&ms_all, e_all0, e_all1);
-  cudaEventElapsedTime(&ms_ritz, e_r0, e_all1);
-  inst->phase_ms[2] = ms_all;
-  inst->phase_ms[3] = t_pol.acc_ms;
-  inst->phase_ms[4] = t_orth.acc_ms;
-  inst->phase_ms[5] = ms_ritz;
-  pevsl->stats->t_polAv += 1e-3 * t_pol.acc_ms;
-  pevsl->stats->t_reorth += 1e-3 * t_orth.acc_ms;
-  cudaEventDestroy(e_all0);
-  cudaEventDestroy(e_all1);
-  cudaEventDestroy(e_r0);
-  free(dT);
-  free(eT);
-  free(EvalT);
+  SliceState S;
+  memset(&S, 0, sizeof S);
+  memcpy(S.intv, intv, sizeof S.intv);
+  S.pol = pol;
+  S.maxit = maxit;
+  g_t_pol.init();
+  g_t_orth.init();
+  int st = cheblannr_group(pevsl, &S, 1, tol, vinit, fstats);
+  pevsl_inst *inst = pevsl_inst_of(pevsl);
+  inst->last_its = S.kdim;
+  inst->last_nconv = S.nconv;
+  if (!st) st = S.status;
   if (st) {
-    free(Lam);
-    free(res);
-    if (Rvec) {
-      pEVSL_ParvecsFree(Rvec);
-      free(Rvec);
-    }
-    *nevOut = 0;
-    *lamo = nullptr;
-    *Wo = nullptr;
-    *reso = nullptr;
+    free_slice_outputs(&S);
     return st;
   }
-  *nevOut = nev;
-  *lamo = Lam;
-  *Wo = Rvec;
-  *reso = res;
-  pevsl->stats->t_ritz = pevsl_now() - tr_start;
+  *nevOut = S.nev;
+  *lamo = S.Lam;
+  *Wo = S.Rvec;
+  *reso = S.res;
   pevsl->stats->t_iter = pevsl_now() - tall;
   return 0;
+}
+
+/* All slices of an interval through the lockstep solver, up to kMaxBatch at
+ * a time; slice s gets intvs[4s..4s+3], pols[s], maxits[s].  Per-slice
+ * outputs as pEVSL_ChebLanNr; status[s] per slice; returns the first
+ * nonzero status.  Equal to calling pEVSL_ChebLanNr slice by slice, except
+ * that the random restart vectors after a lucky breakdown are drawn in
+ * lockstep order. */
+int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intvs,
+                              const int *maxits, double tol, pevsl_Parvec *vinit,
+                              pevsl_Polparams *pols, int *nevOut, double **lamo,
+                              pevsl_Parvecs **Wo, double **reso, int *its, int *status,
+                              FILE *fstats) {
+  const double tall = pevsl_now();
+  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  if (nslices < 0) return PEVSL_ERR_ARG;
+  int first_err = 0;
+  g_t_pol.init();
+  g_t_orth.init();
+  double ms_total = 0.0, pol_total = 0.0, orth_total = 0.0;
+  for (int s0 = 0; s0 < nslices; s0 += kMaxBatch) {
+    const int ns = PEVSL_MIN(kMaxBatch, nslices - s0);
+    SliceState SL[kMaxBatch];
+    memset(SL, 0, sizeof SL);
+    for (int s = 0; s < ns; s++) {
+      memcpy(SL[s].intv, intvs + 4 * (size_t)(s0 + s), sizeof SL[s].intv);
+      SL[s].pol = &pols[s0 + s];
+      SL[s].maxit = maxits[s0 + s];
+    }
+    int st = cheblannr_group(pevsl, SL, ns, tol, vinit, fstats);
+    pevsl_inst *inst = pevsl_inst_of(pevsl);
+    ms_total += inst->phase_ms[2];
+    pol_total += inst->phase_ms[3];
+    orth_total += inst->phase_ms[4];
+    for (int s = 0; s < ns; s++) {
+      SliceState *S = &SL[s];
+      const int ss = st ? st : S->status;
+      status[s0 + s] = ss;
+      its[s0 + s] = S->kdim;
+      if (ss) {
+        free_slice_outputs(S);
+        nevOut[s0 + s] = 0;
+        lamo[s0 + s] = nullptr;
+        Wo[s0 + s] = nullptr;
+        reso[s0 + s] = nullptr;
+        if (!first_err) first_err = ss;
+      } else {
+        nevOut[s0 + s] = S->nev;
+        lamo[s0 + s] = S->Lam;
+        Wo[s0 + s] = S->Rvec;
+        reso[s0 + s] = S->res;
+      }
+    }
+  }
+  pevsl_inst *inst = pevsl_inst_of(pevsl);
+  inst->phase_ms[2] = ms_total;
+  inst->phase_ms[3] = pol_total;
+  inst->phase_ms[4] = orth_total;
+  pevsl->stats->t_iter = pevsl_now() - tall;
+  return first_err;
 }
 
 }  // extern "C"

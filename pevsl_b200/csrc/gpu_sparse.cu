@@ -24,6 +24,7 @@
 #include <string.h>
 
 #include "gpu.cuh"
+#include "gpu_device.cuh"
 
 namespace pv {
 
@@ -81,11 +82,10 @@ __global__ void __launch_bounds__(kThreads)
   const unsigned mask = group_mask<L>();
   const double r = group_sum<L>(row_dot<L>(row, ia, ja, a, vk, lane), mask);
   if (lane == 0) {
-    const double x = vk[row];
-    double w = (r - cc * x) * t;
-    if (vkm1) w -= vkm1[row];
+    double w, yv = first ? 0.0 : y[row];
+    cheb_update(r, vk[row], vkm1 ? vkm1 + row : nullptr, cc, t, mu0, muk, first, &w, &yv);
     vkp1[row] = w;
-    y[row] = first ? mu0 * x + muk * w : y[row] + muk * w;
+    y[row] = yv;
   }
 }
 
@@ -94,12 +94,88 @@ __global__ void k_cheb_combine(long n, const double *__restrict__ ax, const doub
                                double *__restrict__ y, double cc, double t, double mu0, double muk,
                                int first) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    const double x = vk[i];
-    double w = (ax[i] - cc * x) * t;
-    if (vkm1) w -= vkm1[i];
+    double w, yv = first ? 0.0 : y[i];
+    cheb_update(ax[i], vk[i], vkm1 ? vkm1 + i : nullptr, cc, t, mu0, muk, first, &w, &yv);
     vkp1[i] = w;
-    y[i] = first ? mu0 * x + muk * w : y[i] + muk * w;
+    y[i] = yv;
   }
+}
+
+/* ---------------------------------------------------------------- CSR-stream
+ * Short rows (the stencil matrices of this path have 5-16 entries): a warp
+ * owns 32 consecutive rows.  Its lanes stream the rows' entries in
+ * contiguous, independent 8-deep batches (column index, value, gathered x),
+ * stage the products a[j]*x[ja[j]] in shared memory, and each lane then adds
+ * its own row's products in index order -- the summation order of the
+ * reference's row loop (SRC/spmat.c:188-193), so the result matches it to
+ * the last bit when the products are not fused.  The epilogue runs one
+ * thread per row, so the vector traffic is coalesced. */
+constexpr int kStreamChunk = 256; /* staged entries per warp per pass */
+
+struct EpiStore {
+  double *y;
+  __device__ __forceinline__ void operator()(int row, double r) const { y[row] = r; }
+};
+
+struct EpiCheb {
+  const double *vk, *vkm1;
+  double *vkp1, *y;
+  double cc, t, mu0, muk;
+  int first;
+  __device__ __forceinline__ void operator()(int row, double r) const {
+    double w, yv = first ? 0.0 : y[row];
+    cheb_update(r, vk[row], vkm1 ? vkm1 + row : nullptr, cc, t, mu0, muk, first, &w, &yv);
+    vkp1[row] = w;
+    y[row] = yv;
+  }
+};
+
+template <class Epi>
+__global__ void __launch_bounds__(kThreads)
+    k_csr_stream(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                 const double *__restrict__ a, const double *__restrict__ x, Epi epi) {
+  __shared__ double prod[kThreads / 32][kStreamChunk];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long r0l = ((long)blockIdx.x * (kThreads / 32) + w) * 32;
+  if (r0l >= n) return; /* the whole warp leaves */
+  const int r0 = (int)r0l;
+  const int nr = n - r0 < 32 ? n - r0 : 32;
+  const int row = r0 + lane;
+  const int base = ia[r0], end = ia[r0 + nr];
+  int rs = 0, re = 0;
+  if (lane < nr) {
+    rs = ia[row] - base;
+    re = ia[row + 1] - base;
+  }
+  double acc = 0.0;
+  double *pw = prod[w];
+  const int len = end - base;
+  for (int c0 = 0; c0 < len; c0 += kStreamChunk) {
+    int col[kStreamChunk / 32];
+    double val[kStreamChunk / 32];
+#pragma unroll
+    for (int q = 0; q < kStreamChunk / 32; q++) {
+      const int t = c0 + q * 32 + lane;
+      col[q] = t < len ? ja[base + t] : -1;
+      val[q] = t < len ? a[base + t] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < kStreamChunk / 32; q++) {
+      const double xv = col[q] >= 0 ? __ldg(x + col[q]) : 0.0;
+      pw[q * 32 + lane] = __dmul_rn(val[q], xv);
+    }
+    __syncwarp();
+    const int lo = rs > c0 ? rs : c0;
+    const int hi = re < c0 + kStreamChunk ? re : c0 + kStreamChunk;
+    for (int t = lo; t < hi; t++) acc = __dadd_rn(acc, pw[t - c0]);
+    __syncwarp();
+  }
+  if (lane < nr) epi(row, acc);
+}
+
+static unsigned stream_grid(int n) {
+  const long rows_per_block = (kThreads / 32) * 32;
+  return (unsigned)((n + rows_per_block - 1) / rows_per_block);
 }
 
 /* KPM degree for s <= 32*CPL interleaved vectors; one warp per row (grid
@@ -124,7 +200,23 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
     for (int q = 0; q < CPL; q++) r[q] = 0.0;
     const int e = ia[row + 1];
-    for (int j = ia[row]; j < e; j++) {
+    int j = ia[row];
+    /* four entries per iteration: their loads are independent and in flight
+     * together; each column still accumulates in entry order */
+    for (; j + 3 < e; j += 4) {
+      const double a0 = a[j], a1 = a[j + 1], a2 = a[j + 2], a3 = a[j + 3];
+      const double *x0 = Xk + (size_t)ja[j] * ld, *x1 = Xk + (size_t)ja[j + 1] * ld;
+      const double *x2 = Xk + (size_t)ja[j + 2] * ld, *x3 = Xk + (size_t)ja[j + 3] * ld;
+#pragma unroll
+      for (int q = 0; q < CPL; q++) {
+        const int c = lane + 32 * q;
+        if (c < s) {
+          const double v0 = x0[c], v1 = x1[c], v2 = x2[c], v3 = x3[c];
+          r[q] = fma(a3, v3, fma(a2, v2, fma(a1, v1, fma(a0, v0, r[q]))));
+        }
+      }
+    }
+    for (; j < e; j++) {
       const double aj = a[j];
       const double *xr = Xk + (size_t)ja[j] * ld;
 #pragma unroll
@@ -229,6 +321,11 @@ __global__ void k_block_normalize(long n, int s, int ld, double *X, const double
 
 int spmv(const pevsl_devcsr *A, const double *x, double *y) {
   if (A->nrows <= 0) return 0;
+  if (A->lanes == 0) {
+    k_csr_stream<<<stream_grid(A->nrows), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a,
+                                                                       x, EpiStore{y});
+    return launched("spmv_stream");
+  }
   PV_LANE_SWITCH(k_spmv, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, x, y);
   return launched("spmv");
 }
@@ -236,6 +333,12 @@ int spmv(const pevsl_devcsr *A, const double *x, double *y) {
 int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1, double *y,
               double cc, double t, double mu0, double muk, int first) {
   if (A->nrows <= 0) return 0;
+  if (A->lanes == 0) {
+    EpiCheb e{vk, vkm1, vkp1, y, cc, t, mu0, muk, first};
+    k_csr_stream<<<stream_grid(A->nrows), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a,
+                                                                       vk, e);
+    return launched("cheb_step_stream");
+  }
   PV_LANE_SWITCH(k_cheb_step, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y,
                  cc, t, mu0, muk, first);
   return launched("cheb_step");
@@ -287,16 +390,18 @@ int block_normalize(long n, int s, int ld, double *X, const double *nrm2) {
 /* ================================================================ parcsr API */
 using namespace pv;
 
+/* 0 selects the CSR-stream kernels (rows up to ~24 entries on average);
+ * longer rows get a group of L lanes per row, L the next power of two. */
 static int choose_lanes(double avg) {
+  if (avg <= 24.0) return 0;
   int L = 1;
   while (L < 32 && L < avg) L <<= 1;
   return L;
 }
 
-static void *alloc_managed(size_t bytes) {
+static void *alloc_dev(size_t bytes) {
   void *p = nullptr;
-  if (fail(cudaMallocManaged(&p, bytes ? bytes : 16, cudaMemAttachGlobal), "cudaMallocManaged"))
-    return nullptr;
+  if (fail(cudaMalloc(&p, bytes ? bytes : 16), "cudaMalloc matrix")) return nullptr;
   return p;
 }
 
@@ -360,25 +465,17 @@ int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
   const char *lenv = getenv("PEVSL_B200_LANES");
   if (lenv) {
     const int L = atoi(lenv);
-    if (L == 1 || L == 2 || L == 4 || L == 8 || L == 16 || L == 32) d->lanes = L;
+    if (L == 0 || L == 1 || L == 2 || L == 4 || L == 8 || L == 16 || L == 32) d->lanes = L;
   }
-  d->ia = (int *)alloc_managed(sizeof(int) * (size_t)(nr + 1));
-  d->ja = (int *)alloc_managed(sizeof(int) * (size_t)nnz);
-  d->a = (double *)alloc_managed(sizeof(double) * (size_t)nnz);
+  d->ia = (int *)alloc_dev(sizeof(int) * (size_t)(nr + 1));
+  d->ja = (int *)alloc_dev(sizeof(int) * (size_t)nnz);
+  d->a = (double *)alloc_dev(sizeof(double) * (size_t)nnz);
   if (!d->ia || !d->ja || !d->a) {
     cudaFree(d->ia);
     cudaFree(d->ja);
     cudaFree(d->a);
     free(d);
     return PEVSL_ERR_NOMEM;
-  }
-  {
-    /* keep the matrix resident in HBM (advice is optional: errors ignored) */
-    const int dev = ctx().device;
-    cudaMemAdvise(d->ia, sizeof(int) * (size_t)(nr + 1), cudaMemAdviseSetPreferredLocation, dev);
-    cudaMemAdvise(d->ja, sizeof(int) * (size_t)nnz, cudaMemAdviseSetPreferredLocation, dev);
-    cudaMemAdvise(d->a, sizeof(double) * (size_t)nnz, cudaMemAdviseSetPreferredLocation, dev);
-    cudaGetLastError();
   }
   int st = memcpy_async(d->ia, Ai->ia, sizeof(int) * (size_t)(nr + 1));
   if (!st) st = memcpy_async(d->ja, Ai->ja, sizeof(int) * (size_t)nnz);

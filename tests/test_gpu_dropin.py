@@ -1,0 +1,63 @@
+"""The reference's own driver programs on this library (drop-in check).
+
+tests/dropin/Makefile compiles TESTS/Lap/LapPLanN.c and
+TESTS0/Matvec/test1.c of the reference, unchanged, against include/pevsl.h
+and links them to libpevsl_b200.so.  Running them must reproduce what the
+reference prints for the same arguments: the README configuration's slices
+and per-slice eigenvalue counts (equal to the analytic counts), and a
+parallel-vs-sequential SpMV difference of 0.
+"""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import HERE, golden
+
+pytestmark = pytest.mark.gpu
+BUILD = os.path.join(HERE, "dropin", "_build")
+
+
+def binary(name):
+    path = os.path.join(BUILD, name)
+    if not os.path.exists(path):
+        if os.path.isdir("/root/reference"):
+            subprocess.run(["make", "-s", "-C", os.path.join(HERE, "dropin")], check=True)
+        else:
+            pytest.fail(f"{path} missing: build tests/dropin where the reference tree exists")
+    return path
+
+
+def test_reference_laplacian_driver(gpu, tmp_path):
+    exe = binary("LapPLanN")
+    os.makedirs(tmp_path / "OUT")
+    r = subprocess.run([exe, "-nx", "20", "-ny", "20", "-nz", "20", "-a", "0.6", "-b", "1.2",
+                        "-nslices", "5", "-ngroups", "1"], cwd=tmp_path, capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    out = (tmp_path / "OUT" / "LapPLanN_G0.out").read_text()
+    found = [(int(a), int(b)) for a, b in
+             re.findall(r"\[Group 0\]: number of eigenvalues: (\d+), found: (\d+)", out)]
+    assert found == [(21, 21), (24, 24), (27, 27), (19, 19), (27, 27)], found
+    # slices: the reference's run with the same (glibc, srand(0)) stream
+    sl = [tuple(float(x) for x in m) for m in
+          re.findall(r"\s*\d+: \[\s*([-\d.e+]+)\s*,\s*([-\d.e+]+)\]", out)]
+    g = golden("lap20_kpm.json")["cases"]["glibc"]["sli"]
+    assert np.max(np.abs(np.array([s[0] for s in sl] + [sl[-1][1]]) - g)) <= 1e-12 * 1.2
+    degs = [int(x) for x in re.findall(r"polynomial \[type \d\] deg (\d+)", out)]
+    assert degs == [59, 73, 92, 96, 113]
+    assert "KPMDOS: estimated eig count in interval: 118.37" in r.stdout
+
+
+def test_reference_matvec_driver(gpu):
+    """TESTS0/Matvec/test1.c writes x.data[i] from the host (managed memory)
+    and compares pEVSL_ParcsrMatvec with the sequential pEVSL_Matvec."""
+    exe = binary("MatvecTest1")
+    r = subprocess.run([exe, "-nx", "16", "-ny", "16", "-nz", "16", "-ngroups", "1"],
+                       capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stdout + r.stderr
+    m = re.search(r"Matvec \|\|SEQ-PARA\|\| = ([-\d.e+]+)", r.stdout)
+    assert m, r.stdout
+    assert float(m.group(1)) == 0.0

@@ -58,15 +58,16 @@ def test_matvec_golden(gpu):
         assert rel(y, case["y"]) <= 1e-14, key
 
 
-@pytest.mark.parametrize("per_row", [1, 3, 7, 13, 29, 70, "ragged"])
+@pytest.mark.parametrize("per_row", [1, 3, 7, 13, 29, 70, "ragged", "ragged_short"])
 def test_spmv_lane_widths(gpu, oracle, per_row):
-    """Rows of 1..70 entries select every lane width (1..32 threads per row);
-    'ragged' mixes empty rows and long rows."""
+    """Rows of 1..70 entries select the CSR-stream kernel (short rows) or a
+    lane width of 1..32 threads per row; 'ragged' mixes empty and long rows."""
     n = 3001
-    if per_row == "ragged":
+    if per_row in ("ragged", "ragged_short"):
         rng = np.random.default_rng(5)
-        pr = rng.integers(0, 120, size=n)
+        pr = rng.integers(0, 120 if per_row == "ragged" else 40, size=n)
         pr[::7] = 0
+        pr[-40:] = 0
         A = random_csr(n, pr, 1)
     else:
         A = random_csr(n, per_row, per_row)
@@ -74,6 +75,25 @@ def test_spmv_lane_widths(gpu, oracle, per_row):
     y = dev_matrix(A).matvec(x)
     ref = oracle.matvec(A, x)
     assert np.max(np.abs(y - ref)) <= 1e-14 * max(1.0, np.max(np.abs(ref))) * 8
+
+
+@pytest.mark.parametrize("lanes", [0, 1, 2, 4, 8, 16, 32])
+def test_every_spmv_kernel_on_one_matrix(gpu, oracle, monkeypatch, lanes):
+    """PEVSL_B200_LANES forces each kernel variant on the same ragged matrix;
+    the CSR-stream kernel (lanes 0) sums in the reference's order without
+    fused multiply-adds, so it matches the sequential row loop exactly."""
+    monkeypatch.setenv("PEVSL_B200_LANES", str(lanes))
+    rng = np.random.default_rng(11)
+    pr = rng.integers(0, 300, size=2000)
+    pr[5:9] = 0
+    A = random_csr(2000, pr, 3)
+    x = rng.standard_normal(2000)
+    y = dev_matrix(A).matvec(x)
+    ref = oracle.matvec(A, x)
+    if lanes == 0:
+        assert np.array_equal(y, ref)
+    else:
+        assert np.max(np.abs(y - ref)) <= 1e-13 * max(1.0, np.max(np.abs(ref)))
 
 
 def test_spmv_empty_and_tiny(gpu, oracle):
@@ -346,3 +366,47 @@ def test_user_matvec_callback(gpu):
     assert cb["status"] == 0 and cb["nev"] == fused["nev"] and cb["its"] == fused["its"]
     assert rel(cb["lam"], fused["lam"]) <= 1e-10
     assert rel(mu_c, mu_f) <= 1e-12 and abs(ec_c - ec_f) <= 1e-10 * abs(ec_f)
+
+
+# ---------------------------------------------------------------- batched slices
+@pytest.mark.parametrize("name", ["lap10_kpm_gauss", "lap30x30_kpm_glibc", "lap12_landos_gauss",
+                                  "lap20_readme_glibc", "lap20_lantr_gauss"])
+def test_batched_pipeline_golden_and_bitwise(gpu, name):
+    """All slices in lockstep (pEVSL_B200_ChebLanNrBatch): same goldens, and
+    bit-for-bit the results of the slice-by-slice drop-in path (2, 3 and 5
+    slices: batch widths 2, 4 and 8 with padded entries)."""
+    g = golden("pipelines.json")[name]
+    A = dev_matrix(laplacian(*g["grid"]))
+    rb = pv.solve_interval(A, pv.SliceRun(**g["spec"]), batched=True)
+    check_pipeline(rb, g, g["grid"])
+    rs = pv.solve_interval(A, pv.SliceRun(**g["spec"]), batched=False)
+    assert rb.its == rs.its and rb.nev == rs.nev
+    for a, b in zip(rb.lam, rs.lam):
+        assert np.array_equal(a, b)
+    for a, b in zip(rb.res, rs.res):
+        assert np.array_equal(a, b)
+
+
+def test_batch_mixed_statuses(gpu):
+    """Invalid interval (no pairs, status 0), filter centre outside [-1,1]
+    (status -1) and valid slices in one batch."""
+    A = laplacian(10, 10, 10)
+    M = dev_matrix(A)
+    good = [[0.6, 1.0, 0.0, 12.0], [1.0, 1.5, 0.0, 12.0]]
+    filters = [pv.findpol(iv)[1] for iv in good]
+    bad = pv.Filter(filters[0].type, filters[0].deg, 2.0, filters[0].bar, filters[0].cc,
+                    filters[0].dd, filters[0].mu)
+    intvs = [good[0], [1.5, 1.0, 0.0, 12.0], good[1], good[0]]
+    fl = [filters[0], filters[0], filters[1], bad]
+    v0 = np.cos(np.arange(A.n) * 0.2)
+    with pv.Instance(M) as ev:
+        r, outs = pv.cheblannr_batch(ev, intvs, [300] * 4, 1e-8, v0, fl)
+        single = [ev.cheblannr(iv, 300, 1e-8, v0, f) for iv, f in zip(good, filters)]
+    assert r == -1
+    assert [o["status"] for o in outs] == [0, 0, 0, -1]
+    assert outs[1]["nev"] == 0
+    for o, s in zip([outs[0], outs[2]], single):
+        assert o["nev"] == s["nev"] and o["its"] == s["its"]
+        assert np.array_equal(o["lam"], s["lam"])
+        ex = exact_eig_lap(10, 10, 10, *(good[0][:2] if s is single[0] else good[1][:2]))
+        assert len(ex) == o["nev"]
