@@ -86,6 +86,8 @@ Ctx &ctx();
 int ensure();                 /* initialise the context; 0 or PEVSL_ERR_CUDA */
 int fail(cudaError_t e, const char *what);
 int launched(const char *what); /* count a launch and check for errors */
+/* point the L2 persisting window at [base, base+bytes) if enabled */
+void l2_window(const void *base, size_t bytes);
 int sync();
 void *ws(int slot, size_t bytes);
 int memcpy_async(void *dst, const void *src, size_t bytes);
@@ -176,6 +178,16 @@ int b_gemv_sub_nrm(long n, int S, int k, CPtrs V, long ldv, const double *w, lon
  * (X[i*S + s]); mu is S rows of mu_ld coefficients */
 int cheb_multi(const pevsl_devcsr *A, int S, const double *vk, const double *vkm1, double *vkp1,
                double *y, const double *mu, int mu_ld, int k, const BatchParams &p);
+
+/* ---------------------------------------------------------------- FP32 (mixed) */
+int csr_make_fp32(pevsl_devcsr *A); /* FP32 copy of the values, once */
+int b_gather32(long n, int S, CPtrs src, float *Z, unsigned mask);
+int b_scatter32(long n, int S, const float *Y, VPtrs dst, unsigned mask);
+int cheb_multi32(const pevsl_devcsr *A, int S, const float *vk, const float *vkm1, float *vkp1,
+                 float *y, const double *mu, int mu_ld, int k, const BatchParams &p);
+int kpm_step32(const pevsl_devcsr *A, int s, int ld, const float *Xk, const float *Xkm1,
+               float *Xkp1, const float *V0, double ctr, double sc, double *mom);
+int cvt_f64_f32(long n, const double *x, float *y);
 
 /* U = V(:, 0:k) Y  (n x m, V column-major ldv, Y k x m column-major ldy) */
 int gemm_nn(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy,

@@ -188,9 +188,10 @@ template <int S>
 __global__ void __launch_bounds__(kThreads)
     k_cheb_multi(int n, const int *__restrict__ ia, const int *__restrict__ ja,
                  const double *__restrict__ a, const double *__restrict__ vk,
-                 const double *__restrict__ vkm1, double *__restrict__ vkp1,
-                 double *__restrict__ y, const double *__restrict__ mu, int mu_ld, int k,
-                 BatchParams p) {
+                 const double *vkm1, double *vkp1, double *__restrict__ y,
+                 const double *__restrict__ mu, int mu_ld, int k, BatchParams p) {
+  /* vkp1 may alias vkm1: each thread reads its v_{k-1} entry before writing
+   * v_{k+1} there */
   const long gt = blockIdx.x * (long)blockDim.x + threadIdx.x;
   const long row = gt / S;
   const int s = (int)(gt & (S - 1));

@@ -68,6 +68,41 @@ int ensure() {
   return 0;
 }
 
+/* Optional L2 residency of the operator (environment variable
+ * PEVSL_B200_L2PERSIST=1): reserve the persisting part of L2 and point the
+ * library stream's access-policy window at the matrix block, so the matrix
+ * stays on chip while the vectors stream through the rest of L2.  The limit
+ * belongs to this process's context and ends with it. */
+void l2_window(const void *base, size_t bytes) {
+  static int enabled = -1;
+  static size_t max_persist = 0, max_window = 0;
+  if (enabled < 0) {
+    const char *e = getenv("PEVSL_B200_L2PERSIST");
+    enabled = e && atoi(e) != 0;
+    if (enabled) {
+      cudaDeviceProp prop;
+      if (cudaGetDeviceProperties(&prop, g_ctx.device) == cudaSuccess) {
+        max_persist = (size_t)prop.persistingL2CacheMaxSize;
+        max_window = (size_t)prop.accessPolicyMaxWindowSize;
+      }
+      if (!max_persist || !max_window) enabled = 0;
+    }
+  }
+  if (!enabled) return;
+  const size_t win = bytes < max_window ? bytes : max_window;
+  const size_t persist = win < max_persist ? win : max_persist;
+  cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, persist);
+  cudaStreamAttrValue attr;
+  memset(&attr, 0, sizeof attr);
+  attr.accessPolicyWindow.base_ptr = const_cast<void *>(base);
+  attr.accessPolicyWindow.num_bytes = win;
+  attr.accessPolicyWindow.hitRatio = (float)((double)persist / (double)win);
+  attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+  attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+  cudaStreamSetAttribute(g_ctx.stream, cudaStreamAttributeAccessPolicyWindow, &attr);
+  cudaGetLastError(); /* the window is a hint: ignore refusals */
+}
+
 int launched(const char *what) {
   g_ctx.launches++;
   return fail(cudaGetLastError(), what);

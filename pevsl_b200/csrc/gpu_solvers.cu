@@ -111,12 +111,13 @@ int cheb_apply(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, d
     return vscal(y, n, mu[0]);
   }
   if (!A && (!pevsl->Amv || !pevsl->Amv->func)) return PEVSL_ERR_NOMATVEC;
-  double *buf[3] = {w3, w3 + n, w3 + 2 * n};
+  double *buf[2] = {w3, w3 + n};
   double *ax = A ? nullptr : (double *)ws(WS_VEC, sizeof(double) * (size_t)n);
   if (!A && !ax) return PEVSL_ERR_NOMEM;
   const double *vk = v, *vkm1 = nullptr;
   for (int k = 1; k <= m; k++) {
-    double *vkp1 = buf[(k - 1) % 3];
+    /* two work vectors: from degree 3 on, v_{k+1} replaces v_{k-1} in place */
+    double *vkp1 = k <= 2 ? buf[k - 1] : const_cast<double *>(vkm1);
     const double t = k == 1 ? t1 : t2;
     int st;
     if (A) {
@@ -179,6 +180,7 @@ void pEVSL_B200_ResetFilterCounters(void) {
  * ChebAv internal. */
 int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y) {
   if (ensure()) return PEVSL_ERR_CUDA;
+  if (pevsl_builtin_A(pevsl)) l2_window(pevsl_builtin_A(pevsl)->a, pevsl_builtin_A(pevsl)->bytes);
   const long n = pevsl->n;
   double *w3 = (double *)ws(WS_CHEB, sizeof(double) * 3 * (size_t)n);
   if (!w3) return PEVSL_ERR_NOMEM;
@@ -826,7 +828,7 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
           r = cheb_apply(pevsl, SL[s].pol, xin ? xin : SL[s].V + (size_t)kin * ld,
                          SL[s].V + (size_t)kout * ld, w3, n);
     } else {
-      double *Z = w3, *Y = w3 + ilv, *buf[3] = {w3 + 2 * ilv, w3 + 3 * ilv, w3 + 4 * ilv};
+      double *Z = w3, *Y = w3 + ilv, *buf[2] = {w3 + 2 * ilv, w3 + 3 * ilv};
       CPtrs src{};
       VPtrs dst{};
       int maxdeg = 0;
@@ -839,7 +841,7 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
       bp.mask = mask;
       const double *vk = Z, *vkm1 = nullptr;
       for (int k = 1; k <= maxdeg && !r; k++) {
-        double *vkp1 = buf[(k - 1) % 3];
+        double *vkp1 = k <= 2 ? buf[k - 1] : const_cast<double *>(vkm1);
         r = cheb_multi(A, Sp, vk, vkm1, vkp1, Y, mu_all, mu_ld, k, bp);
         /* one read of the matrix serves every slice still filtering */
         g_filter_launches++;
@@ -860,6 +862,7 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     t_pol.end();
     return r;
   };
+  if (A) l2_window(A->a, A->bytes);
   cudaEvent_t e_all0, e_all1;
   cudaEventCreate(&e_all0);
   cudaEventCreate(&e_all1);

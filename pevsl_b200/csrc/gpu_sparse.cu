@@ -117,6 +117,7 @@ struct EpiStore {
   __device__ __forceinline__ void operator()(int row, double r) const { y[row] = r; }
 };
 
+/* vkp1 may alias vkm1: the thread of a row reads v_{k-1} there first */
 struct EpiCheb {
   const double *vk, *vkm1;
   double *vkp1, *y;
@@ -467,16 +468,20 @@ int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
     const int L = atoi(lenv);
     if (L == 0 || L == 1 || L == 2 || L == 4 || L == 8 || L == 16 || L == 32) d->lanes = L;
   }
-  d->ia = (int *)alloc_dev(sizeof(int) * (size_t)(nr + 1));
-  d->ja = (int *)alloc_dev(sizeof(int) * (size_t)nnz);
-  d->a = (double *)alloc_dev(sizeof(double) * (size_t)nnz);
-  if (!d->ia || !d->ja || !d->a) {
-    cudaFree(d->ia);
-    cudaFree(d->ja);
-    cudaFree(d->a);
+  /* one allocation [values | column indices | row pointers], 256-byte
+   * aligned parts, so that a single L2 access-policy window can cover it */
+  const size_t bytes_a = ((sizeof(double) * (size_t)nnz + 255) / 256) * 256;
+  const size_t bytes_ja = ((sizeof(int) * (size_t)nnz + 255) / 256) * 256;
+  const size_t bytes_ia = sizeof(int) * (size_t)(nr + 1);
+  char *base = (char *)alloc_dev(bytes_a + bytes_ja + bytes_ia);
+  if (!base) {
     free(d);
     return PEVSL_ERR_NOMEM;
   }
+  d->a = (double *)base;
+  d->ja = (int *)(base + bytes_a);
+  d->ia = (int *)(base + bytes_a + bytes_ja);
+  d->bytes = bytes_a + bytes_ja + bytes_ia;
   int st = memcpy_async(d->ia, Ai->ia, sizeof(int) * (size_t)(nr + 1));
   if (!st) st = memcpy_async(d->ja, Ai->ja, sizeof(int) * (size_t)nnz);
   if (!st) st = memcpy_async(d->a, Ai->a, sizeof(double) * (size_t)nnz);
@@ -499,9 +504,7 @@ void pEVSL_ParcsrFree(pevsl_Parcsr *A) {
   pevsl_devcsr *d = pevsl_devcsr_of(A);
   if (d) {
     cudaStreamSynchronize(ctx().stream);
-    cudaFree(d->ia);
-    cudaFree(d->ja);
-    cudaFree(d->a);
+    cudaFree(d->a); /* the whole [values | indices | pointers] block */
     if (d->a32) cudaFree(d->a32);
     d->magic = 0;
     free(d);

@@ -44,6 +44,7 @@ typedef struct pevsl_devcsr {
   int max_row_nnz;
   double avg_row_nnz;
   int lanes; /* threads per row in the row-group SpMV kernels */
+  size_t bytes; /* size of the one device block holding a, ja, ia */
 } pevsl_devcsr;
 
 /* The device matrix behind a Parcsr, or NULL if it was never set up here. */

@@ -42,8 +42,10 @@ def test_reference_laplacian_driver(gpu, tmp_path):
              re.findall(r"\[Group 0\]: number of eigenvalues: (\d+), found: (\d+)", out)]
     assert found == [(21, 21), (24, 24), (27, 27), (19, 19), (27, 27)], found
     # slices: the reference's run with the same (glibc, srand(0)) stream
+    block = out.split("SLICES FOUND")[1].split("=====\n")[1]
     sl = [tuple(float(x) for x in m) for m in
-          re.findall(r"\s*\d+: \[\s*([-\d.e+]+)\s*,\s*([-\d.e+]+)\]", out)]
+          re.findall(r"\s*\d+: \[\s*([-\d.e+]+)\s*,\s*([-\d.e+]+)\]", block)]
+    assert len(sl) == 5
     g = golden("lap20_kpm.json")["cases"]["glibc"]["sli"]
     assert np.max(np.abs(np.array([s[0] for s in sl] + [sl[-1][1]]) - g)) <= 1e-12 * 1.2
     degs = [int(x) for x in re.findall(r"polynomial \[type \d\] deg (\d+)", out)]
