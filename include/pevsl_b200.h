@@ -73,6 +73,21 @@ int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intv
                               pevsl_Parvecs **Wo, double **reso, int *its, int *status,
                               FILE *fstats);
 
+/* w = V(:, 0:k)' x (the projection of pEVSL_ParvecsGemtv) without any device
+ * allocation; no counterpart in the reference.  For callers that must not
+ * let the library allocate: a framework that owns all device memory through
+ * its own pool, latency-critical loops that cannot take cudaMalloc's device
+ * synchronisation, programs with a fixed memory budget.  V (column major,
+ * n x k, leading dimension ld >= n), x (n) and w (k) are device pointers
+ * owned by the caller; stream is a cudaStream_t or NULL (legacy default
+ * stream).  The only workspace is a fixed 256 KiB array that the library
+ * holds on every GPU it is loaded on, so k is limited to 1..256 (other
+ * values return PEVSL_ERR_ARG).  The first call on a device looks up that
+ * array's device address, so make it before any stream capture.  All calls
+ * on a device share the array: calls that overlap on the GPU race. */
+int pEVSL_B200_ParvecsGemtvNoAlloc(const double *V, long n, long ld, int k, const double *x,
+                                   double *w, void *stream);
+
 /* Release cached device workspaces (they are reused across calls). */
 void pEVSL_B200_ReleaseWorkspace(void);
 
