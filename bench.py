@@ -154,8 +154,9 @@ def ncu_traffic(workload):
     try:
         with open(path) as f:
             d = json.load(f)
-        return d.get(workload)
-    except (OSError, ValueError):
+        e = d.get(workload)
+        return e.get("dram_bytes_per_launch") if e else None
+    except (OSError, ValueError, AttributeError):
         return None
 
 
@@ -284,7 +285,7 @@ def run_b200(args, dist):
         "gpu_launches": int(launches),
         "clocks": clk,
         "roofline": {
-            "kernel": ("cheb_multi (fused SpMV + Chebyshev recurrence, all slices per launch)"
+            "kernel": ("cheb_step_batch (fused SpMV + Chebyshev recurrence, CSR-stream, all slices per launch)"
                        if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream)"),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
@@ -408,12 +409,25 @@ REF_COUNTS = {
 
 
 def kernel_case(args):
-    """A few launches of one kernel on a matrix larger than L2, for ncu:
-    --kernel-case cheb_step runs two degree-8 filter applications (16 fused
-    filter-degree launches) on the 3D Laplacian of side --grid; kpm_step runs
-    8 KPM degrees for 16 vectors."""
+    """A few launches of one kernel on a matrix larger than L2, for ncu, on
+    the 3D Laplacian of side --grid:
+      cheb_step  two degree-8 filter applications (16 fused filter-degree
+                 launches, one vector);
+      cheb_batch --batch slices of [0.80, 0.82] with degree-8 filters in
+                 lockstep, 3 Lanczos steps (32 batched filter-degree
+                 launches);
+      kpm_step   8 KPM degrees for 16 vectors;
+      pipeline   one whole batched solve of --workload (for launch lists)."""
     import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian
+    if args.kernel_case == "pipeline":
+        w = WORKLOADS[args.workload]
+        n, ia, ja, a = laplacian(*w["grid"])
+        M = pv.Matrix.from_csr(n, ia, ja, a)
+        r = pv.solve_interval(M, slice_run(w, 0), batched=True)
+        print(json.dumps({"kernel_case": "pipeline", "workload": args.workload,
+                          "nev": [int(x) for x in r.nev], "status": r.status}))
+        return
     g = args.grid
     n, ia, ja, a = laplacian(g, g, g)
     M = pv.Matrix.from_csr(n, ia, ja, a)
@@ -424,6 +438,13 @@ def kernel_case(args):
             v = np.cos(np.arange(n) * 0.1)
             for _ in range(2):
                 ev.chebav(f, v)
+        elif args.kernel_case == "cheb_batch":
+            S = args.batch
+            edges = np.linspace(0.80, 0.82, S + 1)
+            intvs = [[edges[i], edges[i + 1], 0.0, 12.0] for i in range(S)]
+            fl = [pv.findpol(iv, deg_in=8)[1] for iv in intvs]
+            v = np.cos(np.arange(n) * 0.1)
+            pv.cheblannr_batch(ev, intvs, [3] * S, 1e-8, v, fl)
         else:
             ev.kpmdos(8, 1, 16, [0.80, 0.82, 0.0, 12.0])
     print(json.dumps({"kernel_case": args.kernel_case, "n": n, "nnz": int(ia[-1])}))
@@ -439,9 +460,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--path", default="batched", choices=["batched", "plain"],
                     help="batched: slices in lockstep; plain: one pEVSL_ChebLanNr per slice")
-    ap.add_argument("--kernel-case", choices=["cheb_step", "kpm_step"],
+    ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "pipeline"],
                     help="run a few launches of one kernel (for ncu) and exit")
     ap.add_argument("--grid", type=int, default=128)
+    ap.add_argument("--batch", type=int, default=4)
     args = ap.parse_args()
     if args.kernel_case:
         kernel_case(args)

@@ -29,6 +29,30 @@ extern "C" {
 int pEVSL_B200_SetRng(int mode, uint64_t seed);
 uint64_t pEVSL_B200_RngDraws(void);
 
+/* Arithmetic of the filter and the KPM moments on this instance.
+ *   PEVSL_PREC_FP64 (default): everything in FP64, the drop-in behaviour.
+ *   PEVSL_PREC_MIXED: the Chebyshev filter and the KPM moments run on FP32
+ *     matrix values and FP32 vectors with FP32 accumulation; the Lanczos
+ *     basis, reorthogonalisation, tridiagonal solves and Ritz vectors stay
+ *     FP64.  The Lanczos convergence test allows the FP32 noise of the
+ *     filter (PEVSL_B200_MIXED_TRTOL, default 1e-9 per converged Ritz
+ *     value).  Before acceptance each slice gets one FP64 filtered
+ *     Rayleigh-Ritz sweep: the Ritz vectors of p(A) with values
+ *     >= guard * bar (PEVSL_B200_MIXED_GUARD, default 0.3; the extra ones
+ *     hold the directions just outside the slice), the FP64 filter applied
+ *     to them (PEVSL_B200_MIXED_PASSES times, default 1), Rayleigh-Ritz with
+ *     A on the filtered block; acceptance (interval and residual < tol) is
+ *     decided on the refined FP64 pairs.  A slice where a refined pair in
+ *     [a, b] stays above tol is solved again in FP64, so the counts are
+ *     those of the FP64 path; pEVSL_B200_LastFallbacks reports how many. */
+#define PEVSL_PREC_FP64 0
+#define PEVSL_PREC_MIXED 1
+int pEVSL_B200_SetPrecision(pevsl_Data *pevsl, int precision);
+
+/* Slices of the last pEVSL_ChebLanNr / pEVSL_B200_ChebLanNrBatch call that
+ * the mixed form solved again in FP64. */
+int pEVSL_B200_LastFallbacks(void);
+
 /* Lanczos steps taken by the last pEVSL_ChebLanNr on this instance, and the
  * number of Ritz values of p(A) above `bar` at its last convergence test. */
 int pEVSL_B200_LastIterations(pevsl_Data *pevsl);

@@ -27,6 +27,8 @@ LIB_PATH = os.path.join(HERE, "libpevsl_b200.so")
 
 RNG_GLIBC = 0
 RNG_GAUSS = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
 
 # error codes of include/pevsl.h
 PEVSL_NOT_IMPLEMENT = 11
@@ -162,6 +164,8 @@ SIGNATURES = [
     ("pEVSL_B200_HostFree", None, [_vp]),
     ("pEVSL_B200_FilterCounters", None, [C.POINTER(C.c_uint64), _dp, _dp]),
     ("pEVSL_B200_ResetFilterCounters", None, []),
+    ("pEVSL_B200_SetPrecision", _I, [C.POINTER(PevslData), _I]),
+    ("pEVSL_B200_LastFallbacks", _I, []),
     ("pEVSL_B200_ChebLanNrBatch", _I, [C.POINTER(PevslData), _I, _dp, _ip, _D,
                                        C.POINTER(Parvec), C.POINTER(Polparams), _ip,
                                        C.POINTER(_dp), C.POINTER(C.POINTER(Parvecs)),
@@ -379,6 +383,11 @@ class Instance:
     def n(self) -> int:
         return self.p.contents.n
 
+    def set_precision(self, precision: int) -> None:
+        """PREC_FP64 (default) or PREC_MIXED (FP32 filter and KPM moments,
+        FP64 Lanczos basis / reorthogonalisation / refinement)."""
+        _check(self.lib.pEVSL_B200_SetPrecision(self.p, precision), "SetPrecision")
+
     def close(self):
         if self.p:
             self.lib.pEVSL_Finish(self.p)
@@ -554,9 +563,11 @@ class SliceResult:
     lam: list = field(default_factory=list)
     res: list = field(default_factory=list)
     times: dict = field(default_factory=dict)
+    fallbacks: int = 0            # mixed form: slices solved again in FP64
 
 
-def solve_interval(A: Matrix, s: SliceRun, batched: bool = False) -> SliceResult:
+def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
+                   precision: int = PREC_FP64) -> SliceResult:
     """Run the whole slicing path through the C API, in the reference
     drivers' order: start vector, bounds, DOS, slicer, then each slice
     (one pEVSL_ChebLanNr per slice, or all slices in lockstep through
@@ -568,6 +579,7 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False) -> SliceResult
     with Instance(A) as ev:
         # pEVSL_Start reseeds rand() with srand(0); restart the chosen stream
         set_rng(s.rng_mode, s.seed)
+        ev.set_precision(precision)
         vinit = Vector(A.n)
         lib.pEVSL_ParvecRand(C.byref(vinit.pv))
         times = {}
@@ -616,6 +628,7 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False) -> SliceResult
                 filters.append(f)
                 intvs.append(iv)
             r, outs = cheblannr_batch(ev, intvs, [mlan] * s.nslices, s.tol, vinit, filters)
+            res.fallbacks = int(lib.pEVSL_B200_LastFallbacks())
             for f, out in zip(filters, outs):
                 if out["status"] and not res.status:
                     res.status = 300 + abs(out["status"])
@@ -636,6 +649,7 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False) -> SliceResult
                 res.status = res.status or 300 + abs(r)
                 continue
             out = ev.cheblannr(iv, mlan, s.tol, vinit, f)
+            res.fallbacks += int(lib.pEVSL_B200_LastFallbacks())
             if out["status"] and not res.status:
                 res.status = 300 + abs(out["status"])
             res.deg.append(f.deg)

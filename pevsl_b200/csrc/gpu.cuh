@@ -63,6 +63,11 @@ enum Ws {
   WS_SMALL,     /* small coefficient arrays                   */
   WS_RITZ,      /* Ritz vectors                               */
   WS_RITZ2,     /* A * Ritz vectors                           */
+  WS_REF1,      /* refinement sweep: A P                      */
+  WS_REF2,      /* refinement sweep: refined vectors          */
+  WS_H,         /* refinement sweep: small projected matrices */
+  WS_GEMM,      /* gemm_tn partial tiles                      */
+  WS_FILT,      /* batched filter work vectors                */
   WS_COUNT
 };
 
@@ -165,8 +170,6 @@ int b_scal(long n, int S, VPtrs x, BScal a, unsigned mask);
 int b_dot(long n, int S, CPtrs x, CPtrs y, double *out, int fin, unsigned mask);
 int b_axpy_dev_nrm2(long n, int S, const double *coef, CPtrs x, VPtrs y, double *nrm,
                     unsigned mask);
-int b_gather(long n, int S, CPtrs src, double *Z, unsigned mask);
-int b_scatter(long n, int S, const double *Y, VPtrs dst, unsigned mask);
 /* w[s*ldw + j] = <V_s(:,j), v_s>, j < k */
 int b_gemvT(long n, int S, int k, CPtrs V, long ldv, CPtrs v, double *w, long ldw, const int *run,
             unsigned mask);
@@ -174,21 +177,27 @@ int b_gemvT(long n, int S, int k, CPtrs V, long ldv, CPtrs v, double *w, long ld
 int b_gemv_sub_nrm(long n, int S, int k, CPtrs V, long ldv, const double *w, long ldw, VPtrs v,
                    double *nrm, const int *run, int *flag_out, double *nrm_old, double eta,
                    unsigned mask);
-/* one filter degree k for S (1,2,4,8,16) row-interleaved vectors
- * (X[i*S + s]); mu is S rows of mu_ld coefficients */
-int cheb_multi(const pevsl_devcsr *A, int S, const double *vk, const double *vkm1, double *vkp1,
-               double *y, const double *mu, int mu_ld, int k, const BatchParams &p);
+/* one filter degree (SRC/chebpol.c:538-568) for nb <= kMaxBatch independent
+ * vectors, one matrix read serving all: entry e's pointers are FP64 vectors,
+ * or FP32 ones when fp32 (then the last degree sets yout, the FP64 result) */
+struct ChebEntry {
+  const void *vk, *vkm1; /* vkm1 NULL at the first degree */
+  void *vkp1, *y;        /* vkp1 may alias vkm1 */
+  double *yout;
+  double cc, t, mu0, muk;
+  int first;
+};
+int cheb_step_batch(const pevsl_devcsr *A, int nb, const ChebEntry *e, bool fp32);
 
 /* ---------------------------------------------------------------- FP32 (mixed) */
 int csr_make_fp32(pevsl_devcsr *A); /* FP32 copy of the values, once */
-int b_gather32(long n, int S, CPtrs src, float *Z, unsigned mask);
-int b_scatter32(long n, int S, const float *Y, VPtrs dst, unsigned mask);
-int cheb_multi32(const pevsl_devcsr *A, int S, const float *vk, const float *vkm1, float *vkp1,
-                 float *y, const double *mu, int mu_ld, int k, const BatchParams &p);
 int kpm_step32(const pevsl_devcsr *A, int s, int ld, const float *Xk, const float *Xkm1,
                float *Xkp1, const float *V0, double ctr, double sc, double *mom);
 int cvt_f64_f32(long n, const double *x, float *y);
 
+/* C = V(:, 0:k)' W(:, 0:m)  (k x m, column-major ldc); deterministic */
+int gemm_tn(long n, int k, int m, const double *V, long ldv, const double *W, long ldw, double *C,
+            long ldc);
 /* U = V(:, 0:k) Y  (n x m, V column-major ldv, Y k x m column-major ldy) */
 int gemm_nn(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy,
             double *U, long ldu);

@@ -9,9 +9,8 @@
  *
  *   b_dot / b_axpy_dev_nrm2  dots and norms: SRC/parvec.c:123-142
  *   b_gemvT / b_gemv_sub_nrm one CGS pass of CGS_DGKS: SRC/miscla.c:211-240
- *   cheb_multi               one filter degree of pEVSL_ChebAv
- *                            (SRC/chebpol.c:538-568) for all entries, the
- *                            matrix read once; vectors row-interleaved
+ *
+ * The batched filter degree is cheb_step_batch (gpu_sparse.cu).
  */
 #include <cuda_runtime.h>
 
@@ -73,22 +72,6 @@ __global__ void k_b_axpy_dev_nrm2(long n, const double *coef, CPtrs x, VPtrs y, 
   bool last;
   const double t = grid_sum(acc, partials + (size_t)s * kMaxRedBlocks, counters + s, FIN_SQRT, &last);
   if (last && threadIdx.x == 0) nrm[s] = t;
-}
-
-__global__ void k_b_gather(long n, int S, CPtrs src, double *Z, unsigned mask) {
-  const int s = blockIdx.y;
-  if (!PV_ACTIVE(mask, s)) return;
-  const double *xs = src.p[s];
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    Z[i * S + s] = xs[i];
-}
-
-__global__ void k_b_scatter(long n, int S, const double *Y, VPtrs dst, unsigned mask) {
-  const int s = blockIdx.y;
-  if (!PV_ACTIVE(mask, s)) return;
-  double *ys = dst.p[s];
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    ys[i] = Y[i * S + s];
 }
 
 /* ---------------------------------------------------------------- CGS pass */
@@ -176,53 +159,6 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-/* ---------------------------------------------------------------- filter, batched
- * One degree k of the filter for S (power of two) row-interleaved vectors:
- * S lanes per row, lane s owns entry s.  The lanes of a row read the same
- * column indices / values (one transaction) and gather x[col*S .. col*S+S)
- * as one contiguous segment; each lane sums its products in entry order
- * without fusing (the order and rounding of the CSR-stream kernel, so a
- * batched entry equals the single-vector result bit for bit).  Entries whose
- * filter degree is below k, or that are inactive, do nothing. */
-template <int S>
-__global__ void __launch_bounds__(kThreads)
-    k_cheb_multi(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                 const double *__restrict__ a, const double *__restrict__ vk,
-                 const double *vkm1, double *vkp1, double *__restrict__ y,
-                 const double *__restrict__ mu, int mu_ld, int k, BatchParams p) {
-  /* vkp1 may alias vkm1: each thread reads its v_{k-1} entry before writing
-   * v_{k+1} there */
-  const long gt = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long row = gt / S;
-  const int s = (int)(gt & (S - 1));
-  if (row >= n) return;
-  if (!PV_ACTIVE(p.mask, s) || k > p.deg[s]) return;
-  const int rs = ia[row], re = ia[row + 1];
-  double acc = 0.0;
-  for (int j0 = rs; j0 < re; j0 += 8) {
-    int col[8];
-    double val[8], xv[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const bool ok = j0 + q < re;
-      col[q] = ok ? ja[j0 + q] : 0;
-      val[q] = ok ? a[j0 + q] : 0.0;
-    }
-#pragma unroll
-    for (int q = 0; q < 8; q++) xv[q] = j0 + q < re ? __ldg(vk + (size_t)col[q] * S + s) : 0.0;
-#pragma unroll
-    for (int q = 0; q < 8; q++)
-      if (j0 + q < re) acc = __dadd_rn(acc, __dmul_rn(val[q], xv[q]));
-  }
-  const size_t idx = (size_t)row * S + s;
-  const double t = k == 1 ? p.t1[s] : p.t2[s];
-  double w;
-  double yv = k == 1 ? 0.0 : y[idx];
-  cheb_update(acc, vk[idx], k == 1 ? nullptr : vkm1 + idx, p.cc[s], t, mu[(size_t)s * mu_ld],
-              mu[(size_t)s * mu_ld + k], k == 1, &w, &yv);
-  vkp1[idx] = w;
-  y[idx] = yv;
-}
 
 /* ---------------------------------------------------------------- host wrappers */
 
@@ -258,20 +194,6 @@ int b_axpy_dev_nrm2(long n, int S, const double *coef, CPtrs x, VPtrs y, double 
   return launched("b_axpy_dev_nrm2");
 }
 
-int b_gather(long n, int S, CPtrs src, double *Z, unsigned mask) {
-  if (n <= 0 || !mask) return 0;
-  dim3 g(col_grid(n, 4), S);
-  k_b_gather<<<g, kThreads, 0, ctx().stream>>>(n, S, src, Z, mask);
-  return launched("b_gather");
-}
-
-int b_scatter(long n, int S, const double *Y, VPtrs dst, unsigned mask) {
-  if (n <= 0 || !mask) return 0;
-  dim3 g(col_grid(n, 4), S);
-  k_b_scatter<<<g, kThreads, 0, ctx().stream>>>(n, S, Y, dst, mask);
-  return launched("b_scatter");
-}
-
 int b_gemvT(long n, int S, int k, CPtrs V, long ldv, CPtrs v, double *w, long ldw, const int *run,
             unsigned mask) {
   if (k <= 0 || !mask) return 0;
@@ -304,22 +226,6 @@ int b_gemv_sub_nrm(long n, int S, int k, CPtrs V, long ldv, const double *w, lon
   k_b_gemv_sub_nrm<<<g, kThreads, sh, ctx().stream>>>(n, k, V, ldv, w, ldw, v, ctx().red, ctx().cnt,
                                                       nrm, run, flag_out, nrm_old, eta, mask);
   return launched("b_gemv_sub_nrm");
-}
-
-int cheb_multi(const pevsl_devcsr *A, int S, const double *vk, const double *vkm1, double *vkp1,
-               double *y, const double *mu, int mu_ld, int k, const BatchParams &p) {
-  if (A->nrows <= 0 || !p.mask) return 0;
-  const long rows_per_block = kThreads / S;
-  const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
-  switch (S) {
-    case 1: k_cheb_multi<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 2: k_cheb_multi<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 4: k_cheb_multi<4><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 8: k_cheb_multi<8><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 16: k_cheb_multi<16><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    default: return PEVSL_ERR_ARG;
-  }
-  return launched("cheb_multi");
 }
 
 /* ---------------------------------------------------------------- single-vector forms */

@@ -70,6 +70,17 @@ __device__ __forceinline__ void cheb_update(double r, double x, const double *xm
   *y = first ? __fma_rn(muk, w, __dmul_rn(mu0, x)) : __fma_rn(muk, w, *y);
 }
 
+/* cheb_update on values already loaded (xm1 used only when has_m1) */
+__device__ __forceinline__ void cheb_update_v(double r, double x, double xm1, bool has_m1,
+                                              double cc, double t, double mu0, double muk,
+                                              bool first, double yold, double *w_out,
+                                              double *y) {
+  double w = __dmul_rn(__fma_rn(-cc, x, r), t);
+  if (has_m1) w = __dsub_rn(w, xm1);
+  *w_out = w;
+  *y = first ? __fma_rn(muk, w, __dmul_rn(mu0, x)) : __fma_rn(muk, w, yold);
+}
+
 }  // namespace pv
 
 #endif

@@ -4,12 +4,10 @@
  * halving the bytes per degree; the Lanczos basis, reorthogonalisation,
  * tridiagonal solves, Ritz vectors and residuals stay FP64 (gpu_solvers.cu).
  *
- *   cheb_multi32   one filter degree (SRC/chebpol.c:538-568) for S
- *                  row-interleaved FP32 vectors, the matrix read once
  *   kpm_step32     one KPM degree (SRC/kpmdos.c:129-156) for s <= 64
  *                  row-interleaved FP32 vectors with the moment dots fused
- *   b_gather32 /   FP64 basis columns <-> FP32 interleaved block
- *   b_scatter32
+ *
+ * The FP32 filter degree is the fp32 form of cheb_step_batch (gpu_sparse.cu).
  */
 #include <cuda_runtime.h>
 
@@ -35,93 +33,6 @@ int csr_make_fp32(pevsl_devcsr *A) {
   }
   A->a32 = p;
   return 0;
-}
-
-__global__ void k_b_gather32(long n, int S, CPtrs src, float *Z, unsigned mask) {
-  const int s = blockIdx.y;
-  if (!((mask >> s) & 1u)) return;
-  const double *xs = src.p[s];
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    Z[i * S + s] = (float)xs[i];
-}
-
-__global__ void k_b_scatter32(long n, int S, const float *Y, VPtrs dst, unsigned mask) {
-  const int s = blockIdx.y;
-  if (!((mask >> s) & 1u)) return;
-  double *ys = dst.p[s];
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
-    ys[i] = (double)Y[i * S + s];
-}
-
-int b_gather32(long n, int S, CPtrs src, float *Z, unsigned mask) {
-  if (n <= 0 || !mask) return 0;
-  dim3 g(grid_for(n, 4), S);
-  k_b_gather32<<<g, kThreads, 0, ctx().stream>>>(n, S, src, Z, mask);
-  return launched("b_gather32");
-}
-
-int b_scatter32(long n, int S, const float *Y, VPtrs dst, unsigned mask) {
-  if (n <= 0 || !mask) return 0;
-  dim3 g(grid_for(n, 4), S);
-  k_b_scatter32<<<g, kThreads, 0, ctx().stream>>>(n, S, Y, dst, mask);
-  return launched("b_scatter32");
-}
-
-/* FP32 filter degree for S row-interleaved vectors: S lanes per row, lane s
- * owns vector s; FP32 products, FP32 sums. */
-template <int S>
-__global__ void __launch_bounds__(kThreads)
-    k_cheb_multi32(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                   const float *__restrict__ a, const float *__restrict__ vk,
-                   const float *vkm1, float *vkp1, float *__restrict__ y,
-                   const double *__restrict__ mu, int mu_ld, int k, BatchParams p) {
-  /* vkp1 may alias vkm1 (read before written by the same thread) */
-  const long gt = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  const long row = gt / S;
-  const int s = (int)(gt & (S - 1));
-  if (row >= n) return;
-  if (!((p.mask >> s) & 1u) || k > p.deg[s]) return;
-  const int rs = ia[row], re = ia[row + 1];
-  float acc = 0.f;
-  for (int j0 = rs; j0 < re; j0 += 8) {
-    int col[8];
-    float val[8], xv[8];
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-      const bool ok = j0 + q < re;
-      col[q] = ok ? ja[j0 + q] : 0;
-      val[q] = ok ? a[j0 + q] : 0.f;
-    }
-#pragma unroll
-    for (int q = 0; q < 8; q++) xv[q] = j0 + q < re ? __ldg(vk + (size_t)col[q] * S + s) : 0.f;
-#pragma unroll
-    for (int q = 0; q < 8; q++) acc = fmaf(val[q], xv[q], acc);
-  }
-  const size_t idx = (size_t)row * S + s;
-  const float t = (float)(k == 1 ? p.t1[s] : p.t2[s]);
-  const float x = vk[idx];
-  float w = (acc - (float)p.cc[s] * x) * t;
-  if (k > 1) w -= vkm1[idx];
-  vkp1[idx] = w;
-  const float muk = (float)mu[(size_t)s * mu_ld + k];
-  y[idx] = k == 1 ? fmaf(muk, w, (float)mu[(size_t)s * mu_ld] * x) : fmaf(muk, w, y[idx]);
-}
-
-int cheb_multi32(const pevsl_devcsr *A, int S, const float *vk, const float *vkm1, float *vkp1,
-                 float *y, const double *mu, int mu_ld, int k, const BatchParams &p) {
-  if (A->nrows <= 0 || !p.mask) return 0;
-  if (!A->a32) return PEVSL_ERR_ARG;
-  const long rows_per_block = kThreads / S;
-  const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
-  switch (S) {
-    case 1: k_cheb_multi32<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a32, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 2: k_cheb_multi32<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a32, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 4: k_cheb_multi32<4><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a32, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 8: k_cheb_multi32<8><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a32, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    case 16: k_cheb_multi32<16><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a32, vk, vkm1, vkp1, y, mu, mu_ld, k, p); break;
-    default: return PEVSL_ERR_ARG;
-  }
-  return launched("cheb_multi32");
 }
 
 /* FP32 KPM degree for s <= 32*CPL interleaved vectors (warp per row); the

@@ -137,6 +137,81 @@ int cheb_apply(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, d
   return 0;
 }
 
+/* y_e = p_e(A) x_e for ne <= kMaxBatch entries on the device CSR
+ * (pEVSL_ChebAv, SRC/chebpol.c:509-574, for all entries at once): one
+ * cheb_step_batch launch per degree serves every entry whose filter degree
+ * has not been reached, so the matrix is read once per degree.  work holds
+ * 16 n bytes per entry: two FP64 recurrence vectors, or, when fp32, the
+ * FP32 copy of x_e, two FP32 recurrence vectors and the FP32 accumulator
+ * (the last degree writes y_e in FP64).  In FP64 every entry gets the bits
+ * of cheb_apply. */
+struct FilterJob {
+  const double *x;
+  double *y;
+  const pevsl_Polparams *pol;
+};
+
+static int cheb_filter_batch(pevsl_Data *pevsl, const pevsl_devcsr *A, int ne,
+                             const FilterJob *jobs, void *work, bool fp32) {
+  const long n = A->nrows;
+  if (ne <= 0) return 0;
+  if (ne > kMaxBatch) return PEVSL_ERR_ARG;
+  if (fp32 && !A->a32) return PEVSL_ERR_ARG;
+  const void *vk[kMaxBatch], *vkm1[kMaxBatch];
+  void *buf[kMaxBatch][2], *acc[kMaxBatch];
+  int maxdeg = 0, st = 0;
+  for (int e = 0; e < ne && !st; e++) {
+    const pevsl_Polparams *pol = jobs[e].pol;
+    pevsl->stats->n_polAv++;
+    pevsl->stats->n_mvA += (size_t)PEVSL_MAX(pol->deg, 0);
+    if (pol->deg <= 0) {
+      st = vcopy(jobs[e].x, jobs[e].y, n);
+      if (!st) st = vscal(jobs[e].y, n, pol->mu[0]);
+      continue;
+    }
+    maxdeg = PEVSL_MAX(maxdeg, pol->deg);
+    if (fp32) {
+      float *w = (float *)work + 4 * (size_t)n * e;
+      st = cvt_f64_f32(n, jobs[e].x, w);
+      vk[e] = w;
+      buf[e][0] = w + n;
+      buf[e][1] = w + 2 * n;
+      acc[e] = w + 3 * n;
+    } else {
+      double *w = (double *)work + 2 * (size_t)n * e;
+      vk[e] = jobs[e].x;
+      buf[e][0] = w;
+      buf[e][1] = w + n;
+      acc[e] = jobs[e].y;
+    }
+    vkm1[e] = nullptr;
+  }
+  const double mat_bytes = (fp32 ? 8.0 : 12.0) * (double)A->nnz + 4.0 * (n + 1.0);
+  const double vb = fp32 ? 4.0 : 8.0;
+  for (int k = 1; k <= maxdeg && !st; k++) {
+    ChebEntry en[kMaxBatch];
+    int nb = 0;
+    double bytes = mat_bytes;
+    for (int e = 0; e < ne; e++) {
+      const pevsl_Polparams *pol = jobs[e].pol;
+      if (k > pol->deg) continue;
+      /* two work vectors: from degree 3 on, v_{k+1} replaces v_{k-1} */
+      void *vkp1 = k <= 2 ? buf[e][k - 1] : const_cast<void *>(vkm1[e]);
+      const bool last = fp32 && k == pol->deg;
+      en[nb++] = ChebEntry{vk[e], vkm1[e], vkp1, acc[e], last ? jobs[e].y : nullptr,
+                           pol->cc, (k == 1 ? 1.0 : 2.0) / pol->dd, pol->mu[0], pol->mu[k],
+                           k == 1};
+      bytes += (k == 1 ? 3.0 : 5.0) * vb * (double)n + (last ? 4.0 * (double)n : 0.0);
+      vkm1[e] = vk[e];
+      vk[e] = vkp1;
+    }
+    st = cheb_step_batch(A, nb, en, fp32);
+    g_filter_launches++;
+    g_filter_bytes += bytes;
+  }
+  return st;
+}
+
 /* One CGS_DGKS (SRC/miscla.c:211-240) of v against V(:, 0:k).  On entry the
  * device slot S_NRM0 holds ||v||; on exit S_NRM holds the final norm.  The
  * second pass runs only if the first kept at most 1/sqrt(2) of the norm,
@@ -220,7 +295,53 @@ int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *int
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, ctx().stream);
-  if (A) {
+  const bool mixed = A && pevsl_inst_of(pevsl)->precision == PEVSL_PREC_MIXED;
+  if (mixed) st = csr_make_fp32(A);
+  if (A && mixed && !st) {
+    /* FP32 moments: blocks of up to 64 vectors drawn and normalised in FP64,
+     * then rounded to FP32; FP32 recurrence and dots, one launch per degree */
+    const int smax = 64;
+    for (int m0 = vec_start; m0 < vec_end && !st; m0 += smax) {
+      const int s = vec_end - m0 < smax ? vec_end - m0 : smax;
+      const int ld = s;
+      const size_t blk = (size_t)n * (size_t)ld;
+      double *X = (double *)ws(WS_KPM, sizeof(double) * 4 * blk);
+      double *mom = (double *)ws(WS_MOM, sizeof(double) * (size_t)(Mdeg + 1) * (size_t)s);
+      double *nrm2 = (double *)ws(WS_SMALL, sizeof(double) * 64);
+      double *hmom = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1) * (size_t)s);
+      if (!X || !mom || !nrm2 || !hmom) {
+        free(hmom);
+        st = PEVSL_ERR_NOMEM;
+        break;
+      }
+      double *V0d = X;
+      float *V0 = (float *)(X + blk), *B[3] = {V0 + blk, V0 + 2 * blk, V0 + 3 * blk};
+      st = pevsl_rand_block_dev(V0d, (int)n, s, ld);
+      if (!st) st = block_colnorm2(n, s, ld, V0d, nrm2);
+      if (!st) st = block_normalize(n, s, ld, V0d, nrm2);
+      if (!st) st = cvt_f64_f32((long)blk, V0d, V0);
+      for (int k = 0; k < Mdeg && !st; k++) {
+        const double sc = (k == 0 ? 1.0 : 2.0) / wid;
+        const float *Xk = k == 0 ? V0 : B[(k - 1) % 3];
+        const float *Xkm1 = k == 0 ? nullptr : (k == 1 ? V0 : B[(k - 2) % 3]);
+        st = kpm_step32(A, s, ld, Xk, Xkm1, B[k % 3], V0, ctr, sc, mom + (size_t)k * s);
+      }
+      if (!st) st = memcpy_async(hmom, mom, sizeof(double) * (size_t)Mdeg * (size_t)s);
+      if (!st) st = sync();
+      pevsl->stats->n_mvA += (size_t)Mdeg * (size_t)s;
+      for (int c = 0; c < s && !st; c++) {
+        mu[0] += jac[0];
+        tcnt -= jac[0] * (beta2 - beta1);
+        for (int k = 0; k < Mdeg; k++) {
+          const int k1 = k + 1;
+          const double t = hmom[(size_t)k * s + c] * 2.0 * jac[k1];
+          mu[k1] += t;
+          tcnt -= t * (sin(k1 * beta2) - sin(k1 * beta1)) / k1;
+        }
+      }
+      free(hmom);
+    }
+  } else if (A && !st) {
     /* blocks of up to 64 vectors, row-interleaved; one launch per degree */
     const int smax = 64;
     for (int m0 = vec_start; m0 < vec_end && !st; m0 += smax) {
@@ -262,7 +383,7 @@ int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *int
       }
       free(hmom);
     }
-  } else {
+  } else if (!st) {
     /* user matvec: one vector at a time, as the reference */
     double *buf = (double *)ws(WS_KPM, sizeof(double) * 4 * (size_t)n);
     double *hdot = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1));
@@ -648,15 +769,10 @@ struct SliceState {
   int active, done;
   /* outputs */
   int status, nev, its;
+  int short_pairs; /* mixed form: refined pairs in [a, b] above tol */
   double *Lam, *res;
   pevsl_Parvecs *Rvec;
 };
-
-static int next_pow2(int s) {
-  int p = 1;
-  while (p < s) p <<= 1;
-  return p;
-}
 
 /* Ritz pairs of one finished slice (SRC/cheblanNr.c:339-413): eigenvectors
  * of T only for Ritz values >= bar, U = V Y, normalise, W = A U, Rayleigh
@@ -664,24 +780,36 @@ static int next_pow2(int s) {
 static int ritz_extract(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, long n, long ld,
                         double tol) {
   Ctx &c = ctx();
-  const int kdim = S->kdim, nconv = S->nconv, count = S->count;
+  const int kdim = S->kdim, count = S->count;
   const double bar = S->pol->bar, aa = S->intv[0], bb = S->intv[1];
-  S->Lam = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
-  S->res = (double *)malloc(sizeof(double) * (size_t)(nconv > 0 ? nconv : 1));
-  S->Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
-  if (!S->Lam || !S->res || !S->Rvec) return PEVSL_ERR_NOMEM;
-  pEVSL_ParvecsDuplParvec(vinit, nconv, (int)n, S->Rvec);
-  if (nconv > 0 && !S->Rvec->data) return PEVSL_ERR_NOMEM;
   S->nev = 0;
-  if (kdim <= 0) return 0;
   int st = 0, nsel = 0;
   const double te = pevsl_now();
-  /* eigenvalues again: the last convergence test may predate the last step */
-  if (pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) return PEVSL_ERR_EIG;
-  int *sel = (int *)malloc(sizeof(int) * (size_t)kdim);
+  /* eigenvalues again: the last convergence test may predate the last step
+   * (a maxit exit), so more Ritz values than nconv may pass the bar test;
+   * the outputs hold max(nconv, nsel) pairs */
+  if (kdim > 0 && pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) return PEVSL_ERR_EIG;
+  int *sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
   if (!sel) return PEVSL_ERR_NOMEM;
-  for (int i = 0; i < count; i++)
+  for (int i = 0; i < count && kdim > 0; i++)
     if (S->EvalT[i] >= bar) sel[nsel++] = i;
+  const int nout = PEVSL_MAX(S->nconv, nsel);
+  S->Lam = (double *)malloc(sizeof(double) * (size_t)(nout > 0 ? nout : 1));
+  S->res = (double *)malloc(sizeof(double) * (size_t)(nout > 0 ? nout : 1));
+  S->Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
+  if (!S->Lam || !S->res || !S->Rvec) {
+    free(sel);
+    return PEVSL_ERR_NOMEM;
+  }
+  pEVSL_ParvecsDuplParvec(vinit, nout, (int)n, S->Rvec);
+  if (nout > 0 && !S->Rvec->data) {
+    free(sel);
+    return PEVSL_ERR_NOMEM;
+  }
+  if (kdim <= 0) {
+    free(sel);
+    return 0;
+  }
   double *Y = nullptr;
   if (nsel > 0) {
     Y = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)nsel);
@@ -736,6 +864,160 @@ static int ritz_extract(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, l
   return st;
 }
 
+/* Ritz pairs of a slice whose Krylov basis came from the FP32 filter: one
+ * FP64 filtered Rayleigh-Ritz sweep.  The FP32 recurrence leaves noise of
+ * about 1e-6 relative in every direction of the basis, which Rayleigh-Ritz
+ * on the basis alone cannot remove; one FP64 application of p(A) damps each
+ * direction by p(lam_out)/p(lam_in), which is small except just outside the
+ * slice, so those near-edge directions are taken into the subspace instead:
+ * U = V Y for the Ritz values of p(A) >= guard * bar (guard < 1; the
+ * reference keeps those >= bar, SRC/cheblanNr.c:350-365), P = p(A) U in
+ * FP64 with unit columns, G = P'P, H = P'AP (gemm_tn), the pencil (H, G)
+ * on the host (Cholesky dropping dependent columns), X = P Z, and the
+ * reference's acceptance on the refined pairs (SRC/cheblanNr.c:366-405):
+ * lam in [a, b] and ||A x - lam x|| < tol. */
+static int ritz_refine(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, long n, long ld,
+                       double tol, double guard, int passes) {
+  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
+  const int kdim = S->kdim, count = S->count;
+  const double bar = S->pol->bar, aa = S->intv[0], bb = S->intv[1];
+  S->nev = 0;
+  int m = 0, st = 0;
+  int *sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
+  if (!sel) return PEVSL_ERR_NOMEM;
+  if (kdim > 0 && pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) st = PEVSL_ERR_EIG;
+  for (int i = 0; i < count && kdim > 0 && !st; i++)
+    if (S->EvalT[i] >= guard * bar) sel[m++] = i;
+  S->Lam = (double *)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
+  S->res = (double *)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
+  S->Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
+  if (!S->Lam || !S->res || !S->Rvec) st = PEVSL_ERR_NOMEM;
+  if (st || m == 0) {
+    if (S->Rvec) pEVSL_ParvecsDuplParvec(vinit, 0, (int)n, S->Rvec);
+    free(sel);
+    return st;
+  }
+  const size_t mm = (size_t)m * m;
+  double *Y = (double *)malloc(sizeof(double) * (size_t)kdim * m);
+  double *Hh = (double *)malloc(sizeof(double) * 2 * mm);
+  double *Zh = (double *)malloc(sizeof(double) * mm);
+  double *lam = (double *)malloc(sizeof(double) * (size_t)m);
+  double *hv = (double *)malloc(sizeof(double) * (size_t)m);
+  double *U = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * m);
+  double *P = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)ld * m);
+  double *W = (double *)ws(WS_REF1, sizeof(double) * (size_t)ld * m);
+  double *X = (double *)ws(WS_REF2, sizeof(double) * (size_t)ld * m);
+  void *fwork = ws(WS_FILT, 16 * (size_t)n * kMaxBatch);
+  /* small device matrices: Y | G | H | Z | 3 m scalars */
+  double *dsm = (double *)ws(WS_H, sizeof(double) * ((size_t)kdim * m + 3 * mm + 3 * (size_t)m));
+  if (!Y || !Hh || !Zh || !lam || !hv || !U || !P || !W || !X || !fwork || !dsm)
+    st = PEVSL_ERR_NOMEM;
+  double *dY = dsm, *dG = dY + (size_t)kdim * m, *dH = dG + mm, *dZ = dH + mm, *dv = dZ + mm;
+  if (!st && pevsl_tridiag_eig_sel(kdim, S->dT, S->eT, S->EvalT, m, sel, Y)) st = PEVSL_ERR_EIG;
+  /* largest Ritz values first: the Cholesky of G then keeps the wanted
+   * directions and drops guard columns that became dependent on them */
+  for (int j = 0; j < m / 2 && !st; j++) {
+    double *c1 = Y + (size_t)j * kdim, *c2 = Y + (size_t)(m - 1 - j) * kdim;
+    for (int i = 0; i < kdim; i++) {
+      const double t = c1[i];
+      c1[i] = c2[i];
+      c2[i] = t;
+    }
+  }
+  /* U = V Y; P = p(A) U in FP64, unit columns */
+  if (!st) st = memcpy_async(dY, Y, sizeof(double) * (size_t)kdim * m);
+  if (!st) st = gemm_nn(n, kdim, m, S->V, ld, dY, kdim, U, ld);
+  for (int pass = 0; pass < passes && !st; pass++) {
+    double *src = pass % 2 == 0 ? U : P, *dst = pass % 2 == 0 ? P : U;
+    for (int c0 = 0; c0 < m && !st; c0 += kMaxBatch) {
+      const int cs = PEVSL_MIN(kMaxBatch, m - c0);
+      FilterJob jobs[kMaxBatch];
+      for (int e = 0; e < cs; e++)
+        jobs[e] = FilterJob{src + (size_t)(c0 + e) * ld, dst + (size_t)(c0 + e) * ld, S->pol};
+      st = cheb_filter_batch(pevsl, A, cs, jobs, fwork, false);
+    }
+    if (!st) st = vdot_cols(n, m, dst, ld, dst, ld, dv);
+    if (!st) st = memcpy_async(hv, dv, sizeof(double) * m);
+    if (!st) st = sync();
+    for (int j = 0; j < m && !st; j++) hv[j] = hv[j] > 0 ? 1.0 / sqrt(hv[j]) : 0.0;
+    if (!st) st = memcpy_async(dv, hv, sizeof(double) * m);
+    if (!st) st = vscal_cols(n, m, dst, ld, dv);
+  }
+  if (!st && passes % 2 == 0) st = vcopy(U, P, (long)ld * m); /* filtered block in P */
+  /* W = A P; G = P'P, H = P'W */
+  for (int j = 0; j < m && !st; j++) st = spmv(A, P + (size_t)j * ld, W + (size_t)j * ld);
+  pevsl->stats->n_mvA += (size_t)m;
+  if (!st) st = gemm_tn(n, m, m, P, ld, P, ld, dG, m);
+  if (!st) st = gemm_tn(n, m, m, P, ld, W, ld, dH, m);
+  if (!st) st = memcpy_async(Hh, dG, sizeof(double) * 2 * mm);
+  if (!st) st = sync();
+  int q = 0;
+  if (!st) {
+    double *G = Hh, *H = Hh + mm;
+    for (int i = 0; i < m; i++)
+      for (int j = 0; j < i; j++) {
+        const double g = 0.5 * (G[(size_t)j * m + i] + G[(size_t)i * m + j]);
+        const double h = 0.5 * (H[(size_t)j * m + i] + H[(size_t)i * m + j]);
+        G[(size_t)j * m + i] = G[(size_t)i * m + j] = g;
+        H[(size_t)j * m + i] = H[(size_t)i * m + j] = h;
+      }
+    const double te = pevsl_now();
+    st = pevsl_gen_symeig_range(m, H, G, m, aa - DBL_EPSILON, bb + DBL_EPSILON, &q, lam, Zh, m);
+    pevsl->stats->t_eig += pevsl_now() - te;
+  }
+  pEVSL_ParvecsDuplParvec(vinit, q, (int)n, S->Rvec);
+  if (!st && q > 0) {
+    /* X = P Z, A X = W Z (into U), unit columns, R = A X - lam X */
+    st = memcpy_async(dZ, Zh, sizeof(double) * (size_t)m * q);
+    if (!st) st = gemm_nn(n, m, q, P, ld, dZ, m, X, ld);
+    if (!st) st = gemm_nn(n, m, q, W, ld, dZ, m, U, ld);
+    if (!st) st = vdot_cols(n, q, X, ld, X, ld, dv);
+    if (!st) st = memcpy_async(hv, dv, sizeof(double) * q);
+    if (!st) st = sync();
+    for (int j = 0; j < q && !st; j++) hv[j] = hv[j] > 0 ? 1.0 / sqrt(hv[j]) : 0.0;
+    if (!st) st = memcpy_async(dv, hv, sizeof(double) * q);
+    if (!st) st = vscal_cols(n, q, X, ld, dv);
+    if (!st) st = vscal_cols(n, q, U, ld, dv);
+    if (!st) st = memcpy_async(dv + m, lam, sizeof(double) * q);
+    if (!st) st = vaxpy_cols(n, q, dv + m, X, ld, U, ld);
+    if (!st) st = vdot_cols(n, q, U, ld, U, ld, dv + 2 * m);
+    if (!st) st = memcpy_async(hv, dv + 2 * m, sizeof(double) * q);
+    if (!st) st = sync();
+    double rmin = HUGE_VAL, rmax = 0.0;
+    for (int j = 0; j < q && !st; j++) {
+      const double r0 = sqrt(hv[j]);
+      rmin = PEVSL_MIN(rmin, r0);
+      rmax = PEVSL_MAX(rmax, r0);
+      if (r0 < tol) {
+        S->Lam[S->nev] = lam[j];
+        S->res[S->nev] = r0;
+        st = vcopy(X + (size_t)j * ld, S->Rvec->data + (size_t)S->nev * S->Rvec->ld, n);
+        S->nev++;
+      }
+    }
+    if (!st) st = sync();
+    /* a refined pair in [a, b] short of the FP64 path's quality (residual
+     * below tol, and below tol * |lam| for |lam| < 1) sends the slice back
+     * to FP64 */
+    S->short_pairs = 0;
+    for (int j = 0; j < q; j++)
+      if (!(sqrt(hv[j]) < tol * PEVSL_MIN(1.0, fabs(lam[j])))) S->short_pairs++;
+    if (getenv("PEVSL_B200_VERBOSE"))
+      fprintf(stderr, "refine [%g, %g]: kdim %d, subspace %d, in [a,b] %d, accepted %d, res %.2e..%.2e\n",
+              aa, bb, kdim, m, q, S->nev, rmin, rmax);
+  } else if (getenv("PEVSL_B200_VERBOSE")) {
+    fprintf(stderr, "refine [%g, %g]: kdim %d, subspace %d, in [a,b] %d, status %d\n", aa, bb, kdim,
+            m, q, st);
+  }
+  free(sel);
+  free(Y);
+  free(Hh);
+  free(Zh);
+  free(lam);
+  free(hv);
+  return st;
+}
+
 static void free_slice_outputs(SliceState *S) {
   free(S->Lam);
   free(S->res);
@@ -748,17 +1030,27 @@ static void free_slice_outputs(SliceState *S) {
 }
 
 /* Lockstep filtered Lanczos over ns <= kMaxBatch slices sharing vinit. */
+static int g_fallbacks = 0; /* slices of the last call re-run in FP64 */
+
+int pEVSL_B200_LastFallbacks(void) { return g_fallbacks; }
+
 static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol,
-                           pevsl_Parvec *vinit, FILE *fstats) {
+                           pevsl_Parvec *vinit, FILE *fstats, bool allow_mixed = true) {
   Ctx &c = ctx();
   const int N = pevsl->N;
   const long n = pevsl->n, ld = round_ld(n);
   pevsl_devcsr *A = pevsl_builtin_A(pevsl);
-  const int Sp = next_pow2(ns);
-  const bool interleaved = A && Sp > 1;
+  const bool mixed = allow_mixed && A && pevsl_inst_of(pevsl)->precision == PEVSL_PREC_MIXED;
+  const bool batched = A && (ns > 1 || mixed);
+  /* mixed form: trace tolerance per converged value, and the guard of the
+   * refinement sweep (PEVSL_B200_MIXED_TRTOL / PEVSL_B200_MIXED_GUARD) */
+  double trtol_mixed = 1e-9, guard = 0.3;
+  int passes = 1;
+  if (getenv("PEVSL_B200_MIXED_TRTOL")) trtol_mixed = atof(getenv("PEVSL_B200_MIXED_TRTOL"));
+  if (getenv("PEVSL_B200_MIXED_GUARD")) guard = atof(getenv("PEVSL_B200_MIXED_GUARD"));
+  if (getenv("PEVSL_B200_MIXED_PASSES")) passes = PEVSL_MAX(1, atoi(getenv("PEVSL_B200_MIXED_PASSES")));
   unsigned act = 0;
   size_t basis_cols = 0;
-  int mu_ld = 1;
   for (int s = 0; s < ns; s++) {
     SliceState *S = &SL[s];
     S->maxit = PEVSL_MIN(N, S->maxit);
@@ -783,19 +1075,20 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
     act |= 1u << s;
     basis_cols += (size_t)S->maxit + 1;
-    mu_ld = PEVSL_MAX(mu_ld, S->pol->deg + 1);
   }
   if (!act) return 0;
   /* bases of all active slices in one workspace */
   double *Vall = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * basis_cols);
-  const size_t ilv = (size_t)n * (size_t)Sp; /* one interleaved block */
-  double *w3 = (double *)ws(WS_CHEB, sizeof(double) * (interleaved ? 5 * ilv : 3 * (size_t)n));
+  /* three FP64 vectors (single-slice filter, breakdown restarts), then the
+   * batched filter's 16 n bytes per slice */
+  const size_t w3_bytes = sizeof(double) * 3 * (size_t)n + (batched ? 16 * (size_t)n * ns : 0);
+  double *w3 = (double *)ws(WS_CHEB, w3_bytes);
+  if (mixed && csr_make_fp32(A)) return PEVSL_ERR_NOMEM;
   double *vrand = (double *)ws(A ? WS_VEC : WS_RITZ2, sizeof(double) * (size_t)n);
-  double *mu_all = interleaved ? (double *)ws(WS_MOM, sizeof(double) * (size_t)Sp * mu_ld) : nullptr;
-  if (!Vall || !w3 || !vrand || (interleaved && !mu_all)) return PEVSL_ERR_NOMEM;
+  if (!Vall || !w3 || !vrand) return PEVSL_ERR_NOMEM;
+  void *bwork = w3 + 3 * (size_t)n;
   int st = 0;
   size_t off = 0;
-  BatchParams bp{};
   for (int s = 0; s < ns; s++) {
     SliceState *S = &SL[s];
     if (!((act >> s) & 1u)) continue;
@@ -807,14 +1100,6 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     if (!S->dT || !S->eT || !S->EvalT) return PEVSL_ERR_NOMEM;
     S->wn = S->tr0 = S->beta = 0.0;
     S->nwn = S->kdim = S->count = S->nconv = 0;
-    if (interleaved) {
-      st = memcpy_async(mu_all + (size_t)s * mu_ld, S->pol->mu, sizeof(double) * (S->pol->deg + 1));
-      bp.deg[s] = S->pol->deg;
-      bp.cc[s] = S->pol->cc;
-      bp.t1[s] = 1.0 / S->pol->dd;
-      bp.t2[s] = 2.0 / S->pol->dd;
-      if (st) return st;
-    }
   }
   SegTimer &t_pol = g_t_pol, &t_orth = g_t_orth;
   /* y_s = p_s(A) x_s for the slices in mask: x_s = V_s(:,k) (or xin for
@@ -822,42 +1107,20 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
   auto filter = [&](unsigned mask, int kin, const double *xin, int kout) -> int {
     t_pol.begin();
     int r = 0;
-    if (!interleaved) {
+    if (!batched) {
       for (int s = 0; s < ns && !r; s++)
         if ((mask >> s) & 1u)
           r = cheb_apply(pevsl, SL[s].pol, xin ? xin : SL[s].V + (size_t)kin * ld,
                          SL[s].V + (size_t)kout * ld, w3, n);
     } else {
-      double *Z = w3, *Y = w3 + ilv, *buf[2] = {w3 + 2 * ilv, w3 + 3 * ilv};
-      CPtrs src{};
-      VPtrs dst{};
-      int maxdeg = 0;
-      for (int s = 0; s < ns; s++) {
-        src.p[s] = xin ? xin : SL[s].V + (size_t)kin * ld;
-        dst.p[s] = SL[s].V + (size_t)kout * ld;
-        if ((mask >> s) & 1u) maxdeg = PEVSL_MAX(maxdeg, SL[s].pol->deg);
-      }
-      r = b_gather(n, Sp, src, Z, mask);
-      bp.mask = mask;
-      const double *vk = Z, *vkm1 = nullptr;
-      for (int k = 1; k <= maxdeg && !r; k++) {
-        double *vkp1 = k <= 2 ? buf[k - 1] : const_cast<double *>(vkm1);
-        r = cheb_multi(A, Sp, vk, vkm1, vkp1, Y, mu_all, mu_ld, k, bp);
-        /* one read of the matrix serves every slice still filtering */
-        g_filter_launches++;
-        g_filter_bytes += 12.0 * (double)A->nnz + 4.0 * (A->nrows + 1.0);
-        for (int s = 0; s < ns; s++)
-          if (((mask >> s) & 1u) && k <= SL[s].pol->deg)
-            g_filter_bytes += (k == 1 ? 24.0 : 40.0) * (double)A->nrows;
-        vkm1 = vk;
-        vk = vkp1;
-      }
-      if (!r) r = b_scatter(n, Sp, Y, dst, mask);
+      /* one matrix read per degree for every slice in mask; mixed: FP32 */
+      FilterJob jobs[kMaxBatch];
+      int ne = 0;
       for (int s = 0; s < ns; s++)
-        if ((mask >> s) & 1u) {
-          pevsl->stats->n_polAv++;
-          pevsl->stats->n_mvA += (size_t)SL[s].pol->deg;
-        }
+        if ((mask >> s) & 1u)
+          jobs[ne++] = FilterJob{xin ? xin : SL[s].V + (size_t)kin * ld,
+                                 SL[s].V + (size_t)kout * ld, SL[s].pol};
+      r = cheb_filter_batch(pevsl, A, ne, jobs, bwork, mixed);
     }
     t_pol.end();
     return r;
@@ -943,7 +1206,8 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
         if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
         st = pevsl_rand_vector_dev(vrand, (int)n);
         t_pol.begin();
-        if (!st) st = cheb_apply(pevsl, S->pol, vrand, znew, w3 + (interleaved ? 2 * ilv : 0), n);
+        if (!st)
+          st = cheb_apply(pevsl, S->pol, vrand, znew, w3, n);
         t_pol.end();
         if (!st) st = vnrm2(n, znew, c.dscal + S_NRM0);
         if (!st) st = cgs_dgks(S->V, ld, k + 1, znew, n);
@@ -986,7 +1250,10 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
         }
       }
       if (fstats) fprintf(fstats, "  k %4d:   nconv %4d  tr1 %21.15e\n", k, S->nconv, tr1);
-      const bool conv = fabs(tr1 - S->tr0) < 2e-12 || fabs(tr1) + fabs(S->tr0) < 1e-10;
+      /* FP64: the reference's test; mixed: differences at the FP32 noise
+       * level of the filtered operator count as converged */
+      const double trtol = mixed ? trtol_mixed * PEVSL_MAX(1, S->nconv) : 2e-12;
+      const bool conv = fabs(tr1 - S->tr0) < trtol || fabs(tr1) + fabs(S->tr0) < 1e-10;
       S->tr0 = tr1;
       if (conv || k == S->maxit - 1) {
         if (!conv && fstats)
@@ -1002,7 +1269,8 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     SliceState *S = &SL[s];
     if (S->done || S->status) continue;
     S->its = S->kdim;
-    const int rs = ritz_extract(pevsl, S, vinit, n, ld, tol);
+    const int rs = mixed ? ritz_refine(pevsl, S, vinit, n, ld, tol, guard, passes)
+                         : ritz_extract(pevsl, S, vinit, n, ld, tol);
     if (rs) S->status = rs;
   }
   pevsl->stats->t_ritz = pevsl_now() - tr_start;
@@ -1026,6 +1294,42 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     free(SL[s].EvalT);
     SL[s].dT = SL[s].eT = SL[s].EvalT = nullptr;
   }
+  if (mixed && !st) {
+    /* a slice whose refined pairs in [a, b] did not all reach tol is run
+     * again in FP64, so the mixed form never reports fewer pairs */
+    SliceState R[kMaxBatch];
+    int idx[kMaxBatch], nr = 0;
+    for (int s = 0; s < ns; s++) {
+      SliceState *S = &SL[s];
+      if (S->done || S->status || S->short_pairs <= 0) continue;
+      free_slice_outputs(S);
+      memset(&R[nr], 0, sizeof R[nr]);
+      memcpy(R[nr].intv, S->intv, sizeof S->intv);
+      R[nr].pol = S->pol;
+      R[nr].maxit = S->maxit;
+      idx[nr++] = s;
+    }
+    if (nr > 0) {
+      g_fallbacks += nr;
+      const float ms0 = inst->phase_ms[2], pol0 = inst->phase_ms[3], orth0 = inst->phase_ms[4];
+      st = cheblannr_group(pevsl, R, nr, tol, vinit, fstats, false);
+      inst->phase_ms[2] += ms0;
+      inst->phase_ms[3] += pol0;
+      inst->phase_ms[4] += orth0;
+      for (int r = 0; r < nr; r++) {
+        SliceState *S = &SL[idx[r]];
+        S->status = R[r].status;
+        S->kdim = R[r].kdim;
+        S->its = R[r].its;
+        S->nconv = R[r].nconv;
+        S->nev = R[r].nev;
+        S->Lam = R[r].Lam;
+        S->res = R[r].res;
+        S->Rvec = R[r].Rvec;
+        S->short_pairs = 0;
+      }
+    }
+  }
   return st;
 }
 
@@ -1046,6 +1350,7 @@ int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevs
   S.maxit = maxit;
   g_t_pol.init();
   g_t_orth.init();
+  g_fallbacks = 0;
   int st = cheblannr_group(pevsl, &S, 1, tol, vinit, fstats);
   pevsl_inst *inst = pevsl_inst_of(pevsl);
   inst->last_its = S.kdim;
@@ -1081,6 +1386,7 @@ int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intv
   int first_err = 0;
   g_t_pol.init();
   g_t_orth.init();
+  g_fallbacks = 0;
   double ms_total = 0.0, pol_total = 0.0, orth_total = 0.0;
   for (int s0 = 0; s0 < nslices; s0 += kMaxBatch) {
     const int ns = PEVSL_MIN(kMaxBatch, nslices - s0);

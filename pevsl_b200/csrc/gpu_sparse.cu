@@ -112,9 +112,19 @@ __global__ void k_cheb_combine(long n, const double *__restrict__ ax, const doub
  * thread per row, so the vector traffic is coalesced. */
 constexpr int kStreamChunk = 256; /* staged entries per warp per pass */
 
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+/* An epilogue loads what it needs of its row (pre) before the row's
+ * products are formed, so those loads overlap the matrix and gather loads,
+ * and then combines (operator()). */
 struct EpiStore {
   double *y;
-  __device__ __forceinline__ void operator()(int row, double r) const { y[row] = r; }
+  struct Pre {};
+  __device__ __forceinline__ Pre pre(int) const { return Pre{}; }
+  __device__ __forceinline__ void operator()(int row, double r, const Pre &) const { y[row] = r; }
 };
 
 /* vkp1 may alias vkm1: the thread of a row reads v_{k-1} there first */
@@ -123,61 +133,159 @@ struct EpiCheb {
   double *vkp1, *y;
   double cc, t, mu0, muk;
   int first;
-  __device__ __forceinline__ void operator()(int row, double r) const {
-    double w, yv = first ? 0.0 : y[row];
-    cheb_update(r, vk[row], vkm1 ? vkm1 + row : nullptr, cc, t, mu0, muk, first, &w, &yv);
+  struct Pre {
+    double x, xm1, y;
+  };
+  __device__ __forceinline__ Pre pre(int row) const {
+    return Pre{vk[row], vkm1 ? vkm1[row] : 0.0, first ? 0.0 : y[row]};
+  }
+  __device__ __forceinline__ void operator()(int row, double r, const Pre &p) const {
+    double w, yv;
+    cheb_update_v(r, p.x, p.xm1, vkm1 != nullptr, cc, t, mu0, muk, first, p.y, &w, &yv);
     vkp1[row] = w;
     y[row] = yv;
   }
 };
 
-template <class Epi>
-__global__ void __launch_bounds__(kThreads)
-    k_csr_stream(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                 const double *__restrict__ a, const double *__restrict__ x, Epi epi) {
-  __shared__ double prod[kThreads / 32][kStreamChunk];
+/* FP32 degree of the mixed-precision filter; the last degree writes the
+ * accumulated p(A) x to the FP64 output (yout) instead of y */
+struct EpiCheb32 {
+  const float *vk, *vkm1;
+  float *vkp1, *y;
+  double *yout;
+  float cc, t, mu0, muk;
+  int first;
+  struct Pre {
+    float x, xm1, y;
+  };
+  __device__ __forceinline__ Pre pre(int row) const {
+    return Pre{vk[row], vkm1 ? vkm1[row] : 0.f, first ? 0.f : y[row]};
+  }
+  __device__ __forceinline__ void operator()(int row, float r, const Pre &p) const {
+    float w = __fmul_rn(__fmaf_rn(-cc, p.x, r), t);
+    if (vkm1) w = __fsub_rn(w, p.xm1);
+    vkp1[row] = w;
+    const float yv = first ? __fmaf_rn(muk, w, __fmul_rn(mu0, p.x)) : __fmaf_rn(muk, w, p.y);
+    if (yout)
+      yout[row] = (double)yv;
+    else
+      y[row] = yv;
+  }
+};
+
+/* Rows [32 R (8 rblk + warp), +32 R) of y = A x, lane l owning rows
+ * l + 32 j (j < R) so that the epilogue is coalesced.  Per pass a warp
+ * stages 256 R consecutive entries of its rows: column indices and values
+ * with independent coalesced loads, then the gathered products
+ * a[j] * x[ja[j]] (unfused) into shared memory; each lane adds its rows'
+ * products in index order -- the summation order of the reference's row
+ * loop (SRC/spmat.c:188-193), so the result matches it to the last bit. */
+template <int R, class T, class Epi>
+__device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
+                                            const int *__restrict__ ja, const T *__restrict__ a,
+                                            const T *__restrict__ x, const Epi &epi, long rblk,
+                                            T (*prod)[kStreamChunk * R]) {
+  constexpr int CH = kStreamChunk * R, PL = CH / 32;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const long r0l = ((long)blockIdx.x * (kThreads / 32) + w) * 32;
+  const long r0l = (rblk * (kThreads / 32) + w) * 32 * R;
   if (r0l >= n) return; /* the whole warp leaves */
   const int r0 = (int)r0l;
-  const int nr = n - r0 < 32 ? n - r0 : 32;
-  const int row = r0 + lane;
-  const int base = ia[r0], end = ia[r0 + nr];
-  int rs = 0, re = 0;
-  if (lane < nr) {
-    rs = ia[row] - base;
-    re = ia[row + 1] - base;
-  }
-  double acc = 0.0;
-  double *pw = prod[w];
-  const int len = end - base;
-  for (int c0 = 0; c0 < len; c0 += kStreamChunk) {
-    int col[kStreamChunk / 32];
-    double val[kStreamChunk / 32];
+  const int nr = n - r0 < 32 * R ? n - r0 : 32 * R;
+  typename Epi::Pre pre[R];
+  int rs[R], re[R];
 #pragma unroll
-    for (int q = 0; q < kStreamChunk / 32; q++) {
+  for (int j = 0; j < R; j++) {
+    const int row = r0 + lane + 32 * j;
+    rs[j] = re[j] = 0;
+    if (lane + 32 * j < nr) {
+      pre[j] = epi.pre(row);
+      rs[j] = ia[row];
+      re[j] = ia[row + 1];
+    }
+  }
+  const int base = ia[r0], len = ia[r0 + nr] - base;
+  T acc[R];
+#pragma unroll
+  for (int j = 0; j < R; j++) {
+    rs[j] -= base;
+    re[j] -= base;
+    acc[j] = T(0);
+  }
+  T *pw = prod[w];
+  for (int c0 = 0; c0 < len; c0 += CH) {
+    int col[PL];
+    T val[PL];
+#pragma unroll
+    for (int q = 0; q < PL; q++) {
       const int t = c0 + q * 32 + lane;
       col[q] = t < len ? ja[base + t] : -1;
-      val[q] = t < len ? a[base + t] : 0.0;
+      val[q] = t < len ? a[base + t] : T(0);
     }
 #pragma unroll
-    for (int q = 0; q < kStreamChunk / 32; q++) {
-      const double xv = col[q] >= 0 ? __ldg(x + col[q]) : 0.0;
-      pw[q * 32 + lane] = __dmul_rn(val[q], xv);
+    for (int q = 0; q < PL; q++) {
+      const T xv = col[q] >= 0 ? __ldg(x + col[q]) : T(0);
+      pw[q * 32 + lane] = mul_rn(val[q], xv);
     }
     __syncwarp();
-    const int lo = rs > c0 ? rs : c0;
-    const int hi = re < c0 + kStreamChunk ? re : c0 + kStreamChunk;
-    for (int t = lo; t < hi; t++) acc = __dadd_rn(acc, pw[t - c0]);
+#pragma unroll
+    for (int j = 0; j < R; j++) {
+      const int lo = rs[j] > c0 ? rs[j] : c0;
+      const int hi = re[j] < c0 + CH ? re[j] : c0 + CH;
+      for (int t = lo; t < hi; t++) acc[j] = add_rn(acc[j], pw[t - c0]);
+    }
     __syncwarp();
   }
-  if (lane < nr) epi(row, acc);
+#pragma unroll
+  for (int j = 0; j < R; j++)
+    if (lane + 32 * j < nr) epi(r0 + lane + 32 * j, acc[j], pre[j]);
 }
 
-static unsigned stream_grid(int n) {
-  const long rows_per_block = (kThreads / 32) * 32;
+/* R = 1 fits 48 registers (5 blocks per SM) without spilling */
+template <int R, class T, class Epi>
+__global__ void __launch_bounds__(kThreads, R == 1 ? 5 : 1)
+    k_csr_stream(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                 const T *__restrict__ a, const T *__restrict__ x, Epi epi) {
+  __shared__ T prod[kThreads / 32][kStreamChunk * R];
+  stream_rows<R>(n, ia, ja, a, x, epi, blockIdx.x, prod);
+}
+
+/* Up to kMaxBatch independent products y_e = A x_e, each with its own
+ * epilogue.  Block b serves entry b % nb on row block b / nb: the nb blocks
+ * that read one stretch of the matrix are adjacent in launch order, so the
+ * stretch comes from HBM once and from L2 for the other entries, while each
+ * entry keeps its vectors in its own columns (no interleaving, no copies).
+ * The per-entry arithmetic is that of k_csr_stream, bit for bit. */
+template <class T, class Epi>
+struct StreamBatch {
+  const T *x[kMaxBatch];
+  Epi epi[kMaxBatch];
+  int nb;
+};
+
+template <int R, class T, class Epi>
+__global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
+    k_csr_stream_batch(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                       const T *__restrict__ a, const __grid_constant__ StreamBatch<T, Epi> b) {
+  __shared__ T prod[kThreads / 32][kStreamChunk * R];
+  const int e = (int)(blockIdx.x % (unsigned)b.nb);
+  stream_rows<R>(n, ia, ja, a, b.x[e], b.epi[e], (long)(blockIdx.x / (unsigned)b.nb), prod);
+}
+
+/* rows per lane of the CSR-stream kernels: 1 or 2 (PEVSL_B200_STREAM_R) */
+static int stream_r() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("PEVSL_B200_STREAM_R");
+    v = (e && atoi(e) == 2) ? 2 : 1;
+  }
+  return v;
+}
+
+static unsigned stream_grid(int n, int R) {
+  const long rows_per_block = (kThreads / 32) * 32L * R;
   return (unsigned)((n + rows_per_block - 1) / rows_per_block);
 }
+
 
 /* KPM degree for s <= 32*CPL interleaved vectors; one warp per row (grid
  * stride), lane c handles columns c, c+32, ...  Moments: per-block partial
@@ -320,11 +428,31 @@ __global__ void k_block_normalize(long n, int s, int ld, double *X, const double
     }                                                                                            \
   } while (0)
 
+/* one CSR-stream launch with R rows per lane */
+template <class T, class Epi>
+static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const Epi &epi) {
+  if (stream_r() == 2)
+    k_csr_stream<2><<<stream_grid(A->nrows, 2), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja,
+                                                                             a, x, epi);
+  else
+    k_csr_stream<1><<<stream_grid(A->nrows, 1), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja,
+                                                                             a, x, epi);
+}
+
+template <class T, class Epi>
+static void launch_stream_batch(const pevsl_devcsr *A, const T *a, const StreamBatch<T, Epi> &b) {
+  const int R = stream_r();
+  const unsigned g = stream_grid(A->nrows, R) * (unsigned)b.nb;
+  if (R == 2)
+    k_csr_stream_batch<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, a, b);
+  else
+    k_csr_stream_batch<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, a, b);
+}
+
 int spmv(const pevsl_devcsr *A, const double *x, double *y) {
   if (A->nrows <= 0) return 0;
   if (A->lanes == 0) {
-    k_csr_stream<<<stream_grid(A->nrows), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a,
-                                                                       x, EpiStore{y});
+    launch_stream(A, (const double *)A->a, x, EpiStore{y});
     return launched("spmv_stream");
   }
   PV_LANE_SWITCH(k_spmv, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, x, y);
@@ -335,14 +463,39 @@ int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, doubl
               double cc, double t, double mu0, double muk, int first) {
   if (A->nrows <= 0) return 0;
   if (A->lanes == 0) {
-    EpiCheb e{vk, vkm1, vkp1, y, cc, t, mu0, muk, first};
-    k_csr_stream<<<stream_grid(A->nrows), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a,
-                                                                       vk, e);
+    launch_stream(A, (const double *)A->a, vk, EpiCheb{vk, vkm1, vkp1, y, cc, t, mu0, muk, first});
     return launched("cheb_step_stream");
   }
   PV_LANE_SWITCH(k_cheb_step, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y,
                  cc, t, mu0, muk, first);
   return launched("cheb_step");
+}
+
+int cheb_step_batch(const pevsl_devcsr *A, int nb, const ChebEntry *e, bool fp32) {
+  if (A->nrows <= 0 || nb <= 0) return 0;
+  if (nb > kMaxBatch) return PEVSL_ERR_ARG;
+  if (fp32) {
+    if (!A->a32) return PEVSL_ERR_ARG;
+    StreamBatch<float, EpiCheb32> b{};
+    b.nb = nb;
+    for (int i = 0; i < nb; i++) {
+      b.x[i] = (const float *)e[i].vk;
+      b.epi[i] = EpiCheb32{(const float *)e[i].vk, (const float *)e[i].vkm1, (float *)e[i].vkp1,
+                           (float *)e[i].y, e[i].yout, (float)e[i].cc, (float)e[i].t,
+                           (float)e[i].mu0, (float)e[i].muk, e[i].first};
+    }
+    launch_stream_batch(A, (const float *)A->a32, b);
+    return launched("cheb_step_batch32");
+  }
+  StreamBatch<double, EpiCheb> b{};
+  b.nb = nb;
+  for (int i = 0; i < nb; i++) {
+    b.x[i] = (const double *)e[i].vk;
+    b.epi[i] = EpiCheb{(const double *)e[i].vk, (const double *)e[i].vkm1, (double *)e[i].vkp1,
+                       (double *)e[i].y, e[i].cc, e[i].t, e[i].mu0, e[i].muk, e[i].first};
+  }
+  launch_stream_batch(A, (const double *)A->a, b);
+  return launched("cheb_step_batch");
 }
 
 int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1, double *vkp1,

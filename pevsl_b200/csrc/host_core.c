@@ -140,6 +140,12 @@ int pEVSL_SetSigmaMult(pevsl_Data *d, double mult) {
   return 0;
 }
 
+int pEVSL_B200_SetPrecision(pevsl_Data *d, int precision) {
+  if (precision != PEVSL_PREC_FP64 && precision != PEVSL_PREC_MIXED) return PEVSL_ERR_ARG;
+  pevsl_inst_of(d)->precision = precision;
+  return 0;
+}
+
 int pEVSL_B200_LastIterations(pevsl_Data *d) { return pevsl_inst_of(d)->last_its; }
 int pEVSL_B200_LastNconv(pevsl_Data *d) { return pevsl_inst_of(d)->last_nconv; }
 double pEVSL_B200_PhaseMs(pevsl_Data *d, int phase) {

@@ -269,3 +269,190 @@ int pevsl_dense_symeig(int n, const double *A, int lda, double *Q, int ldq, doub
   free(V);
   return 0;
 }
+
+/* Eigenpairs of a dense symmetric matrix (column major, both triangles set)
+ * whose eigenvalues lie in [lo, hi]: Householder reduction to tridiagonal
+ * form Q' H Q = T (Golub & Van Loan, Alg. 8.3.1, with the symmetric rank-2
+ * update), the tridiagonal QR above for the eigenvalues and the selected
+ * eigenvectors y, then x = Q y by applying the reflectors last to first
+ * (Q is never formed).  lam (ascending) and Z (n x *m) must hold n
+ * entries / columns.  O(n^3) for the reduction, O(n^2 *m) for the vectors. */
+int pevsl_dense_symeig_range(int n, const double *H, int ldh, double lo, double hi, int *m,
+                             double *lam, double *Z, int ldz) {
+  *m = 0;
+  if (n <= 0) return 0;
+  double *A = (double *)malloc((size_t)n * (size_t)n * sizeof(double));
+  double *d = (double *)malloc((size_t)n * sizeof(double));
+  double *e = (double *)calloc((size_t)n, sizeof(double));
+  double *beta = (double *)calloc((size_t)n, sizeof(double));
+  double *p = (double *)malloc((size_t)n * sizeof(double));
+  double *w = (double *)malloc((size_t)n * sizeof(double));
+  int *sel = (int *)malloc((size_t)n * sizeof(int));
+  int st = 0;
+  if (!A || !d || !e || !beta || !p || !w || !sel) st = PEVSL_ERR_NOMEM;
+  if (!st) {
+    for (int j = 0; j < n; j++) memcpy(A + (size_t)j * n, H + (size_t)j * ldh, (size_t)n * sizeof(double));
+    /* reflector k acts on rows/cols k+1..n-1; its vector v (v[0] = 1 is not
+     * stored implicitly: the whole v is kept) replaces A(k+1:n, k) */
+    for (int k = 0; k + 2 < n; k++) {
+      double *x = A + (size_t)k * n + (k + 1);
+      const int len = n - k - 1;
+      double sig = 0.0;
+      for (int i = 1; i < len; i++) sig += x[i] * x[i];
+      if (sig == 0.0) {
+        beta[k] = 0.0;
+        e[k] = x[0];
+        continue;
+      }
+      const double nx = sqrt(x[0] * x[0] + sig);
+      const double alpha = x[0] > 0 ? -nx : nx;
+      x[0] -= alpha; /* v = x - alpha e1 */
+      const double vv = x[0] * x[0] + sig;
+      const double b = 2.0 / vv;
+      beta[k] = b;
+      e[k] = alpha;
+      /* p = b * A22 v */
+      double *A22 = A + (size_t)(k + 1) * n + (k + 1);
+      for (int i = 0; i < len; i++) p[i] = 0.0;
+      for (int j = 0; j < len; j++) {
+        const double vj = x[j];
+        const double *col = A22 + (size_t)j * n;
+        for (int i = 0; i < len; i++) p[i] += col[i] * vj;
+      }
+      double pv = 0.0;
+      for (int i = 0; i < len; i++) {
+        p[i] *= b;
+        pv += p[i] * x[i];
+      }
+      /* w = p - (b/2)(p'v) v;  A22 -= v w' + w v' */
+      const double c = 0.5 * b * pv;
+      for (int i = 0; i < len; i++) w[i] = p[i] - c * x[i];
+      for (int j = 0; j < len; j++) {
+        double *col = A22 + (size_t)j * n;
+        const double vj = x[j], wj = w[j];
+        for (int i = 0; i < len; i++) col[i] -= x[i] * wj + w[i] * vj;
+      }
+    }
+    for (int i = 0; i < n; i++) d[i] = A[(size_t)i * n + i];
+    if (n >= 2) e[n - 2] = A[(size_t)(n - 2) * n + (n - 1)];
+    for (int k = 0; k + 2 < n; k++)
+      if (beta[k] == 0.0) e[k] = A[(size_t)k * n + (k + 1)];
+    /* eigenvalues, then the vectors of those in [lo, hi] */
+    st = pevsl_tridiag_eig(n, d, e, w, NULL);
+    int ns = 0;
+    for (int i = 0; !st && i < n; i++)
+      if (w[i] >= lo && w[i] <= hi) sel[ns++] = i;
+    if (!st && ns > 0) {
+      double *Y = (double *)malloc((size_t)n * (size_t)ns * sizeof(double));
+      if (!Y) st = PEVSL_ERR_NOMEM;
+      if (!st) st = pevsl_tridiag_eig_sel(n, d, e, w, ns, sel, Y);
+      for (int j = 0; !st && j < ns; j++) {
+        double *y = Y + (size_t)j * n;
+        for (int k = n - 3; k >= 0; k--) {
+          if (beta[k] == 0.0) continue;
+          const double *v = A + (size_t)k * n + (k + 1);
+          double s = 0.0;
+          for (int i = 0; i < n - k - 1; i++) s += v[i] * y[k + 1 + i];
+          s *= beta[k];
+          for (int i = 0; i < n - k - 1; i++) y[k + 1 + i] -= s * v[i];
+        }
+        lam[j] = w[sel[j]];
+        memcpy(Z + (size_t)j * ldz, y, (size_t)n * sizeof(double));
+      }
+      free(Y);
+      if (!st) *m = ns;
+    }
+  }
+  free(A);
+  free(d);
+  free(e);
+  free(beta);
+  free(p);
+  free(w);
+  free(sel);
+  return st;
+}
+
+/* Eigenpairs with eigenvalues in [lo, hi] of the pencil (H, G), G = P'P a
+ * Gram matrix with unit diagonal, H = P' A P (both m x m, column major):
+ * Cholesky G = L L' processed column by column, a column whose pivot falls
+ * below 1e-10 (numerically dependent on the earlier ones) is dropped, then
+ * C = L^-1 H L^-T on the kept columns, the ranged eigensolver above, and
+ * Z = L^-T Zc scattered back to the m rows (dropped rows zero).  Returns
+ * the eigenvalues (ascending) in lam and the m x *nout coefficients in Z. */
+int pevsl_gen_symeig_range(int m, const double *H, const double *G, int ld, double lo, double hi,
+                           int *nout, double *lam, double *Z, int ldz) {
+  *nout = 0;
+  if (m <= 0) return 0;
+  double *L = (double *)calloc((size_t)m * m, sizeof(double)); /* kept x kept, column major */
+  int *keep = (int *)malloc((size_t)m * sizeof(int));
+  double *Cm = (double *)malloc((size_t)m * m * sizeof(double));
+  double *Zc = (double *)malloc((size_t)m * m * sizeof(double));
+  double *tmp = (double *)malloc((size_t)m * sizeof(double));
+  int st = (!L || !keep || !Cm || !Zc || !tmp) ? PEVSL_ERR_NOMEM : 0;
+  int q = 0;
+  /* left-looking Cholesky over the kept columns */
+  for (int j = 0; j < m && !st; j++) {
+    /* row q of L for candidate column j: L(q, i) for i < q solve L(0:q,0:q) l = G(keep, j) */
+    for (int i = 0; i < q; i++) {
+      double s = G[(size_t)j * ld + keep[i]];
+      for (int t = 0; t < i; t++) s -= L[(size_t)t * m + i] * tmp[t];
+      tmp[i] = s / L[(size_t)i * m + i];
+    }
+    double d = G[(size_t)j * ld + j];
+    for (int i = 0; i < q; i++) d -= tmp[i] * tmp[i];
+    if (!(d > 1e-10 * G[(size_t)j * ld + j])) continue; /* dependent: drop */
+    for (int i = 0; i < q; i++) L[(size_t)i * m + q] = tmp[i];
+    L[(size_t)q * m + q] = sqrt(d);
+    keep[q++] = j;
+  }
+  if (!st && q > 0) {
+    /* C = L^-1 Hk L^-T, Hk = H(keep, keep): solve column by column */
+    for (int c = 0; c < q; c++) {
+      for (int r = 0; r < q; r++) Cm[(size_t)c * q + r] = H[(size_t)keep[c] * ld + keep[r]];
+    }
+    /* Cm <- L^-1 Cm (forward substitution on each column) */
+    for (int c = 0; c < q; c++) {
+      double *col = Cm + (size_t)c * q;
+      for (int r = 0; r < q; r++) {
+        double s = col[r];
+        for (int t = 0; t < r; t++) s -= L[(size_t)t * m + r] * col[t];
+        col[r] = s / L[(size_t)r * m + r];
+      }
+    }
+    /* Cm <- Cm L^-T: rows of Cm solved against L, i.e. (L^-1 Cm^T)^T */
+    for (int r = 0; r < q; r++) {
+      for (int c = 0; c < q; c++) {
+        double s = Cm[(size_t)c * q + r];
+        for (int t = 0; t < c; t++) s -= L[(size_t)t * m + c] * Cm[(size_t)t * q + r];
+        Cm[(size_t)c * q + r] = s / L[(size_t)c * m + c];
+      }
+    }
+    for (int c = 0; c < q; c++)
+      for (int r = 0; r < c; r++) {
+        const double h = 0.5 * (Cm[(size_t)c * q + r] + Cm[(size_t)r * q + c]);
+        Cm[(size_t)c * q + r] = Cm[(size_t)r * q + c] = h;
+      }
+    int ns = 0;
+    st = pevsl_dense_symeig_range(q, Cm, q, lo, hi, &ns, lam, Zc, q);
+    /* Z(keep, j) = L^-T zc (back substitution), other rows zero */
+    for (int j = 0; j < ns && !st; j++) {
+      double *zc = Zc + (size_t)j * q;
+      for (int r = q - 1; r >= 0; r--) {
+        double s = zc[r];
+        for (int t = r + 1; t < q; t++) s -= L[(size_t)r * m + t] * zc[t];
+        zc[r] = s / L[(size_t)r * m + r];
+      }
+      double *z = Z + (size_t)j * ldz;
+      for (int r = 0; r < m; r++) z[r] = 0.0;
+      for (int r = 0; r < q; r++) z[keep[r]] = zc[r];
+    }
+    if (!st) *nout = ns;
+  }
+  free(L);
+  free(keep);
+  free(Cm);
+  free(Zc);
+  free(tmp);
+  return st;
+}

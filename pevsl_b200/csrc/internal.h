@@ -24,6 +24,7 @@ typedef struct pevsl_inst {
   pevsl_Ltsol ltsol;
   int last_its, last_nconv;
   double phase_ms[8];
+  int precision; /* PEVSL_PREC_FP64 or PEVSL_PREC_MIXED */
 } pevsl_inst;
 
 static inline pevsl_inst *pevsl_inst_of(pevsl_Data *d) { return (pevsl_inst *)d; }
@@ -68,6 +69,14 @@ int pevsl_tridiag_eig_sel(int n, const double *d, const double *e, double *w, in
                           const int *sel, double *Zsel);
 /* eigen-decomposition of a dense symmetric matrix (column major) */
 int pevsl_dense_symeig(int n, const double *A, int lda, double *Q, int ldq, double *lam);
+/* eigenpairs with eigenvalues in [lo, hi] of a dense symmetric matrix
+ * (Householder tridiagonalisation + tridiagonal QR); *m of them */
+int pevsl_dense_symeig_range(int n, const double *H, int ldh, double lo, double hi, int *m,
+                             double *lam, double *Z, int ldz);
+/* eigenpairs with eigenvalues in [lo, hi] of the pencil (H, G), G a Gram
+ * matrix with unit diagonal; dependent columns are dropped */
+int pevsl_gen_symeig_range(int m, const double *H, const double *G, int ld, double lo, double hi,
+                           int *nout, double *lam, double *Z, int ldz);
 void pevsl_simpson(const double *xi, double *yi, int npts);
 
 /* RNG state (host side; rng.cu owns the device generator) */

@@ -410,3 +410,29 @@ def test_batch_mixed_statuses(gpu):
         assert np.array_equal(o["lam"], s["lam"])
         ex = exact_eig_lap(10, 10, 10, *(good[0][:2] if s is single[0] else good[1][:2]))
         assert len(ex) == o["nev"]
+
+
+# ---------------------------------------------------------------- mixed precision
+@pytest.mark.parametrize("name", ["lap20_lantr_gauss", "lap10_kpm_gauss", "lap20_readme_glibc"])
+def test_mixed_precision_counts_and_residuals(gpu, name):
+    """FP32 filter + FP32 KPM moments, FP64 basis / reorthogonalisation /
+    one FP64 filtered Rayleigh-Ritz sweep (slices whose refined pairs miss
+    tol are solved again in FP64): every slice holds exactly the eigenvalues
+    of A inside it, each within 1e-10 (relative) of the exact value, with
+    ||Ax - lam x|| < 1e-8 and ||Ax - lam x||/|lam| <= 1e-8.  The FP32 KPM
+    moves the slice ends by at most 1e-5 (relative); where the slices are
+    the FP64 run's, so are the per-slice counts."""
+    g = golden("pipelines.json")[name]
+    A = dev_matrix(laplacian(*g["grid"]))
+    r = pv.solve_interval(A, pv.SliceRun(**g["spec"]), batched=True, precision=pv.PREC_MIXED)
+    assert r.status == 0
+    assert 0 <= r.fallbacks <= len(r.nev)
+    assert rel(r.sli, g["sli"]) <= 1e-5, (r.sli, g["sli"])
+    if rel(r.sli, g["sli"]) <= 1e-12:
+        assert r.nev == g["nev"]
+    for sl in range(len(r.nev)):
+        lam = r.lam[sl]
+        assert np.all(r.res[sl] / np.abs(lam) <= 1e-8) and np.all(r.res[sl] < 1e-8)
+        ex = exact_eig_lap(*g["grid"], r.sli[sl], r.sli[sl + 1])
+        assert len(lam) == len(ex), (sl, len(lam), len(ex))
+        assert np.max(np.abs(lam - ex) / np.abs(ex)) <= 1e-10
