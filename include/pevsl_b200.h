@@ -49,8 +49,15 @@ uint64_t pEVSL_B200_RngDraws(void);
 #define PEVSL_PREC_MIXED 1
 int pEVSL_B200_SetPrecision(pevsl_Data *pevsl, int precision);
 
-/* Slices of the last pEVSL_ChebLanNr / pEVSL_B200_ChebLanNrBatch call that
- * the mixed form solved again in FP64. */
+/* Form of the batched filter: -1 automatic (one launch per degree), 0 one
+ * launch per degree serving every slice still filtering, 1 one persistent
+ * cooperative launch running every degree of every slice (per-slice degree
+ * counters, a grid barrier between degrees).  The results are the same
+ * bits either way.  PEVSL_B200_FILTER_FORM sets the start value. */
+int pEVSL_B200_SetFilterForm(int form);
+
+/* Slices of the last pEVSL_ChebLanNr / pEVSL_B200_ChebLanNrBatch /
+ * pEVSL_B200_ChebLanNrMulti call that the mixed form solved again in FP64. */
 int pEVSL_B200_LastFallbacks(void);
 
 /* Lanczos steps taken by the last pEVSL_ChebLanNr on this instance, and the
@@ -81,9 +88,11 @@ int pEVSL_B200_LastError(void);
 int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y);
 
 /* pEVSL_ChebLanNr for nslices slices at once.  The slices advance in
- * lockstep: one fused filter kernel per polynomial degree serves every slice
- * still filtering (the matrix is read once per degree for all of them), the
- * reorthogonalisation kernels run batched, and one host read per Lanczos
+ * lockstep (up to 256 per group): one fused filter launch per polynomial
+ * degree serves every slice still filtering (the matrix is read once per
+ * degree for all of them), or (PEVSL_B200_FILTER_FORM=1) one persistent
+ * launch runs every degree;
+ * the reorthogonalisation kernels run batched, and one host read per Lanczos
  * step fetches all slices' recurrence scalars.  Slice s uses
  * intvs[4s..4s+3], pols[s], maxits[s]; its outputs are nevOut[s], lamo[s],
  * Wo[s], reso[s] (allocated as by pEVSL_ChebLanNr), its[s] (Lanczos steps)
@@ -96,6 +105,21 @@ int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intv
                               pevsl_Polparams *pols, int *nevOut, double **lamo,
                               pevsl_Parvecs **Wo, double **reso, int *its, int *status,
                               FILE *fstats);
+
+/* pEVSL_B200_ChebLanNrBatch for several problems at once: problem p (its
+ * own instance pevsls[p], matrix and start vector vinits[p]) has nslices[p]
+ * slices, stored one after the other in intvs (4 doubles each), maxits,
+ * pols and the per-slice outputs.  All slices of all problems advance in
+ * lockstep (up to 256 per group); every filter degree of a step is one
+ * launch over all slices still filtering, each with its own matrix,
+ * polynomial and degree (or one persistent launch for all degrees, see
+ * pEVSL_B200_SetFilterForm).  Each slice's result equals solving it
+ * alone. */
+int pEVSL_B200_ChebLanNrMulti(int nprob, pevsl_Data **pevsls, const int *nslices,
+                              const double *intvs, const int *maxits, double tol,
+                              pevsl_Parvec **vinits, pevsl_Polparams *pols, int *nevOut,
+                              double **lamo, pevsl_Parvecs **Wo, double **reso, int *its,
+                              int *status, FILE *fstats);
 
 /* w = V(:, 0:k)' x (the projection of pEVSL_ParvecsGemtv) without any device
  * allocation; no counterpart in the reference.  For callers that must not

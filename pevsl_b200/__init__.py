@@ -166,8 +166,13 @@ SIGNATURES = [
     ("pEVSL_B200_ResetFilterCounters", None, []),
     ("pEVSL_B200_SetPrecision", _I, [C.POINTER(PevslData), _I]),
     ("pEVSL_B200_LastFallbacks", _I, []),
+    ("pEVSL_B200_SetFilterForm", _I, [_I]),
     ("pEVSL_B200_ChebLanNrBatch", _I, [C.POINTER(PevslData), _I, _dp, _ip, _D,
                                        C.POINTER(Parvec), C.POINTER(Polparams), _ip,
+                                       C.POINTER(_dp), C.POINTER(C.POINTER(Parvecs)),
+                                       C.POINTER(_dp), _ip, _ip, _vp]),
+    ("pEVSL_B200_ChebLanNrMulti", _I, [_I, C.POINTER(C.POINTER(PevslData)), _ip, _dp, _ip, _D,
+                                       C.POINTER(C.POINTER(Parvec)), C.POINTER(Polparams), _ip,
                                        C.POINTER(_dp), C.POINTER(C.POINTER(Parvecs)),
                                        C.POINTER(_dp), _ip, _ip, _vp]),
 ]
@@ -511,6 +516,68 @@ def cheblannr_batch(ev: "Instance", intvs, maxits, tol, vinit, filters):
             o["lam"], o["res"] = la[order], rs[order]
         _free_outputs(lib, lam[i], res[i], W[i])
         outs.append(o)
+    return r, outs
+
+
+def cheblannr_multi(problems):
+    """pEVSL_B200_ChebLanNrMulti: several problems, all their slices in
+    lockstep.  problems is a list of (Instance, intvs, maxits, tol, vinit,
+    filters); tol is taken from the first.  Returns (code, list per problem of
+    per-slice dicts like cheblannr_batch)."""
+    if not problems:
+        return 0, []
+    lib = problems[0][0].lib
+    tol = problems[0][3]
+    nprob = len(problems)
+    ns = [len(p[5]) for p in problems]
+    tot = sum(ns)
+    pevs = (C.POINTER(PevslData) * nprob)(*[p[0].p for p in problems])
+    vecs, keep = [], []
+    for p in problems:
+        v = p[4] if isinstance(p[4], Vector) else Vector(p[0].n, p[4])
+        keep.append(v)
+        vecs.append(C.pointer(v.pv))
+    vin = (C.POINTER(Parvec) * nprob)(*vecs)
+    pols = (Polparams * max(tot, 1))()
+    iv = np.zeros(4 * max(tot, 1))
+    mx = np.zeros(max(tot, 1), np.int32)
+    o = 0
+    for p in problems:
+        for k, f in enumerate(p[5]):
+            pp, mu = _polparams(f)
+            pols[o] = pp
+            keep.append(mu)
+            iv[4 * o:4 * o + 4] = p[1][k]
+            mx[o] = p[2][k]
+            o += 1
+    nsl = np.ascontiguousarray(ns, np.int32)
+    nev = np.zeros(max(tot, 1), np.int32)
+    its = np.zeros(max(tot, 1), np.int32)
+    status = np.zeros(max(tot, 1), np.int32)
+    lam = (_dp * max(tot, 1))()
+    res = (_dp * max(tot, 1))()
+    W = (C.POINTER(Parvecs) * max(tot, 1))()
+    r = lib.pEVSL_B200_ChebLanNrMulti(nprob, pevs, _ptr(nsl, _ip), _ptr(iv), _ptr(mx, _ip), tol,
+                                      vin, pols, _ptr(nev, _ip), lam, W, res, _ptr(its, _ip),
+                                      _ptr(status, _ip), None)
+    outs, o = [], 0
+    for p in problems:
+        per = []
+        for _ in p[5]:
+            m = int(nev[o])
+            d = dict(status=int(status[o]), nev=m, its=int(its[o]))
+            if status[o] == 0:
+                la = np.ctypeslib.as_array(lam[o], shape=(m,)).copy() if m else np.zeros(0)
+                rs = np.ctypeslib.as_array(res[o], shape=(m,)).copy() if m else np.zeros(0)
+                order = np.argsort(la, kind="stable")
+                d["lam"], d["res"] = la[order], rs[order]
+            _free_outputs(lib, lam[o], res[o], W[o])
+            per.append(d)
+            o += 1
+        outs.append(per)
+    for v, p in zip(keep[:nprob], problems):
+        if v is not p[4]:
+            v.free()
     return r, outs
 
 

@@ -18,6 +18,7 @@ namespace pv {
 constexpr int kThreads = 256;      /* block size of the streaming kernels      */
 constexpr int kMaxRedBlocks = 1184; /* 8 x 148 SMs: partial sums per reduction */
 constexpr int kMaxBatch = 16;       /* entries of one batched launch            */
+constexpr int kMaxEntries = 256;    /* entries of one lockstep group / persistent filter */
 
 /* per-entry pointers / scalars of a batched launch (kernel parameters) */
 struct VPtrs {
@@ -68,6 +69,8 @@ enum Ws {
   WS_H,         /* refinement sweep: small projected matrices */
   WS_GEMM,      /* gemm_tn partial tiles                      */
   WS_FILT,      /* batched filter work vectors                */
+  WS_MU,        /* filter coefficients on the device          */
+  WS_GROUP,     /* per-entry coefficient vectors of a group   */
   WS_COUNT
 };
 
@@ -81,6 +84,14 @@ struct Ctx {
   double *dscal = nullptr;     /* S_COUNT device scalars          */
   double *hscal = nullptr;     /* pinned mirror of dscal          */
   int *dflag = nullptr;        /* F_COUNT device flags            */
+  double *gscal = nullptr;     /* 4 * kMaxEntries per-entry device scalars */
+  double *hgscal = nullptr;    /* pinned mirror of gscal          */
+  int *gflag = nullptr;        /* kMaxEntries per-entry device flags       */
+  void *htab = nullptr;        /* pinned staging of the persistent filter table, kTabSlots slots */
+  void *dtab = nullptr;        /* device copies of those tables   */
+  cudaEvent_t tab_ev[4] = {};  /* copy of slot i done             */
+  int tab_next = 0;
+  unsigned *bar = nullptr;     /* grid barrier: count, generation, error   */
   void *ws[WS_COUNT] = {};
   size_t wsz[WS_COUNT] = {};
   uint64_t launches = 0;
@@ -163,31 +174,65 @@ int gemvT(long n, int k, const double *V, long ldv, const double *v, double *w, 
 int gemv_sub_nrm(long n, int k, const double *V, long ldv, const double *w, double *v,
                  double *nrm, const int *run, int *flag_out, double *nrm_old, double eta);
 /* ---------------------------------------------------------------- batched
- * Entry s of every call uses pointer p[s] / scalar v[s]; only entries whose
- * bit is set in mask run.  Per-entry outputs go to out[s]. */
-int b_axpy(long n, int S, CPtrs x, VPtrs y, BScal a, unsigned mask);
-int b_scal(long n, int S, VPtrs x, BScal a, unsigned mask);
-int b_dot(long n, int S, CPtrs x, CPtrs y, double *out, int fin, unsigned mask);
-int b_axpy_dev_nrm2(long n, int S, const double *coef, CPtrs x, VPtrs y, double *nrm,
+ * Entry s of every call uses pointer p[s] / scalar v[s] and length
+ * len.n[s] (leading dimension len.ld[s] for basis blocks); only entries
+ * whose bit is set in mask run.  Per-entry outputs go to out[s]. */
+struct BLen {
+  long n[kMaxBatch];
+  long ld[kMaxBatch];
+};
+BLen blen_uniform(long n, long ld, int S);
+int b_axpy(const BLen &len, int S, CPtrs x, VPtrs y, BScal a, unsigned mask);
+int b_scal(const BLen &len, int S, VPtrs x, BScal a, unsigned mask);
+int b_dot(const BLen &len, int S, CPtrs x, CPtrs y, double *out, int fin, unsigned mask);
+int b_axpy_dev_nrm2(const BLen &len, int S, const double *coef, CPtrs x, VPtrs y, double *nrm,
                     unsigned mask);
 /* w[s*ldw + j] = <V_s(:,j), v_s>, j < k */
-int b_gemvT(long n, int S, int k, CPtrs V, long ldv, CPtrs v, double *w, long ldw, const int *run,
+int b_gemvT(const BLen &len, int S, int k, CPtrs V, CPtrs v, double *w, long ldw, const int *run,
             unsigned mask);
 /* v_s -= V_s w_s; nrm[s] = ||v_s||; flag/nrm_old per entry as gemv_sub_nrm */
-int b_gemv_sub_nrm(long n, int S, int k, CPtrs V, long ldv, const double *w, long ldw, VPtrs v,
+int b_gemv_sub_nrm(const BLen &len, int S, int k, CPtrs V, const double *w, long ldw, VPtrs v,
                    double *nrm, const int *run, int *flag_out, double *nrm_old, double eta,
                    unsigned mask);
-/* one filter degree (SRC/chebpol.c:538-568) for nb <= kMaxBatch independent
- * vectors, one matrix read serving all: entry e's pointers are FP64 vectors,
- * or FP32 ones when fp32 (then the last degree sets yout, the FP64 result) */
+/* one filter degree (SRC/chebpol.c:538-568) for nb <= kMaxEntries
+ * independent vectors, each on its own matrix A (entries on one matrix read
+ * it once per launch): entry e's pointers are FP64 vectors, or FP32 ones
+ * when fp32 (then the last degree sets yout, the FP64 result) */
 struct ChebEntry {
+  const pevsl_devcsr *A;
   const void *vk, *vkm1; /* vkm1 NULL at the first degree */
   void *vkp1, *y;        /* vkp1 may alias vkm1 */
   double *yout;
   double cc, t, mu0, muk;
   int first;
 };
-int cheb_step_batch(const pevsl_devcsr *A, int nb, const ChebEntry *e, bool fp32);
+int cheb_step_batch(int nb, const ChebEntry *e, bool fp32);
+
+/* One entry of the persistent filter: y = p(A) x for its own matrix and
+ * polynomial (mu on the device).  FP64 entries: b0, b1 are two work vectors
+ * of n doubles and acc == y.  FP32 entries (a = the FP32 values): x is the
+ * FP32 copy of the input, b0, b1, acc are FP32 and the last degree writes
+ * y in FP64. */
+struct FiltDev {
+  const int *ia, *ja;
+  const void *a;
+  int n, deg, fp32, pad;
+  double cc, t1, t2;
+  const double *mu;
+  const void *x;
+  void *b0, *b1, *acc;
+  double *y;
+};
+constexpr size_t kFiltTabBytes = sizeof(FiltDev) * kMaxEntries + sizeof(int) * (kMaxEntries + 8);
+constexpr int kTabSlots = 4; /* staging slots: a slot is reused only after its copy ran */
+/* All degrees of ne <= kMaxEntries filters in one cooperative launch: the
+ * blocks sweep the (entry, 256-row block) items of every entry whose degree
+ * has not been reached, then meet at a grid barrier before the next degree.
+ * The entries must be sorted by non-increasing degree.  Returns 0,
+ * PEVSL_ERR_CUDA, or PEVSL_ERR_ARG if the launch cannot be co-resident. */
+int cheb_filter_persistent(int ne, const FiltDev *entries, int maxdeg);
+/* the barrier's timeout flag of the last persistent filter (read after a sync) */
+int persistent_filter_error();
 
 /* ---------------------------------------------------------------- FP32 (mixed) */
 int csr_make_fp32(pevsl_devcsr *A); /* FP32 copy of the values, once */

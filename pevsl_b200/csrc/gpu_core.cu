@@ -64,6 +64,22 @@ int ensure() {
     return PEVSL_ERR_CUDA;
   if (fail(cudaMalloc(&g_ctx.dflag, sizeof(int) * F_COUNT), "cudaMalloc flag")) return PEVSL_ERR_CUDA;
   if (fail(cudaMemset(g_ctx.dflag, 0, sizeof(int) * F_COUNT), "cudaMemset flag")) return PEVSL_ERR_CUDA;
+  if (fail(cudaMalloc(&g_ctx.gscal, sizeof(double) * 4 * kMaxEntries), "cudaMalloc gscal"))
+    return PEVSL_ERR_CUDA;
+  if (fail(cudaMallocHost(&g_ctx.hgscal, sizeof(double) * 4 * kMaxEntries), "cudaMallocHost"))
+    return PEVSL_ERR_CUDA;
+  if (fail(cudaMalloc(&g_ctx.gflag, sizeof(int) * kMaxEntries), "cudaMalloc gflag"))
+    return PEVSL_ERR_CUDA;
+  if (fail(cudaMemset(g_ctx.gflag, 0, sizeof(int) * kMaxEntries), "cudaMemset gflag"))
+    return PEVSL_ERR_CUDA;
+  if (fail(cudaMallocHost(&g_ctx.htab, kFiltTabBytes * kTabSlots), "cudaMallocHost tab"))
+    return PEVSL_ERR_CUDA;
+  if (fail(cudaMalloc(&g_ctx.dtab, kFiltTabBytes * kTabSlots), "cudaMalloc tab")) return PEVSL_ERR_CUDA;
+  for (int i = 0; i < kTabSlots; i++)
+    if (fail(cudaEventCreateWithFlags(&g_ctx.tab_ev[i], cudaEventDisableTiming), "cudaEventCreate"))
+      return PEVSL_ERR_CUDA;
+  if (fail(cudaMalloc(&g_ctx.bar, sizeof(unsigned) * 4), "cudaMalloc bar")) return PEVSL_ERR_CUDA;
+  if (fail(cudaMemset(g_ctx.bar, 0, sizeof(unsigned) * 4), "cudaMemset bar")) return PEVSL_ERR_CUDA;
   g_ctx.ready = true;
   return 0;
 }

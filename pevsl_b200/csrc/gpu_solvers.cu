@@ -22,6 +22,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <vector>
+
 #include "gpu.cuh"
 #include "gpu_device.cuh"
 
@@ -74,6 +76,7 @@ SegTimer g_t_pol, g_t_orth;
 
 /* process-wide counters of the fused filter kernel (pEVSL_B200_FilterCounters) */
 uint64_t g_filter_launches = 0;
+uint64_t g_filter_persistent = 0; /* persistent filter launches (each covers many degrees) */
 double g_filter_bytes = 0.0;
 double g_filter_ms = 0.0;
 
@@ -137,75 +140,177 @@ int cheb_apply(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, d
   return 0;
 }
 
-/* y_e = p_e(A) x_e for ne <= kMaxBatch entries on the device CSR
- * (pEVSL_ChebAv, SRC/chebpol.c:509-574, for all entries at once): one
- * cheb_step_batch launch per degree serves every entry whose filter degree
- * has not been reached, so the matrix is read once per degree.  work holds
- * 16 n bytes per entry: two FP64 recurrence vectors, or, when fp32, the
- * FP32 copy of x_e, two FP32 recurrence vectors and the FP32 accumulator
- * (the last degree writes y_e in FP64).  In FP64 every entry gets the bits
- * of cheb_apply. */
+/* One filter application of a batch: y = p(A) x (pEVSL_ChebAv,
+ * SRC/chebpol.c:509-574) for entry e with its own device CSR, polynomial
+ * and work space of 16 * ld bytes (two FP64 recurrence vectors, or, in
+ * FP32, the FP32 copy of x, two FP32 recurrence vectors and the FP32
+ * accumulator; the last degree writes y in FP64). */
 struct FilterJob {
+  pevsl_Data *pevsl;          /* statistics */
+  const pevsl_devcsr *A;
   const double *x;
   double *y;
   const pevsl_Polparams *pol;
+  const double *dmu;          /* pol->mu on the device (persistent form) */
+  void *work;
+  long ld;                    /* spacing of the work vectors: >= n, 256-byte multiple */
 };
 
-static int cheb_filter_batch(pevsl_Data *pevsl, const pevsl_devcsr *A, int ne,
-                             const FilterJob *jobs, void *work, bool fp32) {
-  const long n = A->nrows;
+/* Form of the batched filter: 0 = one cheb_step_batch launch per degree
+ * serving every entry (any matrices, up to kMaxEntries), 1 = one persistent
+ * cooperative launch for all degrees and entries.  One launch per degree is
+ * the default: measured faster (81 vs 119 us per degree for 4 slices at
+ * 10^6 rows, 4.1 vs 6.1 us at 8000 rows), the grid barrier costing more
+ * than the gap between launches. */
+static int g_filter_form_override = -1; /* -1: not read yet, 2: automatic */
+static int filter_form() {
+  if (g_filter_form_override < 0) {
+    const char *e = getenv("PEVSL_B200_FILTER_FORM");
+    g_filter_form_override = e ? atoi(e) : 2;
+  }
+  return g_filter_form_override == 1 ? 1 : 0;
+}
+
+static double filter_bytes_degree(const pevsl_devcsr *A, int deg_k, bool fp32, bool last) {
+  const double n = A->nrows, vb = fp32 ? 4.0 : 8.0;
+  return (deg_k == 1 ? 3.0 : 5.0) * vb * n + (last ? 4.0 * n : 0.0);
+}
+
+static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
   if (ne <= 0) return 0;
-  if (ne > kMaxBatch) return PEVSL_ERR_ARG;
-  if (fp32 && !A->a32) return PEVSL_ERR_ARG;
-  const void *vk[kMaxBatch], *vkm1[kMaxBatch];
-  void *buf[kMaxBatch][2], *acc[kMaxBatch];
-  int maxdeg = 0, st = 0;
+  if (ne > kMaxEntries) return PEVSL_ERR_ARG;
+  int st = 0, maxdeg = 0, nlive = 0;
+  bool one_matrix = true;
+  long rows = 0;
+  int live[kMaxEntries];
   for (int e = 0; e < ne && !st; e++) {
-    const pevsl_Polparams *pol = jobs[e].pol;
-    pevsl->stats->n_polAv++;
-    pevsl->stats->n_mvA += (size_t)PEVSL_MAX(pol->deg, 0);
+    const FilterJob &J = jobs[e];
+    const pevsl_Polparams *pol = J.pol;
+    const long n = J.A->nrows;
+    if (fp32 && !J.A->a32) return PEVSL_ERR_ARG;
+    J.pevsl->stats->n_polAv++;
+    J.pevsl->stats->n_mvA += (size_t)PEVSL_MAX(pol->deg, 0);
     if (pol->deg <= 0) {
-      st = vcopy(jobs[e].x, jobs[e].y, n);
-      if (!st) st = vscal(jobs[e].y, n, pol->mu[0]);
+      st = vcopy(J.x, J.y, n);
+      if (!st) st = vscal(J.y, n, pol->mu[0]);
       continue;
     }
+    if (J.A != jobs[0].A) one_matrix = false;
     maxdeg = PEVSL_MAX(maxdeg, pol->deg);
-    if (fp32) {
-      float *w = (float *)work + 4 * (size_t)n * e;
-      st = cvt_f64_f32(n, jobs[e].x, w);
-      vk[e] = w;
-      buf[e][0] = w + n;
-      buf[e][1] = w + 2 * n;
-      acc[e] = w + 3 * n;
-    } else {
-      double *w = (double *)work + 2 * (size_t)n * e;
-      vk[e] = jobs[e].x;
-      buf[e][0] = w;
-      buf[e][1] = w + n;
-      acc[e] = jobs[e].y;
-    }
-    vkm1[e] = nullptr;
+    rows += n;
+    if (fp32) st = cvt_f64_f32(n, J.x, (float *)J.work);
+    live[nlive++] = e;
   }
-  const double mat_bytes = (fp32 ? 8.0 : 12.0) * (double)A->nnz + 4.0 * (n + 1.0);
-  const double vb = fp32 ? 4.0 : 8.0;
-  for (int k = 1; k <= maxdeg && !st; k++) {
-    ChebEntry en[kMaxBatch];
-    int nb = 0;
+  if (st || !nlive) return st;
+  (void)one_matrix;
+  (void)rows;
+  /* matrix bytes: each distinct matrix once per degree, up to the largest
+   * degree of its entries */
+  double mat_bytes = 0.0;
+  for (int i = 0; i < nlive; i++) {
+    const pevsl_devcsr *A = jobs[live[i]].A;
+    bool seen = false;
+    for (int t = 0; t < i && !seen; t++) seen = jobs[live[t]].A == A;
+    if (seen) continue;
+    int dmax = 0;
+    for (int t = i; t < nlive; t++)
+      if (jobs[live[t]].A == A) dmax = PEVSL_MAX(dmax, jobs[live[t]].pol->deg);
+    mat_bytes += (double)dmax * ((fp32 ? 8.0 : 12.0) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
+  }
+  const int form = filter_form();
+  if (form == 1) {
+    /* table sorted by non-increasing degree (stable: ties keep their order) */
+    FiltDev tab[kMaxEntries];
+    int ord[kMaxEntries];
+    for (int i = 0; i < nlive; i++) ord[i] = live[i];
+    for (int i = 1; i < nlive; i++) {
+      const int v = ord[i];
+      int j = i - 1;
+      while (j >= 0 && jobs[ord[j]].pol->deg < jobs[v].pol->deg) {
+        ord[j + 1] = ord[j];
+        j--;
+      }
+      ord[j + 1] = v;
+    }
     double bytes = mat_bytes;
-    for (int e = 0; e < ne; e++) {
-      const pevsl_Polparams *pol = jobs[e].pol;
+    for (int i = 0; i < nlive; i++) {
+      const FilterJob &J = jobs[ord[i]];
+      const pevsl_devcsr *A = J.A;
+      FiltDev &E = tab[i];
+      E.ia = A->ia;
+      E.ja = A->ja;
+      E.a = fp32 ? (const void *)A->a32 : (const void *)A->a;
+      E.n = (int)A->nrows;
+      E.deg = J.pol->deg;
+      E.fp32 = fp32;
+      E.pad = 0;
+      E.cc = J.pol->cc;
+      E.t1 = 1.0 / J.pol->dd;
+      E.t2 = 2.0 / J.pol->dd;
+      E.mu = J.dmu;
+      if (fp32) {
+        float *w = (float *)J.work;
+        E.x = w;
+        E.b0 = w + J.ld;
+        E.b1 = w + 2 * J.ld;
+        E.acc = w + 3 * J.ld;
+      } else {
+        double *w = (double *)J.work;
+        E.x = J.x;
+        E.b0 = w;
+        E.b1 = w + J.ld;
+        E.acc = J.y;
+      }
+      E.y = J.y;
+      for (int k = 1; k <= E.deg; k++) bytes += filter_bytes_degree(A, k, fp32, fp32 && k == E.deg);
+    }
+    st = cheb_filter_persistent(nlive, tab, maxdeg);
+    g_filter_launches += (uint64_t)maxdeg;
+    g_filter_bytes += bytes;
+    g_filter_persistent++;
+    return st;
+  }
+  /* one launch per degree for all live entries; a matrix is read once per
+   * launch for all entries on it */
+  std::vector<const void *> vk(nlive), vkm1(nlive);
+  std::vector<void *> b0(nlive), b1(nlive), acc(nlive);
+  for (int i = 0; i < nlive; i++) {
+    const FilterJob &J = jobs[live[i]];
+    if (fp32) {
+      float *w = (float *)J.work;
+      vk[i] = w;
+      b0[i] = w + J.ld;
+      b1[i] = w + 2 * J.ld;
+      acc[i] = w + 3 * J.ld;
+    } else {
+      double *w = (double *)J.work;
+      vk[i] = J.x;
+      b0[i] = w;
+      b1[i] = w + J.ld;
+      acc[i] = J.y;
+    }
+    vkm1[i] = nullptr;
+  }
+  g_filter_bytes += mat_bytes;
+  std::vector<ChebEntry> en(nlive);
+  for (int k = 1; k <= maxdeg && !st; k++) {
+    int nb = 0;
+    double bytes = 0.0;
+    for (int i = 0; i < nlive; i++) {
+      const FilterJob &J = jobs[live[i]];
+      const pevsl_Polparams *pol = J.pol;
       if (k > pol->deg) continue;
       /* two work vectors: from degree 3 on, v_{k+1} replaces v_{k-1} */
-      void *vkp1 = k <= 2 ? buf[e][k - 1] : const_cast<void *>(vkm1[e]);
+      void *vkp1 = k == 1 ? b0[i] : k == 2 ? b1[i] : const_cast<void *>(vkm1[i]);
       const bool last = fp32 && k == pol->deg;
-      en[nb++] = ChebEntry{vk[e], vkm1[e], vkp1, acc[e], last ? jobs[e].y : nullptr,
+      en[nb++] = ChebEntry{J.A, vk[i], vkm1[i], vkp1, acc[i], last ? J.y : nullptr,
                            pol->cc, (k == 1 ? 1.0 : 2.0) / pol->dd, pol->mu[0], pol->mu[k],
                            k == 1};
-      bytes += (k == 1 ? 3.0 : 5.0) * vb * (double)n + (last ? 4.0 * (double)n : 0.0);
-      vkm1[e] = vk[e];
-      vk[e] = vkp1;
+      bytes += filter_bytes_degree(J.A, k, fp32, last);
+      vkm1[i] = vk[i];
+      vk[i] = vkp1;
     }
-    st = cheb_step_batch(A, nb, en, fp32);
+    st = cheb_step_batch(nb, en.data(), fp32);
     g_filter_launches++;
     g_filter_bytes += bytes;
   }
@@ -246,6 +351,7 @@ void pEVSL_B200_FilterCounters(uint64_t *launches, double *bytes, double *ms) {
 
 void pEVSL_B200_ResetFilterCounters(void) {
   g_filter_launches = 0;
+  g_filter_persistent = 0;
   g_filter_bytes = 0.0;
   g_filter_ms = 0.0;
 }
@@ -757,10 +863,14 @@ int pEVSL_LanTrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pevsl_
  * exactly the reference's sequence of operations. */
 
 struct SliceState {
-  /* inputs */
+  /* inputs: the slice and the problem it belongs to */
   double intv[4];
   const pevsl_Polparams *pol;
   int maxit;
+  pevsl_Data *pevsl;
+  pevsl_devcsr *A; /* built-in device CSR, or NULL for a user matvec */
+  pevsl_Parvec *vinit;
+  long n, ld;
   /* state */
   double *V;      /* basis, ld x (maxit+1) */
   double *dT, *eT, *EvalT;
@@ -886,8 +996,12 @@ static int ritz_refine(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, lo
   int *sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
   if (!sel) return PEVSL_ERR_NOMEM;
   if (kdim > 0 && pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) st = PEVSL_ERR_EIG;
-  for (int i = 0; i < count && kdim > 0 && !st; i++)
+  int nbar = 0; /* Ritz values of p(A) above bar: the FP64 path's candidates */
+  for (int i = 0; i < count && kdim > 0 && !st; i++) {
     if (S->EvalT[i] >= guard * bar) sel[m++] = i;
+    if (S->EvalT[i] >= bar) nbar++;
+  }
+  S->short_pairs = nbar;
   S->Lam = (double *)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
   S->res = (double *)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1));
   S->Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
@@ -907,10 +1021,12 @@ static int ritz_refine(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, lo
   double *P = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)ld * m);
   double *W = (double *)ws(WS_REF1, sizeof(double) * (size_t)ld * m);
   double *X = (double *)ws(WS_REF2, sizeof(double) * (size_t)ld * m);
-  void *fwork = ws(WS_FILT, 16 * (size_t)n * kMaxBatch);
+  void *fwork = ws(WS_FILT, 16 * (size_t)ld * kMaxBatch);
+  double *dmu = (double *)ws(WS_MU, sizeof(double) * (size_t)(S->pol->deg + 1));
+  if (dmu && memcpy_async(dmu, S->pol->mu, sizeof(double) * (size_t)(S->pol->deg + 1))) dmu = nullptr;
   /* small device matrices: Y | G | H | Z | 3 m scalars */
   double *dsm = (double *)ws(WS_H, sizeof(double) * ((size_t)kdim * m + 3 * mm + 3 * (size_t)m));
-  if (!Y || !Hh || !Zh || !lam || !hv || !U || !P || !W || !X || !fwork || !dsm)
+  if (!Y || !Hh || !Zh || !lam || !hv || !U || !P || !W || !X || !fwork || !dsm || !dmu)
     st = PEVSL_ERR_NOMEM;
   double *dY = dsm, *dG = dY + (size_t)kdim * m, *dH = dG + mm, *dZ = dH + mm, *dv = dZ + mm;
   if (!st && pevsl_tridiag_eig_sel(kdim, S->dT, S->eT, S->EvalT, m, sel, Y)) st = PEVSL_ERR_EIG;
@@ -933,8 +1049,9 @@ static int ritz_refine(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, lo
       const int cs = PEVSL_MIN(kMaxBatch, m - c0);
       FilterJob jobs[kMaxBatch];
       for (int e = 0; e < cs; e++)
-        jobs[e] = FilterJob{src + (size_t)(c0 + e) * ld, dst + (size_t)(c0 + e) * ld, S->pol};
-      st = cheb_filter_batch(pevsl, A, cs, jobs, fwork, false);
+        jobs[e] = FilterJob{pevsl, A, src + (size_t)(c0 + e) * ld, dst + (size_t)(c0 + e) * ld,
+                            S->pol, dmu, (char *)fwork + 16 * (size_t)ld * e, ld};
+      st = cheb_filter_batch(cs, jobs, false);
     }
     if (!st) st = vdot_cols(n, m, dst, ld, dst, ld, dv);
     if (!st) st = memcpy_async(hv, dv, sizeof(double) * m);
@@ -999,9 +1116,10 @@ static int ritz_refine(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, lo
     /* a refined pair in [a, b] short of the FP64 path's quality (residual
      * below tol, and below tol * |lam| for |lam| < 1) sends the slice back
      * to FP64 */
-    S->short_pairs = 0;
+    int weak = 0;
     for (int j = 0; j < q; j++)
-      if (!(sqrt(hv[j]) < tol * PEVSL_MIN(1.0, fabs(lam[j])))) S->short_pairs++;
+      if (!(sqrt(hv[j]) < tol * PEVSL_MIN(1.0, fabs(lam[j])))) weak++;
+    S->short_pairs = PEVSL_MAX(weak, nbar - S->nev);
     if (getenv("PEVSL_B200_VERBOSE"))
       fprintf(stderr, "refine [%g, %g]: kdim %d, subspace %d, in [a,b] %d, accepted %d, res %.2e..%.2e\n",
               aa, bb, kdim, m, q, S->nev, rmin, rmax);
@@ -1034,14 +1152,34 @@ static int g_fallbacks = 0; /* slices of the last call re-run in FP64 */
 
 int pEVSL_B200_LastFallbacks(void) { return g_fallbacks; }
 
-static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol,
-                           pevsl_Parvec *vinit, FILE *fstats, bool allow_mixed = true) {
+int pEVSL_B200_SetFilterForm(int form) {
+  if (form < -1 || form > 1) return PEVSL_ERR_ARG;
+  g_filter_form_override = form < 0 ? 2 : form;
+  return 0;
+}
+
+/* Filtered Lanczos in lockstep (pEVSL_ChebLanNr, SRC/cheblanNr.c:54-448) for
+ * ns <= kMaxEntries slices, which may belong to different problems (each
+ * entry carries its instance, matrix, length and start vector).  Every
+ * step runs one filter application for all active slices (one launch per
+ * degree, or one persistent launch), then the Lanczos recurrence and
+ * CGS-DGKS as batched launches of up to kMaxBatch entries.  Per entry the
+ * work decomposition is that of a one-slice run, so each slice's result is
+ * bit-identical to solving it alone. */
+static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
+                           bool allow_mixed = true) {
   Ctx &c = ctx();
-  const int N = pevsl->N;
-  const long n = pevsl->n, ld = round_ld(n);
-  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
-  const bool mixed = allow_mixed && A && pevsl_inst_of(pevsl)->precision == PEVSL_PREC_MIXED;
-  const bool batched = A && (ns > 1 || mixed);
+  if (ns <= 0) return 0;
+  if (ns > kMaxEntries) return PEVSL_ERR_ARG;
+  const bool mixed = allow_mixed && SL[0].A &&
+                     pevsl_inst_of(SL[0].pevsl)->precision == PEVSL_PREC_MIXED;
+  bool all_builtin = true;
+  long nmax = 0;
+  for (int s = 0; s < ns; s++) {
+    all_builtin = all_builtin && SL[s].A != nullptr;
+    nmax = PEVSL_MAX(nmax, SL[s].n);
+  }
+  const bool batched = all_builtin && (ns > 1 || mixed);
   /* mixed form: trace tolerance per converged value, and the guard of the
    * refinement sweep (PEVSL_B200_MIXED_TRTOL / PEVSL_B200_MIXED_GUARD) */
   double trtol_mixed = 1e-9, guard = 0.3;
@@ -1049,14 +1187,16 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
   if (getenv("PEVSL_B200_MIXED_TRTOL")) trtol_mixed = atof(getenv("PEVSL_B200_MIXED_TRTOL"));
   if (getenv("PEVSL_B200_MIXED_GUARD")) guard = atof(getenv("PEVSL_B200_MIXED_GUARD"));
   if (getenv("PEVSL_B200_MIXED_PASSES")) passes = PEVSL_MAX(1, atoi(getenv("PEVSL_B200_MIXED_PASSES")));
-  unsigned act = 0;
-  size_t basis_cols = 0;
+  std::vector<char> act(ns, 0);
+  int nact = 0;
+  size_t basis_elems = 0, work_bytes = 0, mu_elems = 0;
   for (int s = 0; s < ns; s++) {
     SliceState *S = &SL[s];
-    S->maxit = PEVSL_MIN(N, S->maxit);
+    S->maxit = PEVSL_MIN(S->pevsl->N, S->maxit);
     S->status = 0;
     S->nev = 0;
     S->its = 0;
+    S->short_pairs = 0;
     if (pevsl_check_intv(S->intv, fstats) < 0) {
       S->done = 1; /* invalid interval: no pairs, status 0 (SRC/cheblanNr.c:96-100) */
       continue;
@@ -1073,164 +1213,243 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
       continue;
     }
     if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
-    act |= 1u << s;
-    basis_cols += (size_t)S->maxit + 1;
+    act[s] = 1;
+    nact++;
+    basis_elems += (size_t)S->ld * ((size_t)S->maxit + 1);
+    work_bytes += 16 * (size_t)S->ld;
+    mu_elems += (size_t)S->pol->deg + 1;
   }
-  if (!act) return 0;
-  /* bases of all active slices in one workspace */
-  double *Vall = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * basis_cols);
-  /* three FP64 vectors (single-slice filter, breakdown restarts), then the
-   * batched filter's 16 n bytes per slice */
-  const size_t w3_bytes = sizeof(double) * 3 * (size_t)n + (batched ? 16 * (size_t)n * ns : 0);
-  double *w3 = (double *)ws(WS_CHEB, w3_bytes);
-  if (mixed && csr_make_fp32(A)) return PEVSL_ERR_NOMEM;
-  double *vrand = (double *)ws(A ? WS_VEC : WS_RITZ2, sizeof(double) * (size_t)n);
-  if (!Vall || !w3 || !vrand) return PEVSL_ERR_NOMEM;
-  void *bwork = w3 + 3 * (size_t)n;
+  if (!nact) return 0;
+  if (mixed)
+    for (int s = 0; s < ns; s++)
+      if (act[s] && csr_make_fp32(SL[s].A)) return PEVSL_ERR_NOMEM;
+  /* bases of all active slices in one workspace; three FP64 vectors for
+   * the one-slice filter and breakdown restarts; 16 ld bytes of batched
+   * filter work per slice; the filter coefficients on the device */
+  double *Vall = (double *)ws(WS_BASIS, sizeof(double) * basis_elems);
+  double *w3 = (double *)ws(WS_CHEB, sizeof(double) * 3 * (size_t)nmax + (batched ? work_bytes : 0));
+  double *vrand = (double *)ws(all_builtin ? WS_VEC : WS_RITZ2, sizeof(double) * (size_t)nmax);
+  double *dmu_all = batched ? (double *)ws(WS_MU, sizeof(double) * mu_elems) : nullptr;
+  if (!Vall || !w3 || !vrand || (batched && !dmu_all)) return PEVSL_ERR_NOMEM;
+  char *bwork = (char *)(w3 + 3 * (size_t)nmax);
+  std::vector<char *> work(ns, nullptr);
+  std::vector<const double *> dmu(ns, nullptr);
   int st = 0;
-  size_t off = 0;
-  for (int s = 0; s < ns; s++) {
+  size_t off = 0, woff = 0, moff = 0;
+  int maxit_all = 0;
+  for (int s = 0; s < ns && !st; s++) {
     SliceState *S = &SL[s];
-    if (!((act >> s) & 1u)) continue;
-    S->V = Vall + off * (size_t)ld;
-    off += (size_t)S->maxit + 1;
+    if (!act[s]) continue;
+    S->V = Vall + off;
+    off += (size_t)S->ld * ((size_t)S->maxit + 1);
+    if (batched) {
+      work[s] = bwork + woff;
+      woff += 16 * (size_t)S->ld;
+      dmu[s] = dmu_all + moff;
+      st = memcpy_async(dmu_all + moff, S->pol->mu, sizeof(double) * ((size_t)S->pol->deg + 1));
+      moff += (size_t)S->pol->deg + 1;
+    }
     S->dT = (double *)malloc(sizeof(double) * (size_t)S->maxit);
     S->eT = (double *)malloc(sizeof(double) * (size_t)S->maxit);
     S->EvalT = (double *)malloc(sizeof(double) * (size_t)S->maxit);
     if (!S->dT || !S->eT || !S->EvalT) return PEVSL_ERR_NOMEM;
     S->wn = S->tr0 = S->beta = 0.0;
     S->nwn = S->kdim = S->count = S->nconv = 0;
+    maxit_all = PEVSL_MAX(maxit_all, S->maxit);
   }
+  if (st) return st;
   SegTimer &t_pol = g_t_pol, &t_orth = g_t_orth;
-  /* y_s = p_s(A) x_s for the slices in mask: x_s = V_s(:,k) (or xin for
-   * all), y_s = V_s(:,k+1) (or column 0) */
-  auto filter = [&](unsigned mask, int kin, const double *xin, int kout) -> int {
+  /* y_s = p_s(A_s) x_s for the slices with sel[s]: x_s = V_s(:,kin) (or the
+   * slice's start vector when xin), y_s = V_s(:,kout) */
+  auto filter = [&](const std::vector<char> &sel, int kin, bool xin, int kout) -> int {
     t_pol.begin();
     int r = 0;
     if (!batched) {
       for (int s = 0; s < ns && !r; s++)
-        if ((mask >> s) & 1u)
-          r = cheb_apply(pevsl, SL[s].pol, xin ? xin : SL[s].V + (size_t)kin * ld,
-                         SL[s].V + (size_t)kout * ld, w3, n);
+        if (sel[s])
+          r = cheb_apply(SL[s].pevsl, SL[s].pol,
+                         xin ? SL[s].vinit->data : SL[s].V + (size_t)kin * SL[s].ld,
+                         SL[s].V + (size_t)kout * SL[s].ld, w3, SL[s].n);
     } else {
-      /* one matrix read per degree for every slice in mask; mixed: FP32 */
-      FilterJob jobs[kMaxBatch];
-      int ne = 0;
+      std::vector<FilterJob> jobs;
+      jobs.reserve(ns);
       for (int s = 0; s < ns; s++)
-        if ((mask >> s) & 1u)
-          jobs[ne++] = FilterJob{xin ? xin : SL[s].V + (size_t)kin * ld,
-                                 SL[s].V + (size_t)kout * ld, SL[s].pol};
-      r = cheb_filter_batch(pevsl, A, ne, jobs, bwork, mixed);
+        if (sel[s])
+          jobs.push_back(FilterJob{SL[s].pevsl, SL[s].A,
+                                   xin ? SL[s].vinit->data : SL[s].V + (size_t)kin * SL[s].ld,
+                                   SL[s].V + (size_t)kout * SL[s].ld, SL[s].pol, dmu[s], work[s],
+                                   SL[s].ld});
+      r = cheb_filter_batch((int)jobs.size(), jobs.data(), mixed);
     }
     t_pol.end();
     return r;
   };
-  if (A) l2_window(A->a, A->bytes);
+  /* a batched operation over the active entries, kMaxBatch at a time:
+   * op(first entry, count, mask, lengths) */
+  auto chunks = [&](const std::vector<char> &sel, auto &&op) -> int {
+    for (int c0 = 0; c0 < ns; c0 += kMaxBatch) {
+      const int cs = PEVSL_MIN(kMaxBatch, ns - c0);
+      unsigned mask = 0;
+      BLen len{};
+      for (int i = 0; i < cs; i++) {
+        len.n[i] = SL[c0 + i].n;
+        len.ld[i] = SL[c0 + i].ld;
+        if (sel[c0 + i]) mask |= 1u << i;
+      }
+      if (!mask) continue;
+      const int r = op(c0, cs, mask, len);
+      if (r) return r;
+    }
+    return 0;
+  };
+  /* per-entry device scalars: alpha, ||v|| before CGS, ||v|| after, and the
+   * DGKS flag */
+  double *dA = c.gscal, *dN0 = c.gscal + kMaxEntries, *dN = c.gscal + 2 * kMaxEntries;
+  double *hA = c.hgscal, *hN = c.hgscal + 2 * kMaxEntries;
+  int *dF = c.gflag;
+  const long ldw = maxit_all + 1;
+  double *dW = (double *)ws(WS_GROUP, sizeof(double) * (size_t)ns * (size_t)ldw);
+  if (!dW) return PEVSL_ERR_NOMEM;
+  for (int s = 0; s < ns; s++)
+    if (act[s] && SL[s].A) l2_window(SL[s].A->a, SL[s].A->bytes);
   cudaEvent_t e_all0, e_all1;
   cudaEventCreate(&e_all0);
   cudaEventCreate(&e_all1);
   cudaEventRecord(e_all0, c.stream);
   /* filter the start vector, normalise (SRC/cheblanNr.c:164-194) */
-  st = filter(act, 0, vinit->data, 0);
-  {
-    CPtrs x{};
-    for (int s = 0; s < ns; s++) x.p[s] = SL[s].V;
-    if (!st) st = b_dot(n, ns, x, x, c.dscal + 16, FIN_SQRT, act);
-    const double *h = st ? nullptr : fetch_scalars(16, ns);
-    if (!h) st = st ? st : PEVSL_ERR_CUDA;
-    BScal inv{};
-    VPtrs y{};
-    for (int s = 0; s < ns && !st; s++) {
-      inv.v[s] = 1.0 / h[s];
-      y.p[s] = SL[s].V;
-    }
-    if (!st) st = b_scal(n, ns, y, inv, act);
-  }
-  double *dA = c.dscal + 16, *dN0 = c.dscal + 32, *dN = c.dscal + 48;
-  int *dF = c.dflag;
-  double *dW = (double *)ws(WS_SMALL, sizeof(double) * kMaxBatch * (size_t)(off + 1));
-  if (!dW) st = PEVSL_ERR_NOMEM;
+  st = filter(act, 0, true, 0);
+  if (!st)
+    st = chunks(act, [&](int c0, int cs, unsigned mask, const BLen &len) {
+      CPtrs x{};
+      for (int i = 0; i < cs; i++) x.p[i] = SL[c0 + i].V;
+      return b_dot(len, cs, x, x, dA + c0, FIN_SQRT, mask);
+    });
+  if (!st) st = memcpy_async(hA, dA, sizeof(double) * (size_t)ns);
+  if (!st) st = sync();
+  if (!st)
+    st = chunks(act, [&](int c0, int cs, unsigned mask, const BLen &len) {
+      BScal inv{};
+      VPtrs y{};
+      for (int i = 0; i < cs; i++) {
+        inv.v[i] = 1.0 / hA[c0 + i];
+        y.p[i] = SL[c0 + i].V;
+      }
+      return b_scal(len, cs, y, inv, mask);
+    });
   int k;
-  for (k = 0; act && !st; k++) {
-    CPtrs vprev{}, vk{}, vks{}, Vc{};
-    VPtrs vnew{};
-    BScal mb{};
-    for (int s = 0; s < ns; s++) {
-      if (!((act >> s) & 1u)) continue;
-      SliceState *S = &SL[s];
-      vk.p[s] = S->V + (size_t)k * ld;
-      vnew.p[s] = S->V + (size_t)(k + 1) * ld;
-      vks.p[s] = vnew.p[s];
-      Vc.p[s] = S->V;
-      if (k > 0) vprev.p[s] = S->V + (size_t)(k - 1) * ld;
-      mb.v[s] = -S->beta;
-    }
-    st = filter(act, k, nullptr, k + 1);
-    if (!st && k > 0) st = b_axpy(n, ns, vprev, vnew, mb, act);
-    if (!st) st = b_dot(n, ns, vk, vks, dA, FIN_ID, act);
+  for (k = 0; nact > 0 && !st; k++) {
+    st = filter(act, k, false, k + 1);
+    auto col = [&](int s, int j) { return SL[s].V + (size_t)j * SL[s].ld; };
+    if (!st && k > 0)
+      st = chunks(act, [&](int c0, int cs, unsigned mask, const BLen &len) {
+        CPtrs vprev{};
+        VPtrs vnew{};
+        BScal mb{};
+        for (int i = 0; i < cs; i++) {
+          vprev.p[i] = col(c0 + i, k - 1);
+          vnew.p[i] = col(c0 + i, k + 1);
+          mb.v[i] = -SL[c0 + i].beta;
+        }
+        return b_axpy(len, cs, vprev, vnew, mb, mask);
+      });
+    if (!st)
+      st = chunks(act, [&](int c0, int cs, unsigned mask, const BLen &len) {
+        CPtrs vk{}, vks{};
+        for (int i = 0; i < cs; i++) {
+          vk.p[i] = col(c0 + i, k);
+          vks.p[i] = col(c0 + i, k + 1);
+        }
+        return b_dot(len, cs, vk, vks, dA + c0, FIN_ID, mask);
+      });
     t_orth.begin();
-    if (!st) st = b_axpy_dev_nrm2(n, ns, dA, vk, vnew, dN0, act);
-    /* CGS_DGKS: pass 1, then pass 2 where the first kept <= 1/sqrt(2) */
-    if (!st) st = b_gemvT(n, ns, k + 1, Vc, ld, vks, dW, k + 1, nullptr, act);
-    if (!st) st = b_gemv_sub_nrm(n, ns, k + 1, Vc, ld, dW, k + 1, vnew, dN, nullptr, dF, dN0, kEta, act);
-    if (!st) st = b_gemvT(n, ns, k + 1, Vc, ld, vks, dW, k + 1, dF, act);
-    if (!st) st = b_gemv_sub_nrm(n, ns, k + 1, Vc, ld, dW, k + 1, vnew, dN, dF, nullptr, nullptr, kEta, act);
+    /* v -= alpha v_k, ||v||; CGS_DGKS: pass 1, then pass 2 where the first
+     * kept <= 1/sqrt(2) of the norm */
+    if (!st)
+      st = chunks(act, [&](int c0, int cs, unsigned mask, const BLen &len) {
+        CPtrs vk{}, Vc{}, vks{};
+        VPtrs vnew{};
+        for (int i = 0; i < cs; i++) {
+          vk.p[i] = col(c0 + i, k);
+          vnew.p[i] = col(c0 + i, k + 1);
+          vks.p[i] = vnew.p[i];
+          Vc.p[i] = SL[c0 + i].V;
+        }
+        int r = b_axpy_dev_nrm2(len, cs, dA + c0, vk, vnew, dN0 + c0, mask);
+        double *w = dW + (size_t)c0 * ldw;
+        if (!r) r = b_gemvT(len, cs, k + 1, Vc, vks, w, ldw, nullptr, mask);
+        if (!r)
+          r = b_gemv_sub_nrm(len, cs, k + 1, Vc, w, ldw, vnew, dN + c0, nullptr, dF + c0, dN0 + c0,
+                             kEta, mask);
+        if (!r) r = b_gemvT(len, cs, k + 1, Vc, vks, w, ldw, dF + c0, mask);
+        if (!r)
+          r = b_gemv_sub_nrm(len, cs, k + 1, Vc, w, ldw, vnew, dN + c0, dF + c0, nullptr, nullptr,
+                             kEta, mask);
+        return r;
+      });
     t_orth.end();
-    if (!st) st = memcpy_async(c.hscal + 16, c.dscal + 16, sizeof(double) * 48);
+    if (!st) st = memcpy_async(hA, dA, sizeof(double) * (size_t)ns);
+    if (!st) st = memcpy_async(hN, dN, sizeof(double) * (size_t)ns);
     if (!st) st = sync();
     if (st) break;
     t_pol.flush();
     t_orth.flush();
-    BScal inv{};
-    VPtrs sc{};
-    unsigned scal_mask = 0;
+    std::vector<char> scal_sel(ns, 0);
+    std::vector<double> inv(ns, 0.0);
     for (int s = 0; s < ns && !st; s++) {
-      if (!((act >> s) & 1u)) continue;
+      if (!act[s]) continue;
       SliceState *S = &SL[s];
-      const double alpha = c.hscal[16 + s];
-      double beta = c.hscal[48 + s];
+      const double alpha = hA[s];
+      double beta = hN[s];
       if (!isfinite(alpha) || !isfinite(beta)) {
         S->status = PEVSL_ERR_NONFINITE;
         S->done = 1;
-        act &= ~(1u << s);
+        act[s] = 0;
+        nact--;
         continue;
       }
       S->dT[k] = alpha;
       S->wn += fabs(alpha);
       S->wn += 2.0 * beta;
       S->nwn += 3;
-      double *znew = S->V + (size_t)(k + 1) * ld;
+      double *znew = S->V + (size_t)(k + 1) * S->ld;
       if (beta * S->nwn < orthTol * S->wn) {
         /* lucky breakdown: restart from a new filtered random vector
          * (SRC/cheblanNr.c:248-281) */
         if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
-        st = pevsl_rand_vector_dev(vrand, (int)n);
+        st = pevsl_rand_vector_dev(vrand, (int)S->n);
         t_pol.begin();
-        if (!st)
-          st = cheb_apply(pevsl, S->pol, vrand, znew, w3, n);
+        if (!st) st = cheb_apply(S->pevsl, S->pol, vrand, znew, w3, S->n);
         t_pol.end();
-        if (!st) st = vnrm2(n, znew, c.dscal + S_NRM0);
-        if (!st) st = cgs_dgks(S->V, ld, k + 1, znew, n);
+        if (!st) st = vnrm2(S->n, znew, c.dscal + S_NRM0);
+        if (!st) st = cgs_dgks(S->V, S->ld, k + 1, znew, S->n);
         const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
         if (!hb) {
           st = st ? st : PEVSL_ERR_CUDA;
           break;
         }
-        st = vscal(znew, n, 1.0 / hb[0]);
+        st = vscal(znew, S->n, 1.0 / hb[0]);
         beta = 0.0;
       } else {
-        inv.v[s] = 1.0 / beta;
-        sc.p[s] = znew;
-        scal_mask |= 1u << s;
+        inv[s] = 1.0 / beta;
+        scal_sel[s] = 1;
       }
       S->beta = beta;
       S->eT[k] = beta;
     }
-    if (!st && scal_mask) st = b_scal(n, ns, sc, inv, scal_mask);
+    if (!st)
+      st = chunks(scal_sel, [&](int c0, int cs, unsigned mask, const BLen &len) {
+        BScal v{};
+        VPtrs sc{};
+        for (int i = 0; i < cs; i++) {
+          v.v[i] = inv[c0 + i];
+          sc.p[i] = col(c0 + i, k + 1);
+        }
+        return b_scal(len, cs, sc, v, mask);
+      });
     if (st) break;
     /* restricted-trace convergence test (SRC/cheblanNr.c:293-332) */
     for (int s = 0; s < ns; s++) {
-      if (!((act >> s) & 1u)) continue;
+      if (!act[s]) continue;
       SliceState *S = &SL[s];
       if ((k < 30 || (k - 30) % 20 != 0) && k != S->maxit - 1) continue;
       S->kdim = k + 1;
@@ -1239,7 +1458,7 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
         st = PEVSL_ERR_EIG;
         break;
       }
-      pevsl->stats->t_eig += pevsl_now() - te;
+      S->pevsl->stats->t_eig += pevsl_now() - te;
       S->count = S->kdim;
       double tr1 = 0.0;
       S->nconv = 0;
@@ -1259,9 +1478,14 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
         if (!conv && fstats)
           fprintf(fstats, "The max number of iterations [%d] has been reached. The eigenvalues "
                           "computed may not have converged\n", S->maxit);
-        act &= ~(1u << s);
+        act[s] = 0;
+        nact--;
       }
     }
+  }
+  if (!st && g_filter_persistent && persistent_filter_error()) {
+    fprintf(stderr, "pevsl_b200: persistent filter barrier timed out\n");
+    st = PEVSL_ERR_CUDA;
   }
   cudaEventRecord(e_all1, c.stream);
   const double tr_start = pevsl_now();
@@ -1269,11 +1493,11 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     SliceState *S = &SL[s];
     if (S->done || S->status) continue;
     S->its = S->kdim;
-    const int rs = mixed ? ritz_refine(pevsl, S, vinit, n, ld, tol, guard, passes)
-                         : ritz_extract(pevsl, S, vinit, n, ld, tol);
+    const int rs = mixed ? ritz_refine(S->pevsl, S, S->vinit, S->n, S->ld, tol, guard, passes)
+                         : ritz_extract(S->pevsl, S, S->vinit, S->n, S->ld, tol);
     if (rs) S->status = rs;
   }
-  pevsl->stats->t_ritz = pevsl_now() - tr_start;
+  for (int s = 0; s < ns; s++) SL[s].pevsl->stats->t_ritz = pevsl_now() - tr_start;
   cudaEventSynchronize(e_all1);
   t_pol.flush();
   t_orth.flush();
@@ -1281,13 +1505,16 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
   cudaEventElapsedTime(&ms_all, e_all0, e_all1);
   cudaEventDestroy(e_all0);
   cudaEventDestroy(e_all1);
-  pevsl_inst *inst = pevsl_inst_of(pevsl);
-  inst->phase_ms[2] = ms_all;
-  inst->phase_ms[3] = t_pol.acc_ms;
-  inst->phase_ms[4] = t_orth.acc_ms;
-  if (A) g_filter_ms += t_pol.acc_ms;
-  pevsl->stats->t_polAv += 1e-3 * t_pol.acc_ms;
-  pevsl->stats->t_reorth += 1e-3 * t_orth.acc_ms;
+  for (int s = 0; s < ns; s++) {
+    pevsl_inst *inst = pevsl_inst_of(SL[s].pevsl);
+    if (s > 0 && SL[s].pevsl == SL[s - 1].pevsl) continue;
+    inst->phase_ms[2] = ms_all;
+    inst->phase_ms[3] = t_pol.acc_ms;
+    inst->phase_ms[4] = t_orth.acc_ms;
+    SL[s].pevsl->stats->t_polAv += 1e-3 * t_pol.acc_ms;
+    SL[s].pevsl->stats->t_reorth += 1e-3 * t_orth.acc_ms;
+  }
+  if (all_builtin) g_filter_ms += t_pol.acc_ms;
   for (int s = 0; s < ns; s++) {
     free(SL[s].dT);
     free(SL[s].eT);
@@ -1295,28 +1522,38 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     SL[s].dT = SL[s].eT = SL[s].EvalT = nullptr;
   }
   if (mixed && !st) {
-    /* a slice whose refined pairs in [a, b] did not all reach tol is run
-     * again in FP64, so the mixed form never reports fewer pairs */
-    SliceState R[kMaxBatch];
-    int idx[kMaxBatch], nr = 0;
+    /* a slice is run again in FP64 when a refined pair in [a, b] misses the
+     * FP64 path's quality, or fewer pairs were accepted than the Lanczos
+     * run had Ritz values above bar, so the mixed form never reports fewer
+     * or worse pairs */
+    std::vector<SliceState> R;
+    std::vector<int> idx;
     for (int s = 0; s < ns; s++) {
       SliceState *S = &SL[s];
       if (S->done || S->status || S->short_pairs <= 0) continue;
       free_slice_outputs(S);
-      memset(&R[nr], 0, sizeof R[nr]);
-      memcpy(R[nr].intv, S->intv, sizeof S->intv);
-      R[nr].pol = S->pol;
-      R[nr].maxit = S->maxit;
-      idx[nr++] = s;
+      SliceState r;
+      memset(&r, 0, sizeof r);
+      memcpy(r.intv, S->intv, sizeof S->intv);
+      r.pol = S->pol;
+      r.maxit = S->maxit;
+      r.pevsl = S->pevsl;
+      r.A = S->A;
+      r.vinit = S->vinit;
+      r.n = S->n;
+      r.ld = S->ld;
+      R.push_back(r);
+      idx.push_back(s);
     }
-    if (nr > 0) {
-      g_fallbacks += nr;
+    if (!R.empty()) {
+      g_fallbacks += (int)R.size();
+      pevsl_inst *inst = pevsl_inst_of(SL[0].pevsl);
       const float ms0 = inst->phase_ms[2], pol0 = inst->phase_ms[3], orth0 = inst->phase_ms[4];
-      st = cheblannr_group(pevsl, R, nr, tol, vinit, fstats, false);
+      st = cheblannr_group(R.data(), (int)R.size(), tol, fstats, false);
       inst->phase_ms[2] += ms0;
       inst->phase_ms[3] += pol0;
       inst->phase_ms[4] += orth0;
-      for (int r = 0; r < nr; r++) {
+      for (size_t r = 0; r < R.size(); r++) {
         SliceState *S = &SL[idx[r]];
         S->status = R[r].status;
         S->kdim = R[r].kdim;
@@ -1331,6 +1568,14 @@ static int cheblannr_group(pevsl_Data *pevsl, SliceState *SL, int ns, double tol
     }
   }
   return st;
+}
+
+static void slice_bind(SliceState *S, pevsl_Data *pevsl, pevsl_Parvec *vinit) {
+  S->pevsl = pevsl;
+  S->A = pevsl_builtin_A(pevsl);
+  S->vinit = vinit;
+  S->n = pevsl->n;
+  S->ld = round_ld(pevsl->n);
 }
 
 int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
@@ -1348,10 +1593,11 @@ int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevs
   memcpy(S.intv, intv, sizeof S.intv);
   S.pol = pol;
   S.maxit = maxit;
+  slice_bind(&S, pevsl, vinit);
   g_t_pol.init();
   g_t_orth.init();
   g_fallbacks = 0;
-  int st = cheblannr_group(pevsl, &S, 1, tol, vinit, fstats);
+  int st = cheblannr_group(&S, 1, tol, fstats);
   pevsl_inst *inst = pevsl_inst_of(pevsl);
   inst->last_its = S.kdim;
   inst->last_nconv = S.nconv;
@@ -1368,12 +1614,32 @@ int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevs
   return 0;
 }
 
-/* All slices of an interval through the lockstep solver, up to kMaxBatch at
- * a time; slice s gets intvs[4s..4s+3], pols[s], maxits[s].  Per-slice
- * outputs as pEVSL_ChebLanNr; status[s] per slice; returns the first
- * nonzero status.  Equal to calling pEVSL_ChebLanNr slice by slice, except
- * that the random restart vectors after a lucky breakdown are drawn in
- * lockstep order. */
+/* outputs of a solved group into the caller's arrays at offset o */
+static int group_outputs(SliceState *SL, int ns, int st, int o, int *nevOut, double **lamo,
+                         pevsl_Parvecs **Wo, double **reso, int *its, int *status) {
+  int first_err = 0;
+  for (int s = 0; s < ns; s++) {
+    SliceState *S = &SL[s];
+    const int ss = st ? st : S->status;
+    status[o + s] = ss;
+    its[o + s] = S->kdim;
+    if (ss) {
+      free_slice_outputs(S);
+      nevOut[o + s] = 0;
+      lamo[o + s] = nullptr;
+      Wo[o + s] = nullptr;
+      reso[o + s] = nullptr;
+      if (!first_err) first_err = ss;
+    } else {
+      nevOut[o + s] = S->nev;
+      lamo[o + s] = S->Lam;
+      Wo[o + s] = S->Rvec;
+      reso[o + s] = S->res;
+    }
+  }
+  return first_err;
+}
+
 int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intvs,
                               const int *maxits, double tol, pevsl_Parvec *vinit,
                               pevsl_Polparams *pols, int *nevOut, double **lamo,
@@ -1388,45 +1654,74 @@ int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intv
   g_t_orth.init();
   g_fallbacks = 0;
   double ms_total = 0.0, pol_total = 0.0, orth_total = 0.0;
-  for (int s0 = 0; s0 < nslices; s0 += kMaxBatch) {
-    const int ns = PEVSL_MIN(kMaxBatch, nslices - s0);
-    SliceState SL[kMaxBatch];
-    memset(SL, 0, sizeof SL);
+  for (int s0 = 0; s0 < nslices; s0 += kMaxEntries) {
+    const int ns = PEVSL_MIN(kMaxEntries, nslices - s0);
+    std::vector<SliceState> SL(ns);
+    memset(SL.data(), 0, sizeof(SliceState) * (size_t)ns);
     for (int s = 0; s < ns; s++) {
       memcpy(SL[s].intv, intvs + 4 * (size_t)(s0 + s), sizeof SL[s].intv);
       SL[s].pol = &pols[s0 + s];
       SL[s].maxit = maxits[s0 + s];
+      slice_bind(&SL[s], pevsl, vinit);
     }
-    int st = cheblannr_group(pevsl, SL, ns, tol, vinit, fstats);
+    int st = cheblannr_group(SL.data(), ns, tol, fstats);
     pevsl_inst *inst = pevsl_inst_of(pevsl);
     ms_total += inst->phase_ms[2];
     pol_total += inst->phase_ms[3];
     orth_total += inst->phase_ms[4];
-    for (int s = 0; s < ns; s++) {
-      SliceState *S = &SL[s];
-      const int ss = st ? st : S->status;
-      status[s0 + s] = ss;
-      its[s0 + s] = S->kdim;
-      if (ss) {
-        free_slice_outputs(S);
-        nevOut[s0 + s] = 0;
-        lamo[s0 + s] = nullptr;
-        Wo[s0 + s] = nullptr;
-        reso[s0 + s] = nullptr;
-        if (!first_err) first_err = ss;
-      } else {
-        nevOut[s0 + s] = S->nev;
-        lamo[s0 + s] = S->Lam;
-        Wo[s0 + s] = S->Rvec;
-        reso[s0 + s] = S->res;
-      }
-    }
+    const int e = group_outputs(SL.data(), ns, st, s0, nevOut, lamo, Wo, reso, its, status);
+    if (!first_err) first_err = e;
   }
   pevsl_inst *inst = pevsl_inst_of(pevsl);
   inst->phase_ms[2] = ms_total;
   inst->phase_ms[3] = pol_total;
   inst->phase_ms[4] = orth_total;
   pevsl->stats->t_iter = pevsl_now() - tall;
+  return first_err;
+}
+
+int pEVSL_B200_ChebLanNrMulti(int nprob, pevsl_Data **pevsls, const int *nslices,
+                              const double *intvs, const int *maxits, double tol,
+                              pevsl_Parvec **vinits, pevsl_Polparams *pols, int *nevOut,
+                              double **lamo, pevsl_Parvecs **Wo, double **reso, int *its,
+                              int *status, FILE *fstats) {
+  if (ensure()) return PEVSL_ERR_CUDA;
+  if (nprob < 0 || (nprob > 0 && (!pevsls || !nslices || !vinits))) return PEVSL_ERR_ARG;
+  for (int p = 0; p < nprob; p++) {
+    if (!pevsls[p] || nslices[p] < 0) return PEVSL_ERR_ARG;
+    if (pevsls[p]->ifGenEv) return PEVSL_NOT_IMPLEMENT;
+  }
+  g_t_pol.init();
+  g_t_orth.init();
+  g_fallbacks = 0;
+  int first_err = 0;
+  /* groups of up to kMaxEntries slices; a problem is kept in one group
+   * where it fits, a problem with more slices fills groups of its own */
+  std::vector<SliceState> SL;
+  int o = 0, o0 = 0;
+  auto flush = [&]() {
+    if (SL.empty()) return;
+    const int st = cheblannr_group(SL.data(), (int)SL.size(), tol, fstats);
+    const int e = group_outputs(SL.data(), (int)SL.size(), st, o0, nevOut, lamo, Wo, reso, its,
+                                status);
+    if (!first_err) first_err = e;
+    o0 += (int)SL.size();
+    SL.clear();
+  };
+  for (int p = 0; p < nprob; p++) {
+    if (!SL.empty() && (int)SL.size() + nslices[p] > kMaxEntries) flush();
+    for (int s = 0; s < nslices[p]; s++, o++) {
+      if ((int)SL.size() == kMaxEntries) flush();
+      SliceState S;
+      memset(&S, 0, sizeof S);
+      memcpy(S.intv, intvs + 4 * (size_t)o, sizeof S.intv);
+      S.pol = &pols[o];
+      S.maxit = maxits[o];
+      slice_bind(&S, pevsls[p], vinits[p]);
+      SL.push_back(S);
+    }
+  }
+  flush();
   return first_err;
 }
 

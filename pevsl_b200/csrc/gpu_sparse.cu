@@ -180,10 +180,10 @@ struct EpiCheb32 {
  * a[j] * x[ja[j]] (unfused) into shared memory; each lane adds its rows'
  * products in index order -- the summation order of the reference's row
  * loop (SRC/spmat.c:188-193), so the result matches it to the last bit. */
-template <int R, class T, class Epi>
+template <int R, class T, class Epi, bool NC = true>
 __device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
                                             const int *__restrict__ ja, const T *__restrict__ a,
-                                            const T *__restrict__ x, const Epi &epi, long rblk,
+                                            const T *x, const Epi &epi, long rblk,
                                             T (*prod)[kStreamChunk * R]) {
   constexpr int CH = kStreamChunk * R, PL = CH / 32;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -223,7 +223,9 @@ __device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
     }
 #pragma unroll
     for (int q = 0; q < PL; q++) {
-      const T xv = col[q] >= 0 ? __ldg(x + col[q]) : T(0);
+      /* NC: x is read-only for the launch (non-coherent path); otherwise it
+       * was written earlier in the same launch by other blocks */
+      const T xv = col[q] >= 0 ? (NC ? __ldg(x + col[q]) : x[col[q]]) : T(0);
       pw[q * 32 + lane] = mul_rn(val[q], xv);
     }
     __syncwarp();
@@ -249,26 +251,265 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 5 : 1)
   stream_rows<R>(n, ia, ja, a, x, epi, blockIdx.x, prod);
 }
 
-/* Up to kMaxBatch independent products y_e = A x_e, each with its own
- * epilogue.  Block b serves entry b % nb on row block b / nb: the nb blocks
- * that read one stretch of the matrix are adjacent in launch order, so the
- * stretch comes from HBM once and from L2 for the other entries, while each
- * entry keeps its vectors in its own columns (no interleaving, no copies).
- * The per-entry arithmetic is that of k_csr_stream, bit for bit. */
-template <class T, class Epi>
+/* Up to CAP independent products y_e = A_e x_e (x_e = epi[e].vk), each with
+ * its own matrix and epilogue, in one launch.  With `shared` (all entries
+ * on one matrix) block b serves entry b % nb on row block b / nb: the nb
+ * blocks that read one stretch of the matrix are adjacent in launch order,
+ * so the stretch comes from HBM once and from L2 for the other entries.
+ * Otherwise block b serves the entry e with off[e] <= b < off[e+1], row
+ * block b - off[e].  Each entry keeps its vectors in its own columns (no
+ * interleaving, no copies), and its arithmetic is that of k_csr_stream, bit
+ * for bit.  The table is a __grid_constant__ parameter (up to 32 KB). */
+template <class T, class Epi, int CAP>
 struct StreamBatch {
-  const T *x[kMaxBatch];
-  Epi epi[kMaxBatch];
-  int nb;
+  const int *ia[CAP];
+  const int *ja[CAP];
+  const T *a[CAP];
+  int n[CAP];
+  int off[CAP + 1];
+  Epi epi[CAP];
+  int nb, shared;
 };
 
-template <int R, class T, class Epi>
+template <int R, class T, class Epi, int CAP>
 __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
-    k_csr_stream_batch(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                       const T *__restrict__ a, const __grid_constant__ StreamBatch<T, Epi> b) {
+    k_csr_stream_batch(const __grid_constant__ StreamBatch<T, Epi, CAP> b) {
   __shared__ T prod[kThreads / 32][kStreamChunk * R];
-  const int e = (int)(blockIdx.x % (unsigned)b.nb);
-  stream_rows<R>(n, ia, ja, a, b.x[e], b.epi[e], (long)(blockIdx.x / (unsigned)b.nb), prod);
+  int e;
+  long rblk;
+  if (b.shared) {
+    e = (int)(blockIdx.x % (unsigned)b.nb);
+    rblk = (long)(blockIdx.x / (unsigned)b.nb);
+  } else {
+    int lo = 0, hi = b.nb; /* off[lo] <= blockIdx.x < off[hi] */
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (b.off[mid] <= (int)blockIdx.x) lo = mid;
+      else hi = mid;
+    }
+    e = lo;
+    rblk = (long)blockIdx.x - b.off[lo];
+  }
+  stream_rows<R>(b.n[e], b.ia[e], b.ja[e], b.a[e], (const T *)b.epi[e].vk, b.epi[e], rblk, prod);
+}
+
+/* ---------------------------------------------------------------- persistent filter */
+
+constexpr unsigned kBarrierSpins = 1u << 24; /* ~2 s of polling before giving up */
+
+/* Sense-counting grid barrier for a cooperative launch (all blocks are
+ * co-resident).  bar[0] counts arrivals, bar[1] is the generation; the
+ * waits are bounded: after kBarrierSpins polls the block sets bar[2] and
+ * continues, and the kernel returns at its next check. */
+__device__ __forceinline__ void grid_barrier(unsigned *bar) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned it = 0;
+      while (*gen == g) {
+        if (++it > kBarrierSpins) {
+          atomicExch(bar + 2, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+/* Operands of degree j of one entry (the two-buffer rotation of
+ * cheb_apply: j = 1 reads x and writes b0, j = 2 reads b0 and x and writes
+ * b1, then odd j write b0 over v_{j-1}, even j write b1). */
+template <class T>
+__device__ __forceinline__ void rotation(const FiltDev &E, int j, const T **vk, const T **vkm1,
+                                         T **vkp1) {
+  const T *x = (const T *)E.x;
+  T *b0 = (T *)E.b0, *b1 = (T *)E.b1;
+  if (j == 1) {
+    *vk = x;
+    *vkm1 = nullptr;
+    *vkp1 = b0;
+  } else if (j == 2) {
+    *vk = b0;
+    *vkm1 = x;
+    *vkp1 = b1;
+  } else if (j & 1) {
+    *vk = b1;
+    *vkm1 = b0;
+    *vkp1 = b0;
+  } else {
+    *vk = b0;
+    *vkm1 = b1;
+    *vkp1 = b1;
+  }
+}
+
+/* Work items of degree j: with `shared` (all entries on one matrix, nblk
+ * row blocks each) item i is row block i / live of entry i % live, so the
+ * entries reading one stretch of the matrix run together and share it in
+ * L2; otherwise entry-major through the row-block offsets.  The table and,
+ * per degree, every entry's mu[0] and mu[j] sit in shared memory, so an
+ * item starts with the loads of its rows. */
+template <class T, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
+    k_filter_persistent(const FiltDev *__restrict__ tab, int ne, const int *__restrict__ blk_off,
+                        int maxdeg, int shared, unsigned *bar) {
+  __shared__ T prod[kThreads / 32][kStreamChunk];
+  extern __shared__ double dyn[];
+  FiltDev *s_tab = (FiltDev *)dyn;                /* ne entries */
+  double *s_mu = (double *)(s_tab + ne);         /* 2 per entry: mu[0], mu[j] */
+  int *s_off = (int *)(s_mu + 2 * ne);           /* ne + 1 */
+  for (int i = threadIdx.x; i < ne * (int)(sizeof(FiltDev) / 8); i += blockDim.x)
+    ((double *)s_tab)[i] = ((const double *)tab)[i];
+  for (int i = threadIdx.x; i <= ne; i += blockDim.x) s_off[i] = blk_off[i];
+  __syncthreads();
+  int live = ne; /* entries sorted by non-increasing degree: a prefix is live */
+  for (int j = 1; j <= maxdeg; j++) {
+    while (live > 0 && s_tab[live - 1].deg < j) live--;
+    for (int i = threadIdx.x; i < live; i += blockDim.x) {
+      s_mu[2 * i] = s_tab[i].mu[0];
+      s_mu[2 * i + 1] = s_tab[i].mu[j];
+    }
+    __syncthreads();
+    const int total = s_off[live];
+    for (int item = blockIdx.x; item < total; item += gridDim.x) {
+      int lo;
+      long rblk;
+      if (shared) {
+        lo = item % live;
+        rblk = item / live;
+      } else {
+        int hi = live; /* s_off[lo] <= item < s_off[hi] */
+        lo = 0;
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) >> 1;
+          if (s_off[mid] <= item) lo = mid;
+          else hi = mid;
+        }
+        rblk = item - s_off[lo];
+      }
+      const FiltDev &E = s_tab[lo];
+      const double t = j == 1 ? E.t1 : E.t2, mu0 = s_mu[2 * lo], muj = s_mu[2 * lo + 1];
+      const T *vk, *vkm1;
+      T *vkp1;
+      rotation<T>(E, j, &vk, &vkm1, &vkp1);
+      if constexpr (sizeof(T) == 8) {
+        EpiCheb epi{vk, vkm1, vkp1, (double *)E.acc, E.cc, t, mu0, muj, j == 1};
+        stream_rows<1, double, EpiCheb, false>(E.n, E.ia, E.ja, (const double *)E.a, vk, epi, rblk,
+                                               prod);
+      } else {
+        EpiCheb32 epi{vk, vkm1, vkp1, (float *)E.acc, j == E.deg ? E.y : nullptr, (float)E.cc,
+                      (float)t, (float)mu0, (float)muj, j == 1};
+        stream_rows<1, float, EpiCheb32, false>(E.n, E.ia, E.ja, (const float *)E.a, vk, epi, rblk,
+                                                prod);
+      }
+    }
+    if (j < maxdeg) {
+      grid_barrier(bar); /* also orders the s_mu rewrite after every use */
+      if (*(volatile unsigned *)(bar + 2)) return;
+    }
+  }
+}
+
+static_assert(sizeof(FiltDev) % 8 == 0, "the table is copied to shared memory in doubles");
+
+static size_t persistent_smem(int ne) {
+  return sizeof(FiltDev) * (size_t)ne + sizeof(double) * 2 * (size_t)ne +
+         sizeof(int) * ((size_t)ne + 1);
+}
+
+static unsigned g_persist_grid = 0;
+
+int cheb_filter_persistent(int ne, const FiltDev *entries, int maxdeg) {
+  if (ne <= 0 || maxdeg <= 0) return 0;
+  if (ne > kMaxEntries) return PEVSL_ERR_ARG;
+  Ctx &c = ctx();
+  /* co-resident grid for this table size (the dynamic shared memory grows
+   * with the entries) */
+  const size_t dsm = persistent_smem(ne);
+  const bool fp32 = entries[0].fp32 != 0;
+  /* blocks per SM the kernel is built for: 4 (64 registers) or 3
+   * (PEVSL_B200_PERSIST_MINB=3, more registers, no spills) */
+  static int minb = 0;
+  if (!minb) {
+    const char *e = getenv("PEVSL_B200_PERSIST_MINB");
+    minb = e && atoi(e) == 3 ? 3 : 4;
+  }
+  const void *fn = fp32 ? (minb == 3 ? (const void *)k_filter_persistent<float, 3>
+                                     : (const void *)k_filter_persistent<float, 4>)
+                        : (minb == 3 ? (const void *)k_filter_persistent<double, 3>
+                                     : (const void *)k_filter_persistent<double, 4>);
+  static bool attr_done = false;
+  if (!attr_done) {
+    const void *all[4] = {(const void *)k_filter_persistent<float, 3>,
+                          (const void *)k_filter_persistent<float, 4>,
+                          (const void *)k_filter_persistent<double, 3>,
+                          (const void *)k_filter_persistent<double, 4>};
+    for (const void *f : all)
+      if (fail(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)persistent_smem(kMaxEntries)),
+               "cudaFuncSetAttribute"))
+        return PEVSL_ERR_CUDA;
+    attr_done = true;
+  }
+  int per_sm = 0;
+  if (fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kThreads, dsm),
+           "cudaOccupancyMaxActiveBlocksPerMultiprocessor"))
+    return PEVSL_ERR_CUDA;
+  if (per_sm < 1) return PEVSL_ERR_ARG;
+  g_persist_grid = (unsigned)(per_sm * c.sms);
+  /* table + row-block offsets staged in pinned memory, one copy; the slot
+   * is rewritten only after its previous copy has run */
+  const int slot = c.tab_next;
+  c.tab_next = (c.tab_next + 1) % kTabSlots;
+  if (fail(cudaEventSynchronize(c.tab_ev[slot]), "cudaEventSynchronize")) return PEVSL_ERR_CUDA;
+  FiltDev *htab = (FiltDev *)((char *)c.htab + kFiltTabBytes * slot);
+  int *hoff = (int *)(htab + kMaxEntries);
+  memcpy(htab, entries, sizeof(FiltDev) * (size_t)ne);
+  long total = 0;
+  int shared = 1;
+  for (int e = 0; e < ne; e++) {
+    hoff[e] = (int)total;
+    total += (entries[e].n + kThreads - 1) / kThreads;
+    if (entries[e].ia != entries[0].ia || entries[e].a != entries[0].a) shared = 0;
+  }
+  hoff[ne] = (int)total;
+  if (total <= 0) return 0;
+  if (total > INT32_MAX) return PEVSL_ERR_ARG;
+  const FiltDev *dtab = (const FiltDev *)((char *)c.dtab + kFiltTabBytes * slot);
+  if (memcpy_async((void *)dtab, htab, kFiltTabBytes)) return PEVSL_ERR_CUDA;
+  if (fail(cudaEventRecord(c.tab_ev[slot], c.stream), "cudaEventRecord")) return PEVSL_ERR_CUDA;
+  unsigned grid = g_persist_grid;
+  if ((long)grid > total) grid = (unsigned)total;
+  const int *doff = (const int *)(dtab + kMaxEntries);
+  unsigned *bar = c.bar;
+  void *args[] = {(void *)&dtab, (void *)&ne,     (void *)&doff,
+                  (void *)&maxdeg, (void *)&shared, (void *)&bar};
+  if (fail(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, dsm, c.stream),
+           "cudaLaunchCooperativeKernel"))
+    return PEVSL_ERR_CUDA;
+  return launched("filter_persistent");
+}
+
+int persistent_filter_error() {
+  unsigned h[4] = {0, 0, 0, 0};
+  if (cudaMemcpy(h, ctx().bar, sizeof h, cudaMemcpyDeviceToHost) != cudaSuccess) return 1;
+  if (h[2]) {
+    const unsigned z = 0;
+    cudaMemcpy(ctx().bar + 2, &z, sizeof z, cudaMemcpyHostToDevice);
+    cudaMemcpy(ctx().bar, &z, sizeof z, cudaMemcpyHostToDevice);
+    return 1;
+  }
+  return 0;
 }
 
 /* rows per lane of the CSR-stream kernels: 1 or 2 (PEVSL_B200_STREAM_R) */
@@ -439,14 +680,35 @@ static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const E
                                                                              a, x, epi);
 }
 
-template <class T, class Epi>
-static void launch_stream_batch(const pevsl_devcsr *A, const T *a, const StreamBatch<T, Epi> &b) {
+/* fill the table from the entries (matrices from e[i].A) and launch */
+template <class T, class Epi, int CAP, class Make>
+static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const char *what) {
+  static StreamBatch<T, Epi, CAP> b; /* host staging: the launch copies it */
   const int R = stream_r();
-  const unsigned g = stream_grid(A->nrows, R) * (unsigned)b.nb;
+  const long rows_per_block = (kThreads / 32) * 32L * R;
+  b.nb = nb;
+  b.shared = 1;
+  long off = 0;
+  for (int i = 0; i < nb; i++) {
+    const pevsl_devcsr *A = en[i].A;
+    b.ia[i] = A->ia;
+    b.ja[i] = A->ja;
+    b.a[i] = (const T *)(sizeof(T) == 4 ? (const void *)A->a32 : (const void *)A->a);
+    b.n[i] = A->nrows;
+    b.off[i] = (int)off;
+    off += (A->nrows + rows_per_block - 1) / rows_per_block;
+    b.epi[i] = make(en[i]);
+    if (A != en[0].A) b.shared = 0;
+  }
+  b.off[nb] = (int)off;
+  if (off <= 0) return 0;
+  if (off > 0x7fffffffL) return PEVSL_ERR_ARG;
+  const unsigned g = (unsigned)off;
   if (R == 2)
-    k_csr_stream_batch<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, a, b);
+    k_csr_stream_batch<2, T, Epi, CAP><<<g, kThreads, 0, ctx().stream>>>(b);
   else
-    k_csr_stream_batch<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, a, b);
+    k_csr_stream_batch<1, T, Epi, CAP><<<g, kThreads, 0, ctx().stream>>>(b);
+  return launched(what);
 }
 
 int spmv(const pevsl_devcsr *A, const double *x, double *y) {
@@ -471,31 +733,27 @@ int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, doubl
   return launched("cheb_step");
 }
 
-int cheb_step_batch(const pevsl_devcsr *A, int nb, const ChebEntry *e, bool fp32) {
-  if (A->nrows <= 0 || nb <= 0) return 0;
-  if (nb > kMaxBatch) return PEVSL_ERR_ARG;
+int cheb_step_batch(int nb, const ChebEntry *e, bool fp32) {
+  if (nb <= 0) return 0;
+  if (nb > kMaxEntries) return PEVSL_ERR_ARG;
   if (fp32) {
-    if (!A->a32) return PEVSL_ERR_ARG;
-    StreamBatch<float, EpiCheb32> b{};
-    b.nb = nb;
-    for (int i = 0; i < nb; i++) {
-      b.x[i] = (const float *)e[i].vk;
-      b.epi[i] = EpiCheb32{(const float *)e[i].vk, (const float *)e[i].vkm1, (float *)e[i].vkp1,
-                           (float *)e[i].y, e[i].yout, (float)e[i].cc, (float)e[i].t,
-                           (float)e[i].mu0, (float)e[i].muk, e[i].first};
-    }
-    launch_stream_batch(A, (const float *)A->a32, b);
-    return launched("cheb_step_batch32");
+    for (int i = 0; i < nb; i++)
+      if (!e[i].A->a32) return PEVSL_ERR_ARG;
+    auto mk = [](const ChebEntry &c) {
+      return EpiCheb32{(const float *)c.vk, (const float *)c.vkm1, (float *)c.vkp1, (float *)c.y,
+                       c.yout, (float)c.cc, (float)c.t, (float)c.mu0, (float)c.muk, c.first};
+    };
+    return nb <= kMaxBatch
+               ? launch_stream_batch<float, EpiCheb32, kMaxBatch>(nb, e, mk, "cheb_step_batch32")
+               : launch_stream_batch<float, EpiCheb32, kMaxEntries>(nb, e, mk, "cheb_step_batch32");
   }
-  StreamBatch<double, EpiCheb> b{};
-  b.nb = nb;
-  for (int i = 0; i < nb; i++) {
-    b.x[i] = (const double *)e[i].vk;
-    b.epi[i] = EpiCheb{(const double *)e[i].vk, (const double *)e[i].vkm1, (double *)e[i].vkp1,
-                       (double *)e[i].y, e[i].cc, e[i].t, e[i].mu0, e[i].muk, e[i].first};
-  }
-  launch_stream_batch(A, (const double *)A->a, b);
-  return launched("cheb_step_batch");
+  auto mk = [](const ChebEntry &c) {
+    return EpiCheb{(const double *)c.vk, (const double *)c.vkm1, (double *)c.vkp1, (double *)c.y,
+                   c.cc, c.t, c.mu0, c.muk, c.first};
+  };
+  return nb <= kMaxBatch
+             ? launch_stream_batch<double, EpiCheb, kMaxBatch>(nb, e, mk, "cheb_step_batch")
+             : launch_stream_batch<double, EpiCheb, kMaxEntries>(nb, e, mk, "cheb_step_batch");
 }
 
 int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1, double *vkp1,

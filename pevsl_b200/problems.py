@@ -43,3 +43,63 @@ def laplacian_eigenvalues(nx: int, ny: int, nz: int, a: float, b: float) -> np.n
     tz = np.sin(np.arange(1, nz + 1) * 0.5 * np.pi / (nz + 1.0)) if nz > 1 else np.zeros(1)
     ev = (4 * (tx[:, None, None] ** 2 + ty[None, :, None] ** 2 + tz[None, None, :] ** 2)).ravel()
     return np.sort(ev[(ev >= a - eps) & (ev <= b + eps)])
+
+
+def laplacian_shifted(nx: int, ny: int, nz: int, shift: float):
+    """laplacian(nx, ny, nz) + shift * I: (n, ia, ja, a).  Its eigenvalues
+    are those of the Laplacian plus shift."""
+    n, ia, ja, a = laplacian(nx, ny, nz)
+    a = a.copy()
+    rows = np.repeat(np.arange(n), np.diff(ia))
+    a[ja == rows] += shift
+    return n, ia, ja, a
+
+
+def _gap_midpoint(ev: np.ndarray, t: float, tol: float = 1e-10) -> float:
+    """Midpoint of the gap between distinct eigenvalues (ascending ev) that
+    lies nearest to t."""
+    j = int(np.clip(np.searchsorted(ev, t), 1, len(ev) - 1))
+    best = None
+    for jj in range(max(1, j - 64), min(len(ev), j + 64)):
+        if ev[jj] - ev[jj - 1] > tol:
+            m = 0.5 * (ev[jj - 1] + ev[jj])
+            if best is None or abs(m - t) < abs(best - t):
+                best = m
+    return float(best if best is not None else t)
+
+
+def multi_laplacian_set(count: int = 32, seed: int = 2024, per_slice: int = 20):
+    """The batched-problem workload: `count` Dirichlet Laplacians, each a 2D
+    5-point or 3D 7-point grid (coin flip) with equal sides drawn uniformly
+    so that n = side^d lies in [1e4, 5e5], plus a diagonal shift drawn from
+    U[0, 0.5], and 2..8 slices.  The interval of a problem starts at 0.5%
+    of its spectral width above the bottom of the spectrum and holds
+    per_slice * nslices eigenvalues; the slices split it about evenly, every
+    slice end lying midway between two distinct eigenvalues.  Returns a list of dicts:
+    grid, n, shift, nslices, intv (slice ends), lmin, lmax (spectrum bounds
+    with a 1e-3 margin), counts (eigenvalues per slice)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        d = 2 if rng.random() < 0.5 else 3
+        smin = int(np.ceil(1e4 ** (1.0 / d)))
+        smax = int(np.floor(5e5 ** (1.0 / d)))
+        s = int(rng.integers(smin, smax + 1))
+        shift = float(rng.uniform(0.0, 0.5))
+        ns = int(rng.integers(2, 9))
+        grid = (s, s, s) if d == 3 else (s, s, 1)
+        ev = laplacian_eigenvalues(*grid, 0.0, 100.0)
+        lo, hi = ev[0], ev[-1]
+        i0 = int(np.searchsorted(ev, lo + 0.005 * (hi - lo)))
+        i1 = min(i0 + per_slice * ns, len(ev) - 1)
+        # slice ends at gap midpoints between distinct eigenvalues (values
+        # closer than 1e-10 count as one), the inner ones nearest the even split
+        a = _gap_midpoint(ev, 0.5 * (ev[i0 - 1] + ev[i0]))
+        b = _gap_midpoint(ev, 0.5 * (ev[i1 - 1] + ev[i1]))
+        edges = np.array([a] + [_gap_midpoint(ev, t) for t in np.linspace(a, b, ns + 1)[1:-1]]
+                         + [b])
+        counts = [int(np.sum((ev >= edges[k]) & (ev < edges[k + 1]))) for k in range(ns)]
+        out.append(dict(grid=grid, n=int(s ** d), shift=shift, nslices=ns,
+                        intv=[float(x) + shift for x in edges], lmin=float(lo + shift - 1e-3),
+                        lmax=float(hi + shift + 1e-3), counts=counts))
+    return out

@@ -436,3 +436,65 @@ def test_mixed_precision_counts_and_residuals(gpu, name):
         ex = exact_eig_lap(*g["grid"], r.sli[sl], r.sli[sl + 1])
         assert len(lam) == len(ex), (sl, len(lam), len(ex))
         assert np.max(np.abs(lam - ex) / np.abs(ex)) <= 1e-10
+
+
+# ---------------------------------------------------------------- batching forms
+def _lap_slices(grid, a, b, ns, seed=3):
+    """Bounds from the analytic spectrum, slices evenly spaced, filters."""
+    L = laplacian(*grid)
+    ev = exact_eig_lap(*grid, 0.0, 100.0)
+    lmin, lmax = ev[0] - 1e-6, ev[-1] + 1e-6
+    edges = np.linspace(a, b, ns + 1)
+    intvs = [[edges[i], edges[i + 1], lmin, lmax] for i in range(ns)]
+    fl = [pv.findpol(iv)[1] for iv in intvs]
+    return pv.Matrix.from_csr(L.n, L.ia, L.ja, L.a), intvs, fl
+
+
+def test_filter_forms_bit_identical(gpu):
+    """One launch per degree and one persistent launch for all degrees give
+    the same bits (same per-row arithmetic, any schedule)."""
+    lib = pv.load()
+    M, intvs, fl = _lap_slices((14, 13, 12), 0.5, 1.3, 4)
+    v = np.cos(np.arange(M.n) * 0.37)
+    outs = []
+    try:
+        for form in (0, 1):
+            assert lib.pEVSL_B200_SetFilterForm(form) == 0
+            with pv.Instance(M) as ev:
+                r, o = pv.cheblannr_batch(ev, intvs, [150] * 4, 1e-8, v, fl)
+            assert r == 0
+            outs.append(o)
+    finally:
+        lib.pEVSL_B200_SetFilterForm(-1)
+    for a, b in zip(*outs):
+        assert a["nev"] == b["nev"] and a["its"] == b["its"]
+        assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
+
+
+def test_multi_problem_equals_separate(gpu):
+    """pEVSL_B200_ChebLanNrMulti over problems of different sizes, slice
+    counts and filter degrees gives every slice the bits of solving its
+    problem alone, and the exact per-slice counts."""
+    specs = [((11, 10, 9), 0.6, 1.4, 3), ((30, 29, 1), 0.3, 0.7, 2), ((9, 9, 9), 1.0, 2.2, 4)]
+    probs, sep = [], []
+    insts = []
+    for grid, a, b, ns in specs:
+        M, intvs, fl = _lap_slices(grid, a, b, ns)
+        v = np.sin(np.arange(M.n) * 0.11 + ns)
+        ev = pv.Instance(M)
+        insts.append(ev)
+        r, o = pv.cheblannr_batch(ev, intvs, [160] * ns, 1e-8, v, fl)
+        assert r == 0
+        sep.append((grid, intvs, o))
+        probs.append((ev, intvs, [160] * ns, 1e-8, v, fl))
+    r, multi = pv.cheblannr_multi(probs)
+    assert r == 0
+    for (grid, intvs, o1), o2 in zip(sep, multi):
+        for iv, a, b in zip(intvs, o1, o2):
+            assert a["nev"] == b["nev"] and a["its"] == b["its"]
+            assert np.array_equal(a["lam"], b["lam"])
+            ex = exact_eig_lap(*grid, iv[0], iv[1])
+            assert b["nev"] == len(ex)
+            assert np.max(np.abs(b["lam"] - ex)) <= 1e-10 * np.max(np.abs(ex))
+    for ev in insts:
+        ev.close()

@@ -121,3 +121,21 @@ def test_part1d_and_sort(lib):
     x = np.zeros(7)
     lib.linspace(0.25, 1.75, 7, x.ctypes.data_as(C.POINTER(C.c_double)))
     assert x[0] == 0.25 and x[-1] == 1.75 and abs(x[3] - 1.0) < 1e-16
+
+
+def test_findpol_too_narrow_is_an_error(lib):
+    """A slice so narrow that the degree search would start at or above
+    max_deg returns PEVSL_ERR_ARG (the reference writes past its max_deg + 1
+    coefficient arrays there, SRC/chebpol.c:433-447)."""
+    import pevsl_b200 as pv
+    r, f = pv.findpol([0.4845065036442954, 0.4850594098995861, 0.4435124791600489,
+                       8.445429558871442], max_deg=3000)
+    assert r == pv.ERR_ARG and f is None
+    # the same slice with room for the degree it needs
+    r, f = pv.findpol([0.4845065036442954, 0.4850594098995861, 0.4435124791600489,
+                       8.445429558871442], max_deg=20000)
+    assert r == 0 and 3600 < f.deg < 20000
+    # a forced degree below the starting degree is the same error
+    r, f = pv.findpol([0.4845065036442954, 0.4850594098995861, 0.4435124791600489,
+                       8.445429558871442], max_deg=3000, deg_in=100)
+    assert r == pv.ERR_ARG
