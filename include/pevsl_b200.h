@@ -152,6 +152,10 @@ double pEVSL_B200_EventElapsedMs(int a, int b);
 /* Page-locked host memory for fast host<->device copies of inputs. */
 void *pEVSL_B200_HostAlloc(size_t bytes);
 void pEVSL_B200_HostFree(void *p);
+/* CUDA managed memory: the host may read and write it between library calls
+ * (after pEVSL_B200_Sync) */
+void *pEVSL_B200_ManagedAlloc(size_t bytes);
+void pEVSL_B200_ManagedFree(void *p);
 
 /* Counters of the fused Chebyshev filter kernel since the last reset:
  * launches inside pEVSL_ChebLanNr, their algorithmic bytes (CSR + vectors),
@@ -161,6 +165,35 @@ void pEVSL_B200_ResetFilterCounters(void);
 
 /* Short build/device description into buf (NUL-terminated). */
 int pEVSL_B200_Info(char *buf, int len);
+
+/* ---------------------------------------------------------------- learned DOS
+ * A small MLP with BF16 weights and activations and FP32 accumulation,
+ * trained and run by this library's own GPU kernels (tensor-core BF16 GEMM
+ * with fused bias/GELU epilogues, GELU' in the backward pass, Adam on FP32
+ * master weights).  Layers: nin -> width -> ... -> width -> nout with GELU
+ * between them ("layers" linear maps); dimensions are padded to multiples
+ * of 16 inside.  The learned DOS maps KPM moments from a few random
+ * vectors to the moments of many (pevsl_b200/learned.py drives it). */
+typedef struct pevsl_mlp pevsl_mlp;
+int pEVSL_B200_MlpCreate(pevsl_mlp **net, int nin, int width, int nout, int layers);
+void pEVSL_B200_MlpFree(pevsl_mlp *net);
+/* parameters incl. padding; per layer l: K_l, N_l (padded), and the offsets
+ * of W_l (N_l x K_l, row-major) and b_l (N_l) in the parameter block;
+ * returns the number of layers */
+long pEVSL_B200_MlpParamCount(const pevsl_mlp *net);
+int pEVSL_B200_MlpLayout(const pevsl_mlp *net, int *kdim, int *ndim, long *woff, long *boff);
+/* FP32 master parameters from / to host memory (setting resets Adam) */
+int pEVSL_B200_MlpSetParams(pevsl_mlp *net, const float *host);
+int pEVSL_B200_MlpGetParams(const pevsl_mlp *net, float *host);
+/* Y [B][nout] = net(X [B][nin]), row-major FP32 device arrays */
+int pEVSL_B200_MlpForward(pevsl_mlp *net, const float *X, float *Y, int B);
+/* mean squared error against T [B][nout] and its gradient (host FP32, the
+ * parameter layout); the weights are not changed */
+int pEVSL_B200_MlpGradients(pevsl_mlp *net, const float *X, const float *T, int B, float *loss,
+                            float *grad_host);
+/* one Adam step (beta 0.9 / 0.999) on (X, T); *loss = the loss before it */
+int pEVSL_B200_MlpTrainStep(pevsl_mlp *net, const float *X, const float *T, int B, float lr,
+                            float *loss);
 
 #ifdef __cplusplus
 }

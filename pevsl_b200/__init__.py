@@ -162,6 +162,18 @@ SIGNATURES = [
     ("pEVSL_B200_EventElapsedMs", _D, [_I, _I]),
     ("pEVSL_B200_HostAlloc", _vp, [C.c_size_t]),
     ("pEVSL_B200_HostFree", None, [_vp]),
+    ("pEVSL_B200_ManagedAlloc", _vp, [C.c_size_t]),
+    ("pEVSL_B200_ManagedFree", None, [_vp]),
+    ("pEVSL_B200_MlpCreate", _I, [C.POINTER(_vp), _I, _I, _I, _I]),
+    ("pEVSL_B200_MlpFree", None, [_vp]),
+    ("pEVSL_B200_MlpParamCount", C.c_long, [_vp]),
+    ("pEVSL_B200_MlpLayout", _I, [_vp, _ip, _ip, C.POINTER(C.c_long), C.POINTER(C.c_long)]),
+    ("pEVSL_B200_MlpSetParams", _I, [_vp, C.POINTER(C.c_float)]),
+    ("pEVSL_B200_MlpGetParams", _I, [_vp, C.POINTER(C.c_float)]),
+    ("pEVSL_B200_MlpForward", _I, [_vp, _vp, _vp, _I]),
+    ("pEVSL_B200_MlpGradients", _I, [_vp, _vp, _vp, _I, C.POINTER(C.c_float),
+                                     C.POINTER(C.c_float)]),
+    ("pEVSL_B200_MlpTrainStep", _I, [_vp, _vp, _vp, _I, C.c_float, C.POINTER(C.c_float)]),
     ("pEVSL_B200_FilterCounters", None, [C.POINTER(C.c_uint64), _dp, _dp]),
     ("pEVSL_B200_ResetFilterCounters", None, []),
     ("pEVSL_B200_SetPrecision", _I, [C.POINTER(PevslData), _I]),
@@ -579,6 +591,95 @@ def cheblannr_multi(problems):
         if v is not p[4]:
             v.free()
     return r, outs
+
+
+class ManagedArray:
+    """A CUDA managed-memory array (pEVSL_B200_ManagedAlloc) with a numpy view."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.lib = load()
+        self.dtype = np.dtype(dtype)
+        self.shape = tuple(shape) if hasattr(shape, "__len__") else (int(shape),)
+        nbytes = int(np.prod(self.shape)) * self.dtype.itemsize
+        self.ptr = self.lib.pEVSL_B200_ManagedAlloc(nbytes)
+        if not self.ptr:
+            raise PevslError("pEVSL_B200_ManagedAlloc failed")
+        buf = (C.c_char * nbytes).from_address(self.ptr)
+        self.a = np.frombuffer(buf, dtype=self.dtype).reshape(self.shape)
+
+    def set(self, x):
+        self.lib.pEVSL_B200_Sync()
+        self.a[...] = x
+        return self
+
+    def get(self):
+        self.lib.pEVSL_B200_Sync()
+        return self.a.copy()
+
+    def free(self):
+        if self.ptr:
+            self.a = None
+            self.lib.pEVSL_B200_ManagedFree(self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Mlp:
+    """The learned-DOS network (pEVSL_B200_Mlp*): nin -> width -> ... -> nout,
+    GELU between the `layers` linear maps, BF16 weights, FP32 accumulation."""
+
+    def __init__(self, nin, width, nout, layers):
+        self.lib = load()
+        self.p = _vp()
+        _check(self.lib.pEVSL_B200_MlpCreate(C.byref(self.p), nin, width, nout, layers), "MlpCreate")
+        self.nin, self.width, self.nout, self.layers = nin, width, nout, layers
+        self.np = int(self.lib.pEVSL_B200_MlpParamCount(self.p))
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.np
+        _check(self.lib.pEVSL_B200_MlpSetParams(self.p, p.ctypes.data_as(C.POINTER(C.c_float))),
+               "MlpSetParams")
+
+    def get_params(self):
+        p = np.zeros(self.np, np.float32)
+        _check(self.lib.pEVSL_B200_MlpGetParams(self.p, p.ctypes.data_as(C.POINTER(C.c_float))),
+               "MlpGetParams")
+        return p
+
+    def forward(self, X: ManagedArray, Y: ManagedArray, B):
+        _check(self.lib.pEVSL_B200_MlpForward(self.p, X.ptr, Y.ptr, B), "MlpForward")
+
+    def gradients(self, X: ManagedArray, T: ManagedArray, B):
+        loss = C.c_float()
+        g = np.zeros(self.np, np.float32)
+        _check(self.lib.pEVSL_B200_MlpGradients(self.p, X.ptr, T.ptr, B, C.byref(loss),
+                                                g.ctypes.data_as(C.POINTER(C.c_float))),
+               "MlpGradients")
+        return float(loss.value), g
+
+    def train_step(self, X: ManagedArray, T: ManagedArray, B, lr, want_loss=False):
+        loss = C.c_float()
+        _check(self.lib.pEVSL_B200_MlpTrainStep(self.p, X.ptr, T.ptr, B, lr,
+                                                C.byref(loss) if want_loss else None),
+               "MlpTrainStep")
+        return float(loss.value) if want_loss else None
+
+    def close(self):
+        if self.p:
+            self.lib.pEVSL_B200_MlpFree(self.p)
+            self.p = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 # ---------------------------------------------------------------- whole run

@@ -476,6 +476,19 @@ void pEVSL_B200_HostFree(void *p) {
   if (p) cudaFreeHost(p);
 }
 
+void *pEVSL_B200_ManagedAlloc(size_t bytes) {
+  void *p = nullptr;
+  if (ensure() || fail(cudaMallocManaged(&p, bytes ? bytes : 1), "cudaMallocManaged")) return nullptr;
+  return p;
+}
+
+void pEVSL_B200_ManagedFree(void *p) {
+  if (p) {
+    cudaStreamSynchronize(g_ctx.stream);
+    cudaFree(p);
+  }
+}
+
 /* Wait for all work queued by the library. */
 int pEVSL_B200_Sync(void) {
   if (ensure()) return PEVSL_ERR_CUDA;

@@ -193,17 +193,18 @@ __device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
   const int nr = n - r0 < 32 * R ? n - r0 : 32 * R;
   typename Epi::Pre pre[R];
   int rs[R], re[R];
+  /* the matrix is read-only for every launch: the non-coherent path */
 #pragma unroll
   for (int j = 0; j < R; j++) {
     const int row = r0 + lane + 32 * j;
     rs[j] = re[j] = 0;
     if (lane + 32 * j < nr) {
       pre[j] = epi.pre(row);
-      rs[j] = ia[row];
-      re[j] = ia[row + 1];
+      rs[j] = __ldg(ia + row);
+      re[j] = __ldg(ia + row + 1);
     }
   }
-  const int base = ia[r0], len = ia[r0 + nr] - base;
+  const int base = __ldg(ia + r0), len = __ldg(ia + r0 + nr) - base;
   T acc[R];
 #pragma unroll
   for (int j = 0; j < R; j++) {
@@ -218,8 +219,8 @@ __device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
 #pragma unroll
     for (int q = 0; q < PL; q++) {
       const int t = c0 + q * 32 + lane;
-      col[q] = t < len ? ja[base + t] : -1;
-      val[q] = t < len ? a[base + t] : T(0);
+      col[q] = t < len ? __ldg(ja + base + t) : -1;
+      val[q] = t < len ? __ldg(a + base + t) : T(0);
     }
 #pragma unroll
     for (int q = 0; q < PL; q++) {
@@ -271,15 +272,17 @@ struct StreamBatch {
   int nb, shared;
 };
 
-template <int R, class T, class Epi, int CAP>
+/* SHARED: the one matrix comes as plain parameters (uniform operands, as in
+ * k_csr_stream); otherwise per entry from the table. */
+template <int R, class T, class Epi, int CAP, bool SHARED>
 __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
-    k_csr_stream_batch(const __grid_constant__ StreamBatch<T, Epi, CAP> b) {
+    k_csr_stream_batch(int n0, const int *__restrict__ ia0, const int *__restrict__ ja0,
+                       const T *__restrict__ a0, const __grid_constant__ StreamBatch<T, Epi, CAP> b) {
   __shared__ T prod[kThreads / 32][kStreamChunk * R];
-  int e;
-  long rblk;
-  if (b.shared) {
-    e = (int)(blockIdx.x % (unsigned)b.nb);
-    rblk = (long)(blockIdx.x / (unsigned)b.nb);
+  if constexpr (SHARED) {
+    const int e = (int)(blockIdx.x % (unsigned)b.nb);
+    stream_rows<R>(n0, ia0, ja0, a0, (const T *)b.epi[e].vk, b.epi[e],
+                   (long)(blockIdx.x / (unsigned)b.nb), prod);
   } else {
     int lo = 0, hi = b.nb; /* off[lo] <= blockIdx.x < off[hi] */
     while (hi - lo > 1) {
@@ -287,10 +290,9 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
       if (b.off[mid] <= (int)blockIdx.x) lo = mid;
       else hi = mid;
     }
-    e = lo;
-    rblk = (long)blockIdx.x - b.off[lo];
+    stream_rows<R>(b.n[lo], b.ia[lo], b.ja[lo], b.a[lo], (const T *)b.epi[lo].vk, b.epi[lo],
+                   (long)blockIdx.x - b.off[lo], prod);
   }
-  stream_rows<R>(b.n[e], b.ia[e], b.ja[e], b.a[e], (const T *)b.epi[e].vk, b.epi[e], rblk, prod);
 }
 
 /* ---------------------------------------------------------------- persistent filter */
@@ -704,10 +706,20 @@ static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const cha
   if (off <= 0) return 0;
   if (off > 0x7fffffffL) return PEVSL_ERR_ARG;
   const unsigned g = (unsigned)off;
-  if (R == 2)
-    k_csr_stream_batch<2, T, Epi, CAP><<<g, kThreads, 0, ctx().stream>>>(b);
-  else
-    k_csr_stream_batch<1, T, Epi, CAP><<<g, kThreads, 0, ctx().stream>>>(b);
+  const int n0 = b.n[0];
+  const int *ia0 = b.ia[0], *ja0 = b.ja[0];
+  const T *a0 = b.a[0];
+  if (b.shared) {
+    if (R == 2)
+      k_csr_stream_batch<2, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+    else
+      k_csr_stream_batch<1, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+  } else {
+    if (R == 2)
+      k_csr_stream_batch<2, T, Epi, CAP, false><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+    else
+      k_csr_stream_batch<1, T, Epi, CAP, false><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+  }
   return launched(what);
 }
 

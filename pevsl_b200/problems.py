@@ -103,3 +103,83 @@ def multi_laplacian_set(count: int = 32, seed: int = 2024, per_slice: int = 20):
                         intv=[float(x) + shift for x in edges], lmin=float(lo + shift - 1e-3),
                         lmax=float(hi + shift + 1e-3), counts=counts))
     return out
+
+
+def random_coef_laplacian(nx: int, ny: int, nz: int, seed: int, lo: float = 0.5, hi: float = 2.0):
+    """Dirichlet Laplacian on an nx x ny x nz grid (nz = 1: 2D) whose every
+    edge, including the edges to the boundary, has a weight drawn from
+    U[lo, hi]: A = sum_e c_e (e_i - e_j)(e_i - e_j)^T over interior edges
+    plus c_e e_i e_i^T for boundary edges.  Returns (n, ia, ja, a), rows
+    sorted by column."""
+    rng = np.random.default_rng(seed)
+    n = nx * ny * nz
+    idx = np.arange(n).reshape(nz, ny, nx)
+    diag = np.zeros(n)
+    rows, cols, vals = [], [], []
+    dims = [(nx, 2), (ny, 1)] + ([(nz, 0)] if nz > 1 else [])
+    for size, axis in dims:
+        # weights of the size+1 edges along this axis for every grid line
+        shape = list(idx.shape)
+        shape[axis] = size + 1
+        c = rng.uniform(lo, hi, shape)
+        lo_sl = [slice(None)] * 3
+        hi_sl = [slice(None)] * 3
+        lo_sl[axis] = slice(0, size)
+        hi_sl[axis] = slice(1, size + 1)
+        np.add.at(diag, idx.ravel(), (c[tuple(lo_sl)] + c[tuple(hi_sl)]).ravel())
+        # interior edges: between index i and i+1 along the axis, weight c[i+1]
+        a_sl = [slice(None)] * 3
+        b_sl = [slice(None)] * 3
+        w_sl = [slice(None)] * 3
+        a_sl[axis] = slice(0, size - 1)
+        b_sl[axis] = slice(1, size)
+        w_sl[axis] = slice(1, size)
+        i = idx[tuple(a_sl)].ravel()
+        j = idx[tuple(b_sl)].ravel()
+        w = c[tuple(w_sl)].ravel()
+        rows += [i, j]
+        cols += [j, i]
+        vals += [-w, -w]
+    rows.append(np.arange(n))
+    cols.append(np.arange(n))
+    vals.append(diag)
+    return _coo_to_csr(n, np.concatenate(rows), np.concatenate(cols), np.concatenate(vals))
+
+
+def random_sparse_symmetric(n: int, per_row: int, bandwidth: int, seed: int):
+    """Symmetric sparse matrix of the general-sparse family: per_row/2
+    off-diagonal entries drawn per row at column offsets uniform in
+    [1, bandwidth] (either side, clipped to the matrix), values N(0,1),
+    symmetrised as (B + B^T), duplicates summed, plus the diagonal
+    4 + U[0, 1].  About per_row nonzeros per row.  Returns (n, ia, ja, a)."""
+    rng = np.random.default_rng(seed)
+    h = max(1, per_row // 2)
+    i = np.repeat(np.arange(n), h)
+    off = rng.integers(1, bandwidth + 1, size=i.size) * np.where(rng.random(i.size) < 0.5, -1, 1)
+    j = np.clip(i + off, 0, n - 1)
+    keep = j != i
+    i, j = i[keep], j[keep]
+    v = rng.standard_normal(i.size)
+    # sum duplicates on the upper triangle, then mirror: exactly symmetric
+    lo, hi = np.minimum(i, j), np.maximum(i, j)
+    _, iu, ju, vu = _coo_to_csr(n, lo, hi, v)
+    ru = np.repeat(np.arange(n), np.diff(iu))
+    rows = np.concatenate([ru, ju, np.arange(n)])
+    cols = np.concatenate([ju, ru, np.arange(n)])
+    vals = np.concatenate([vu, vu, 4.0 + rng.random(n)])
+    return _coo_to_csr(n, rows, cols, vals)
+
+
+def _coo_to_csr(n, rows, cols, vals):
+    """CSR (int32 indices, rows sorted by column, duplicates summed)."""
+    key = rows.astype(np.int64) * n + cols
+    order = np.argsort(key, kind="stable")
+    key, vals = key[order], vals[order]
+    uniq, start = np.unique(key, return_index=True)
+    sums = np.add.reduceat(vals, start)
+    r = (uniq // n).astype(np.int64)
+    c = (uniq % n).astype(np.int32)
+    ia = np.zeros(n + 1, np.int32)
+    np.add.at(ia, r + 1, 1)
+    ia = np.cumsum(ia).astype(np.int32)
+    return n, ia, c, np.ascontiguousarray(sums, dtype=np.float64)
