@@ -56,6 +56,16 @@ int pEVSL_B200_SetPrecision(pevsl_Data *pevsl, int precision);
  * bits either way.  PEVSL_B200_FILTER_FORM sets the start value. */
 int pEVSL_B200_SetFilterForm(int form);
 
+/* The cross-group sum of a split KPM: pEVSL_Kpmdos with ngroups > 1 computes
+ * the moments of its group's share of the random vectors (pEVSL_Part1d)
+ * and then, in place of MPI_Allreduce on gl_comm (SRC/kpmdos.c:160-176),
+ * calls reduce(buf, Mdeg + 2, ctx) with buf = [partial moments mu[0..Mdeg],
+ * partial count]; reduce must leave the sums over all groups in buf (with
+ * one process per GPU: an all-reduce over the processes).  NULL restores
+ * MPI. */
+int pEVSL_B200_SetGroupReduce(pevsl_Data *pevsl, void (*reduce)(double *buf, int count, void *ctx),
+                              void *ctx);
+
 /* Slices of the last pEVSL_ChebLanNr / pEVSL_B200_ChebLanNrBatch /
  * pEVSL_B200_ChebLanNrMulti call that the mixed form solved again in FP64. */
 int pEVSL_B200_LastFallbacks(void);

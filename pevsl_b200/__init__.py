@@ -179,6 +179,7 @@ SIGNATURES = [
     ("pEVSL_B200_SetPrecision", _I, [C.POINTER(PevslData), _I]),
     ("pEVSL_B200_LastFallbacks", _I, []),
     ("pEVSL_B200_SetFilterForm", _I, [_I]),
+    ("pEVSL_B200_SetGroupReduce", _I, [C.POINTER(PevslData), _vp, _vp]),
     ("pEVSL_B200_ChebLanNrBatch", _I, [C.POINTER(PevslData), _I, _dp, _ip, _D,
                                        C.POINTER(Parvec), C.POINTER(Polparams), _ip,
                                        C.POINTER(_dp), C.POINTER(C.POINTER(Parvecs)),
@@ -416,12 +417,15 @@ class Instance:
     def __exit__(self, *exc):
         self.close()
 
-    def kpmdos(self, Mdeg, damping, nvec, intv):
+    def kpmdos(self, Mdeg, damping, nvec, intv, ngroups=1, groupid=0):
+        """pEVSL_Kpmdos; with ngroups > 1 this instance computes group
+        `groupid`'s share of the vectors and the sum over the groups goes
+        through the reduction installed by pEVSL_B200_SetGroupReduce."""
         mu = np.zeros(Mdeg + 1)
         ec = C.c_double()
         iv = np.asarray(intv, dtype=np.float64)
-        r = self.lib.pEVSL_Kpmdos(self.p, Mdeg, damping, nvec, _ptr(iv), 1, 0, 0, _ptr(mu),
-                                  C.byref(ec))
+        r = self.lib.pEVSL_Kpmdos(self.p, Mdeg, damping, nvec, _ptr(iv), ngroups, groupid, 0,
+                                  _ptr(mu), C.byref(ec))
         return r, mu, ec.value
 
     def landos(self, nvec, msteps, npts, intv):

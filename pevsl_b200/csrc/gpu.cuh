@@ -160,6 +160,8 @@ int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1,
  *   Xkp1 = (A Xk - ctr Xk) sc - Xkm1;   mom[c] = <Xkp1[:,c], V0[:,c]>   */
 int kpm_step(const pevsl_devcsr *A, int s, int ld, const double *Xk, const double *Xkm1,
              double *Xkp1, const double *V0, double ctr, double sc, double *mom);
+/* out[c] = sum_b partials[b*s + c] over nb blocks, fixed order */
+int col_reduce(const double *partials, int nb, int s, double *out);
 /* Column sums of squares of an interleaved block: out[c] = sum_i X[i*ld+c]^2 */
 int block_colnorm2(long n, int s, int ld, const double *X, double *out);
 /* X[i*ld+c] *= 1/sqrt(nrm2[c]) */

@@ -45,7 +45,6 @@ __global__ void __launch_bounds__(kThreads)
                  const float *__restrict__ V0, float ctr, float sc, double *partials,
                  unsigned *counter, double *mom) {
   __shared__ float acc_sh[kThreads / 32][32 * CPL];
-  __shared__ bool am_last;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
   float acc[CPL];
@@ -96,18 +95,8 @@ __global__ void __launch_bounds__(kThreads)
     for (int w = 0; w < wpb; w++) t += acc_sh[w][c];
     partials[(size_t)blockIdx.x * s + c] = (double)t;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  for (int c = threadIdx.x; c < s; c += blockDim.x) {
-    double t = 0.0;
-    for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(partials + (size_t)b * s + c);
-    mom[c] = t;
-  }
-  if (threadIdx.x == 0) *counter = 0;
+  /* the columns are added across blocks by k_col_reduce */
+  (void)counter;
 }
 
 int kpm_step32(const pevsl_devcsr *A, int s, int ld, const float *Xk, const float *Xkm1,
@@ -122,7 +111,8 @@ int kpm_step32(const pevsl_devcsr *A, int s, int ld, const float *Xk, const floa
   } else {
     k_kpm_step32<2><<<(unsigned)g, kThreads, 0, ctx().stream>>>(A->nrows, s, ld, A->ia, A->ja, A->a32, Xk, Xkm1, Xkp1, V0, (float)ctr, (float)sc, ctx().red, ctx().cnt, mom);
   }
-  return launched("kpm_step32");
+  if (launched("kpm_step32")) return PEVSL_ERR_CUDA;
+  return col_reduce(ctx().red, (int)g, s, mom);
 }
 
 /* y = (float) x for an interleaved block */

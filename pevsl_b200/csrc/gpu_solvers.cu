@@ -395,6 +395,12 @@ int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *int
   double tcnt = 0.0;
   int vec_start = 0, vec_end = nvec;
   if (ngroups > 1) pEVSL_Part1d(nvec, ngroups, &groupid, &vec_start, &vec_end, 1);
+  /* counter-based Gaussian stream: a group starts at its first vector's
+   * draw, so the groups' vectors are exactly one process's nvec vectors and
+   * the summed moments equal the one-group moments (the C library stream is
+   * per process, as the reference's per-rank srand) */
+  if (ngroups > 1 && pevsl_rng_mode() == PEVSL_RNG_GAUSS && vec_start > 0)
+    pevsl_rng_take((uint64_t)vec_start);
   pevsl_devcsr *A = pevsl_builtin_A(pevsl);
   int st = 0;
   cudaEvent_t e0, e1;
@@ -544,12 +550,25 @@ int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *int
   free(jac);
   if (st) return st;
   if (ngroups > 1) {
-    double *mu_g = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1));
-    double tcnt_g = 0.0;
-    MPI_Allreduce(mu, mu_g, Mdeg + 1, MPI_DOUBLE, MPI_SUM, gl_comm);
-    MPI_Allreduce(&tcnt, &tcnt_g, 1, MPI_DOUBLE, MPI_SUM, gl_comm);
-    memcpy(mu, mu_g, sizeof(double) * (size_t)(Mdeg + 1));
-    tcnt = tcnt_g;
+    /* the groups' partial sums (SRC/kpmdos.c:160-176): through the
+     * instance's reduction (one process per GPU) when one is installed,
+     * else MPI on gl_comm */
+    pevsl_inst *inst = pevsl_inst_of(pevsl);
+    double *mu_g = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 2));
+    if (!mu_g) return PEVSL_ERR_NOMEM;
+    if (inst->group_reduce) {
+      memcpy(mu_g, mu, sizeof(double) * (size_t)(Mdeg + 1));
+      mu_g[Mdeg + 1] = tcnt;
+      inst->group_reduce(mu_g, Mdeg + 2, inst->group_reduce_ctx);
+      memcpy(mu, mu_g, sizeof(double) * (size_t)(Mdeg + 1));
+      tcnt = mu_g[Mdeg + 1];
+    } else {
+      double tcnt_g = 0.0;
+      MPI_Allreduce(mu, mu_g, Mdeg + 1, MPI_DOUBLE, MPI_SUM, gl_comm);
+      MPI_Allreduce(&tcnt, &tcnt_g, 1, MPI_DOUBLE, MPI_SUM, gl_comm);
+      memcpy(mu, mu_g, sizeof(double) * (size_t)(Mdeg + 1));
+      tcnt = tcnt_g;
+    }
     free(mu_g);
   }
   const double t = 1.0 / (((double)nvec) * M_PI);
@@ -1151,6 +1170,15 @@ static void free_slice_outputs(SliceState *S) {
 static int g_fallbacks = 0; /* slices of the last call re-run in FP64 */
 
 int pEVSL_B200_LastFallbacks(void) { return g_fallbacks; }
+
+int pEVSL_B200_SetGroupReduce(pevsl_Data *pevsl, void (*reduce)(double *buf, int count, void *ctx),
+                              void *ctx) {
+  if (!pevsl) return PEVSL_ERR_ARG;
+  pevsl_inst *inst = pevsl_inst_of(pevsl);
+  inst->group_reduce = reduce;
+  inst->group_reduce_ctx = ctx;
+  return 0;
+}
 
 int pEVSL_B200_SetFilterForm(int form) {
   if (form < -1 || form > 1) return PEVSL_ERR_ARG;

@@ -541,7 +541,6 @@ __global__ void __launch_bounds__(kThreads)
                const double *__restrict__ V0, double ctr, double sc, double *partials,
                unsigned *counter, double *mom) {
   __shared__ double acc_sh[kThreads / 32][32 * CPL];
-  __shared__ bool am_last;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
   double acc[CPL];
@@ -597,25 +596,14 @@ __global__ void __launch_bounds__(kThreads)
     for (int w = 0; w < wpb; w++) t += acc_sh[w][c];
     partials[(size_t)blockIdx.x * s + c] = t;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  for (int c = threadIdx.x; c < s; c += blockDim.x) {
-    double t = 0.0;
-    for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(partials + (size_t)b * s + c);
-    mom[c] = t;
-  }
-  if (threadIdx.x == 0) *counter = 0;
+  /* the columns are added across blocks by k_col_reduce */
+  (void)counter;
 }
 
 /* out[c] = sum_i X[i*ld + c]^2: per-block partials, last block adds them */
 __global__ void k_block_colnorm2(long n, int s, int ld, const double *__restrict__ X,
                                  double *partials, unsigned *counter, double *out) {
   __shared__ double acc_sh[kThreads / 32][64];
-  __shared__ bool am_last;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, wpb = blockDim.x >> 5;
   double acc[2] = {0.0, 0.0};
   for (long row = blockIdx.x * wpb + wib; row < n; row += (long)gridDim.x * wpb) {
@@ -635,18 +623,8 @@ __global__ void k_block_colnorm2(long n, int s, int ld, const double *__restrict
     for (int w = 0; w < wpb; w++) t += acc_sh[w][c];
     partials[(size_t)blockIdx.x * s + c] = t;
   }
-  __threadfence();
-  __syncthreads();
-  if (threadIdx.x == 0) am_last = atomicAdd(counter, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!am_last) return;
-  __threadfence();
-  for (int c = threadIdx.x; c < s; c += blockDim.x) {
-    double t = 0.0;
-    for (unsigned b = 0; b < gridDim.x; b++) t += __ldcg(partials + (size_t)b * s + c);
-    out[c] = t;
-  }
-  if (threadIdx.x == 0) *counter = 0;
+  /* the columns are added across blocks by k_col_reduce */
+  (void)counter;
 }
 
 __global__ void k_block_normalize(long n, int s, int ld, double *X, const double *nrm2) {
@@ -776,6 +754,22 @@ int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1,
   return launched("cheb_combine");
 }
 
+/* out[c] = sum over nb blocks of partials[b*s + c]: one block per column,
+ * thread t adds blocks t, t + 256, ... and a fixed tree adds the threads */
+__global__ void k_col_reduce(const double *__restrict__ partials, int nb, int s, double *out) {
+  __shared__ double sh[32];
+  const int c = blockIdx.x;
+  double t = 0.0;
+  for (int b = threadIdx.x; b < nb; b += blockDim.x) t += partials[(size_t)b * s + c];
+  t = block_sum(t, sh);
+  if (threadIdx.x == 0) out[c] = t;
+}
+
+int col_reduce(const double *partials, int nb, int s, double *out) {
+  k_col_reduce<<<s, kThreads, 0, ctx().stream>>>(partials, nb, s, out);
+  return launched("col_reduce");
+}
+
 static unsigned warp_row_grid(long n) {
   const long wpb = kThreads / 32;
   long g = (n + wpb - 1) / wpb;
@@ -794,14 +788,16 @@ int kpm_step(const pevsl_devcsr *A, int s, int ld, const double *Xk, const doubl
     k_kpm_step<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, s, ld, A->ia, A->ja, A->a, Xk, Xkm1,
                                                     Xkp1, V0, ctr, sc, ctx().red, ctx().cnt, mom);
   }
-  return launched("kpm_step");
+  if (launched("kpm_step")) return PEVSL_ERR_CUDA;
+  return col_reduce(ctx().red, (int)g, s, mom);
 }
 
 int block_colnorm2(long n, int s, int ld, const double *X, double *out) {
   if (s < 1 || s > 64) return PEVSL_ERR_ARG;
-  k_block_colnorm2<<<warp_row_grid(n), kThreads, 0, ctx().stream>>>(n, s, ld, X, ctx().red,
-                                                                     ctx().cnt, out);
-  return launched("block_colnorm2");
+  const unsigned g = warp_row_grid(n);
+  k_block_colnorm2<<<g, kThreads, 0, ctx().stream>>>(n, s, ld, X, ctx().red, ctx().cnt, out);
+  if (launched("block_colnorm2")) return PEVSL_ERR_CUDA;
+  return col_reduce(ctx().red, (int)g, s, out);
 }
 
 int block_normalize(long n, int s, int ld, double *X, const double *nrm2) {

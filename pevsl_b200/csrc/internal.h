@@ -25,6 +25,9 @@ typedef struct pevsl_inst {
   int last_its, last_nconv;
   double phase_ms[8];
   int precision; /* PEVSL_PREC_FP64 or PEVSL_PREC_MIXED */
+  /* sum across the groups of a split KPM (pEVSL_B200_SetGroupReduce) */
+  void (*group_reduce)(double *buf, int count, void *ctx);
+  void *group_reduce_ctx;
 } pevsl_inst;
 
 static inline pevsl_inst *pevsl_inst_of(pevsl_Data *d) { return (pevsl_inst *)d; }

@@ -498,3 +498,29 @@ def test_multi_problem_equals_separate(gpu):
             assert np.max(np.abs(b["lam"] - ex)) <= 1e-10 * np.max(np.abs(ex))
     for ev in insts:
         ev.close()
+
+
+def test_kpm_groups_sum_to_one_group(gpu):
+    """pEVSL_Kpmdos with the vectors split over two groups (SRC/kpmdos.c:
+    97-102): in the counter-based Gaussian stream each group draws exactly
+    its share of one process's vectors, so the groups' moments and counts
+    (left unsummed by a no-op reduction) add up to the one-group result."""
+    from pevsl_b200.distributed import REDUCE_FN
+    lib = pv.load()
+    A = dev_matrix(laplacian(20, 20, 20))
+    intv = [0.6, 1.2, 0.0, 12.0]
+    noop = REDUCE_FN(lambda buf, n, ctx: None)
+    with pv.Instance(A) as ev:
+        pv.set_rng(pv.RNG_GAUSS, 3)
+        r, mu, ec = ev.kpmdos(100, 1, 30, intv)
+        assert r == 0
+        lib.pEVSL_B200_SetGroupReduce(ev.p, C.cast(noop, C.c_void_p), None)
+        parts = []
+        for g in range(2):
+            pv.set_rng(pv.RNG_GAUSS, 3)
+            r, mu_g, ec_g = ev.kpmdos(100, 1, 30, intv, ngroups=2, groupid=g)
+            assert r == 0
+            parts.append((mu_g, ec_g))
+        lib.pEVSL_B200_SetGroupReduce(ev.p, None, None)
+    assert rel(parts[0][0] + parts[1][0], mu) <= 1e-13
+    assert abs(parts[0][1] + parts[1][1] - ec) <= 1e-12 * abs(ec)
