@@ -49,11 +49,14 @@ uint64_t pEVSL_B200_RngDraws(void);
 #define PEVSL_PREC_MIXED 1
 int pEVSL_B200_SetPrecision(pevsl_Data *pevsl, int precision);
 
-/* Form of the batched filter: -1 automatic (one launch per degree), 0 one
- * launch per degree serving every slice still filtering, 1 one persistent
- * cooperative launch running every degree of every slice (per-slice degree
- * counters, a grid barrier between degrees).  The results are the same
- * bits either way.  PEVSL_B200_FILTER_FORM sets the start value. */
+/* Form of the batched filter: -1 automatic (= 2), 0 one launch per degree
+ * serving every slice still filtering, 1 one persistent cooperative launch
+ * running every degree of every slice (per-slice degree counters, a grid
+ * barrier between degrees), 2 the launches of form 0 captured once per set
+ * of live slices in a CUDA graph and replayed at every Lanczos step (the
+ * slices' input and output pass through staging vectors in their work
+ * space).  The results are the same bits in every form.
+ * PEVSL_B200_FILTER_FORM sets the start value. */
 int pEVSL_B200_SetFilterForm(int form);
 
 /* The cross-group sum of a split KPM: pEVSL_Kpmdos with ngroups > 1 computes
@@ -86,6 +89,13 @@ double pEVSL_B200_PhaseMs(pevsl_Data *pevsl, int phase);
 /* Synchronous copy between host memory and library memory (device or
  * managed), either direction; and a wait for all queued library work. */
 int pEVSL_B200_Memcpy(void *dst, const void *src, size_t bytes);
+
+/* The first nvec eigenvectors of a pEVSL_ChebLanNr result (Wo) into the
+ * caller's array: vector i (n_local values) to vec + i * ld, ld >= n_local;
+ * vec may be host or device memory.  What the reference's Fortran
+ * pevsl_copy_result does for its saved result (FORTRAN/pevsl_f90.c:311-331),
+ * as one strided copy. */
+int pEVSL_B200_CopyEigenvectors(const pevsl_Parvecs *W, int nvec, double *vec, long ld);
 int pEVSL_B200_Sync(void);
 
 /* Sticky CUDA error of the void entry points (pEVSL_Parvec*, ...): returns

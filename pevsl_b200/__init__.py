@@ -179,6 +179,7 @@ SIGNATURES = [
     ("pEVSL_B200_SetPrecision", _I, [C.POINTER(PevslData), _I]),
     ("pEVSL_B200_LastFallbacks", _I, []),
     ("pEVSL_B200_SetFilterForm", _I, [_I]),
+    ("pEVSL_B200_CopyEigenvectors", _I, [C.POINTER(Parvecs), _I, _dp, C.c_long]),
     ("pEVSL_B200_SetGroupReduce", _I, [C.POINTER(PevslData), _vp, _vp]),
     ("pEVSL_B200_ChebLanNrBatch", _I, [C.POINTER(PevslData), _I, _dp, _ip, _D,
                                        C.POINTER(Parvec), C.POINTER(Polparams), _ip,
@@ -470,10 +471,10 @@ class Instance:
             order = np.argsort(lam_a, kind="stable")
             out["lam"], out["res"] = lam_a[order], res_a[order]
             if want_vectors and m:
-                Wh = np.empty((W.contents.n_vecs, W.contents.ld))
-                _check(self.lib.pEVSL_B200_Memcpy(Wh.ctypes.data, W.contents.data, Wh.nbytes),
-                       "memcpy")
-                out["W"] = Wh[order, : self.n].copy() if m else None
+                Wh = np.empty((m, self.n))
+                _check(self.lib.pEVSL_B200_CopyEigenvectors(W, m, _ptr(Wh), self.n),
+                       "CopyEigenvectors")
+                out["W"] = Wh[order].copy()
             if lam:
                 libc.free(C.cast(lam, _vp))
             if res:

@@ -209,6 +209,8 @@ struct ChebEntry {
   int first;
 };
 int cheb_step_batch(int nb, const ChebEntry *e, bool fp32);
+/* choose the CSR-stream rows per lane of a matrix by timing (once) */
+int stream_tune(pevsl_devcsr *A);
 
 /* One entry of the persistent filter: y = p(A) x for its own matrix and
  * polynomial (mu on the device).  FP64 entries: b0, b1 are two work vectors

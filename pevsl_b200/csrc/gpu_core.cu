@@ -438,6 +438,20 @@ int pEVSL_B200_Memcpy(void *dst, const void *src, size_t bytes) {
   return sync();
 }
 
+int pEVSL_B200_CopyEigenvectors(const pevsl_Parvecs *W, int nvec, double *vec, long ld) {
+  if (!W || nvec < 0 || nvec > W->n_vecs || (nvec > 0 && (!vec || ld < W->n_local)))
+    return PEVSL_ERR_ARG;
+  if (nvec == 0 || W->n_local == 0) return 0;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  /* one strided copy: column i of W (ld W->ld) to vec + i * ld */
+  if (fail(cudaMemcpy2DAsync(vec, sizeof(double) * (size_t)ld, W->data, sizeof(double) * (size_t)W->ld,
+                             sizeof(double) * (size_t)W->n_local, (size_t)nvec, cudaMemcpyDefault,
+                             g_ctx.stream),
+           "cudaMemcpy2DAsync"))
+    return PEVSL_ERR_CUDA;
+  return sync();
+}
+
 int pEVSL_B200_SetDevice(int device) {
   if (g_ctx.ready) return g_ctx.device == device ? 0 : PEVSL_ERR_ARG;
   g_req_device = device;

@@ -158,18 +158,21 @@ struct FilterJob {
 
 /* Form of the batched filter: 0 = one cheb_step_batch launch per degree
  * serving every entry (any matrices, up to kMaxEntries), 1 = one persistent
- * cooperative launch for all degrees and entries.  One launch per degree is
- * the default: measured faster (81 vs 119 us per degree for 4 slices at
- * 10^6 rows, 4.1 vs 6.1 us at 8000 rows), the grid barrier costing more
- * than the gap between launches. */
-static int g_filter_form_override = -1; /* -1: not read yet, 2: automatic */
-static int filter_form() {
+ * cooperative launch for all degrees and entries, 2 (default) = the
+ * launches of form 0 captured in a CUDA graph per set of live slices and
+ * replayed (filter_graphed).  One launch per degree beat the persistent
+ * kernel (81 vs 119 us per degree for 4 slices at 10^6 rows, 4.1 vs 6.1 us
+ * at 8000 rows): the grid barrier costs more than the gap between launches. */
+static int g_filter_form_override = -1; /* -1: not read yet */
+static int filter_form_setting() {
   if (g_filter_form_override < 0) {
     const char *e = getenv("PEVSL_B200_FILTER_FORM");
-    g_filter_form_override = e ? atoi(e) : 2;
+    const int v = e ? atoi(e) : 2;
+    g_filter_form_override = (v >= 0 && v <= 2) ? v : 2;
   }
-  return g_filter_form_override == 1 ? 1 : 0;
+  return g_filter_form_override;
 }
+static int filter_form() { return filter_form_setting() == 1 ? 1 : 0; }
 
 static double filter_bytes_degree(const pevsl_devcsr *A, int deg_k, bool fp32, bool last) {
   const double n = A->nrows, vb = fp32 ? 4.0 : 8.0;
@@ -314,6 +317,77 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     g_filter_launches++;
     g_filter_bytes += bytes;
   }
+  return st;
+}
+
+/* CUDA graph form of one batched filter application.  The degrees read the
+ * input from, and accumulate into, two staging vectors in each slice's
+ * work space (at 16 ld and 24 ld bytes), so that the launch sequence of a
+ * given set of slices never changes: it is captured once (all degrees, the
+ * FP32 conversion included) and replayed, with one copy in and one copy out
+ * per slice around it.  A new set of live slices is captured anew. */
+static bool filter_graph_enabled() { return filter_form_setting() == 2; }
+
+struct FilterGraph {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<char> key; /* live slices of the captured sequence */
+  bool mixed = false;
+  uint64_t launches = 0, kernel_launches = 0;
+  double bytes = 0.0;
+  ~FilterGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+static int filter_graphed(FilterGraph &fg, const std::vector<char> &sel, std::vector<FilterJob> &jobs) {
+  Ctx &c = ctx();
+  const int ne = (int)jobs.size();
+  std::vector<FilterJob> staged(jobs);
+  int st = 0;
+  for (int e = 0; e < ne && !st; e++) {
+    double *xs = (double *)((char *)jobs[e].work + 16 * (size_t)jobs[e].ld);
+    st = memcpy_async(xs, jobs[e].x, sizeof(double) * (size_t)jobs[e].A->nrows);
+    staged[e].x = xs;
+    staged[e].y = xs + jobs[e].ld;
+  }
+  if (st) return st;
+  if (!fg.exec || fg.key != sel) {
+    if (fg.exec) cudaGraphExecDestroy(fg.exec);
+    fg.exec = nullptr;
+    const uint64_t l0 = g_filter_launches, k0 = c.launches;
+    const double b0 = g_filter_bytes;
+    if (fail(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal), "BeginCapture"))
+      return PEVSL_ERR_CUDA;
+    st = cheb_filter_batch(ne, staged.data(), fg.mixed);
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c.stream, &gr);
+    if (st || fail(ec, "EndCapture")) {
+      if (gr) cudaGraphDestroy(gr);
+      return st ? st : PEVSL_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&fg.exec, gr, 0);
+    cudaGraphDestroy(gr);
+    if (fail(ei, "cudaGraphInstantiate")) {
+      fg.exec = nullptr;
+      return PEVSL_ERR_CUDA;
+    }
+    fg.key = sel;
+    fg.launches = g_filter_launches - l0;
+    fg.kernel_launches = c.launches - k0;
+    fg.bytes = g_filter_bytes - b0;
+  } else {
+    /* the statistics a direct call would have counted */
+    for (int e = 0; e < ne; e++) {
+      jobs[e].pevsl->stats->n_polAv++;
+      jobs[e].pevsl->stats->n_mvA += (size_t)PEVSL_MAX(jobs[e].pol->deg, 0);
+    }
+    g_filter_launches += fg.launches;
+    g_filter_bytes += fg.bytes;
+    c.launches += fg.kernel_launches;
+  }
+  if (fail(cudaGraphLaunch(fg.exec, c.stream), "cudaGraphLaunch")) return PEVSL_ERR_CUDA;
+  for (int e = 0; e < ne && !st; e++)
+    st = memcpy_async(jobs[e].y, staged[e].y, sizeof(double) * (size_t)jobs[e].A->nrows);
   return st;
 }
 
@@ -1181,7 +1255,7 @@ int pEVSL_B200_SetGroupReduce(pevsl_Data *pevsl, void (*reduce)(double *buf, int
 }
 
 int pEVSL_B200_SetFilterForm(int form) {
-  if (form < -1 || form > 1) return PEVSL_ERR_ARG;
+  if (form < -1 || form > 2) return PEVSL_ERR_ARG;
   g_filter_form_override = form < 0 ? 2 : form;
   return 0;
 }
@@ -1244,10 +1318,13 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
     act[s] = 1;
     nact++;
     basis_elems += (size_t)S->ld * ((size_t)S->maxit + 1);
-    work_bytes += 16 * (size_t)S->ld;
+    work_bytes += 32 * (size_t)S->ld; /* filter work + the graph form's staging */
     mu_elems += (size_t)S->pol->deg + 1;
   }
   if (!nact) return 0;
+  /* tune each matrix's stream kernels now: the filter may be captured */
+  for (int s = 0; s < ns; s++)
+    if (act[s] && SL[s].A && stream_tune(SL[s].A)) return PEVSL_ERR_CUDA;
   if (mixed)
     for (int s = 0; s < ns; s++)
       if (act[s] && csr_make_fp32(SL[s].A)) return PEVSL_ERR_NOMEM;
@@ -1272,7 +1349,7 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
     off += (size_t)S->ld * ((size_t)S->maxit + 1);
     if (batched) {
       work[s] = bwork + woff;
-      woff += 16 * (size_t)S->ld;
+      woff += 32 * (size_t)S->ld;
       dmu[s] = dmu_all + moff;
       st = memcpy_async(dmu_all + moff, S->pol->mu, sizeof(double) * ((size_t)S->pol->deg + 1));
       moff += (size_t)S->pol->deg + 1;
@@ -1287,6 +1364,11 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
   }
   if (st) return st;
   SegTimer &t_pol = g_t_pol, &t_orth = g_t_orth;
+  /* CUDA graph form of the batched filter: one captured launch sequence per
+   * set of live slices, replayed every step */
+  const bool graph_form = batched && filter_form() == 0 && filter_graph_enabled();
+  FilterGraph fg;
+  fg.mixed = mixed;
   /* y_s = p_s(A_s) x_s for the slices with sel[s]: x_s = V_s(:,kin) (or the
    * slice's start vector when xin), y_s = V_s(:,kout) */
   auto filter = [&](const std::vector<char> &sel, int kin, bool xin, int kout) -> int {
@@ -1307,7 +1389,10 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
                                    xin ? SL[s].vinit->data : SL[s].V + (size_t)kin * SL[s].ld,
                                    SL[s].V + (size_t)kout * SL[s].ld, SL[s].pol, dmu[s], work[s],
                                    SL[s].ld});
-      r = cheb_filter_batch((int)jobs.size(), jobs.data(), mixed);
+      if (graph_form)
+        r = filter_graphed(fg, sel, jobs);
+      else
+        r = cheb_filter_batch((int)jobs.size(), jobs.data(), mixed);
     }
     t_pol.end();
     return r;

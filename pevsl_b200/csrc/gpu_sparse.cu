@@ -295,6 +295,131 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
   }
 }
 
+/* Grouped form of the shared-matrix batch: block b serves row block
+ * b / ngroups for the G slices of group b % ngroups.  A warp loads its rows'
+ * column indices and values once, prefetches every slice's epilogue
+ * operands, issues every slice's gathers x_s[col] together as asynchronous
+ * copies into shared memory (cp.async: no registers held while they fly),
+ * then forms the products and sums each slice's rows in index order -- the
+ * arithmetic of stream_rows, bit for bit.  The matrix stretch is read once
+ * per group instead of once per slice. */
+template <class T>
+__device__ __forceinline__ void gather_async(T *dst, const T *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T))
+               : "memory");
+}
+
+template <class T, class Epi, int CAP, int G>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_csr_stream_group(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+                       const T *__restrict__ a, const __grid_constant__ StreamBatch<T, Epi, CAP> b,
+                       int ngroups) {
+  extern __shared__ __align__(16) unsigned char dyn_raw[];
+  T(*xs)[G][kStreamChunk] = reinterpret_cast<T(*)[G][kStreamChunk]>(dyn_raw);
+  constexpr int PL = kStreamChunk / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const long rblk = blockIdx.x / (unsigned)ngroups;
+  const int g0 = (int)(blockIdx.x % (unsigned)ngroups) * G;
+  const int ng = b.nb - g0 < G ? b.nb - g0 : G;
+  const long r0l = (rblk * (kThreads / 32) + w) * 32;
+  if (r0l >= n) return;
+  const int r0 = (int)r0l;
+  const int nr = n - r0 < 32 ? n - r0 : 32;
+  const int row = r0 + lane;
+  typename Epi::Pre pre[G];
+  int rs = 0, re = 0;
+  if (lane < nr) {
+#pragma unroll
+    for (int j = 0; j < G; j++)
+      if (j < ng) pre[j] = b.epi[g0 + j].pre(row);
+    rs = __ldg(ia + row);
+    re = __ldg(ia + row + 1);
+  }
+  const int base = __ldg(ia + r0), len = __ldg(ia + r0 + nr) - base;
+  rs -= base;
+  re -= base;
+  T acc[G];
+#pragma unroll
+  for (int j = 0; j < G; j++) acc[j] = T(0);
+  for (int c0 = 0; c0 < len; c0 += kStreamChunk) {
+    int col[PL];
+    T val[PL];
+#pragma unroll
+    for (int q = 0; q < PL; q++) {
+      const int t = c0 + q * 32 + lane;
+      col[q] = t < len ? __ldg(ja + base + t) : -1;
+      val[q] = t < len ? __ldg(a + base + t) : T(0);
+    }
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+      if (j >= ng) break;
+      const T *x = (const T *)b.epi[g0 + j].vk;
+#pragma unroll
+      for (int q = 0; q < PL; q++) {
+        T *d = &xs[w][j][q * 32 + lane];
+        if (col[q] >= 0)
+          gather_async(d, x + col[q]);
+        else
+          *d = T(0);
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+      if (j >= ng) break;
+#pragma unroll
+      for (int q = 0; q < PL; q++) {
+        T *d = &xs[w][j][q * 32 + lane];
+        *d = mul_rn(val[q], *d);
+      }
+    }
+    __syncwarp();
+    const int lo = rs > c0 ? rs : c0;
+    const int hi = re < c0 + kStreamChunk ? re : c0 + kStreamChunk;
+#pragma unroll
+    for (int j = 0; j < G; j++) {
+      if (j >= ng) break;
+      for (int t = lo; t < hi; t++) acc[j] = add_rn(acc[j], xs[w][j][t - c0]);
+    }
+    __syncwarp();
+  }
+  if (lane < nr) {
+#pragma unroll
+    for (int j = 0; j < G; j++)
+      if (j < ng) b.epi[g0 + j](row, acc[j], pre[j]);
+  }
+}
+
+/* 0: grid-interleaved blocks (k_csr_stream_batch), 1: grouped blocks
+ * (k_csr_stream_group); PEVSL_B200_BATCH_KERNEL */
+static int batch_kernel() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("PEVSL_B200_BATCH_KERNEL");
+    v = e ? (atoi(e) == 1) : 0;
+  }
+  return v;
+}
+
+template <class T, class Epi, int CAP>
+static void launch_group(const StreamBatch<T, Epi, CAP> &b, int n0, const int *ia0, const int *ja0,
+                         const T *a0) {
+  constexpr int G = 4;
+  const size_t smem = sizeof(T) * (kThreads / 32) * G * kStreamChunk;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_csr_stream_group<T, Epi, CAP, G>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  const int ngroups = (b.nb + G - 1) / G;
+  const unsigned g = (unsigned)(((n0 + kThreads - 1) / kThreads) * (long)ngroups);
+  k_csr_stream_group<T, Epi, CAP, G><<<g, kThreads, smem, ctx().stream>>>(n0, ia0, ja0, a0, b,
+                                                                          ngroups);
+}
+
 /* ---------------------------------------------------------------- persistent filter */
 
 constexpr unsigned kBarrierSpins = 1u << 24; /* ~2 s of polling before giving up */
@@ -514,15 +639,8 @@ int persistent_filter_error() {
   return 0;
 }
 
-/* rows per lane of the CSR-stream kernels: 1 or 2 (PEVSL_B200_STREAM_R) */
-static int stream_r() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("PEVSL_B200_STREAM_R");
-    v = (e && atoi(e) == 2) ? 2 : 1;
-  }
-  return v;
-}
+/* Rows per lane of the CSR-stream kernels, per matrix: 1 until tuned */
+static int stream_r(const pevsl_devcsr *A) { return A && A->stream_r == 2 ? 2 : 1; }
 
 static unsigned stream_grid(int n, int R) {
   const long rows_per_block = (kThreads / 32) * 32L * R;
@@ -649,10 +767,73 @@ __global__ void k_block_normalize(long n, int s, int ld, double *X, const double
     }                                                                                            \
   } while (0)
 
-/* one CSR-stream launch with R rows per lane */
+/* Autotuner of the CSR-stream kernels: on a matrix's first use, time one
+ * Chebyshev degree with one and with two rows per lane (1 warm-up + 5 timed
+ * launches each, CUDA events, scratch vectors of the matrix's size) and keep
+ * the faster; two rows per lane must win by 3%.  Both give the same bits
+ * (the per-row summation order is the same), so the choice never changes a
+ * result.  PEVSL_B200_STREAM_R=1|2 fixes it; matrices under 4096 rows keep
+ * one.  Must not run while the stream is being captured. */
+int stream_tune(pevsl_devcsr *A) {
+  if (!A || A->stream_r) return 0;
+  const char *e = getenv("PEVSL_B200_STREAM_R");
+  if (e && (atoi(e) == 1 || atoi(e) == 2)) {
+    A->stream_r = atoi(e);
+    return 0;
+  }
+  A->stream_r = 1;
+  const long n = A->nrows;
+  if (n < 4096) return 0;
+  double *buf = nullptr;
+  if (cudaMalloc(&buf, sizeof(double) * 4 * (size_t)n) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaStream_t st = ctx().stream;
+  cudaMemsetAsync(buf, 0, sizeof(double) * 4 * (size_t)n, st);
+  double *x = buf, *xm1 = buf + n, *xp1 = buf + 2 * n, *y = buf + 3 * n;
+  const EpiCheb epi{x, xm1, xp1, y, 0.5, 0.5, 0.0, 0.5, 0};
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float ms[3] = {0.f, 0.f, 0.f};
+  for (int R = 1; R <= 2; R++) {
+    for (int it = 0; it < 6; it++) {
+      if (it == 1) cudaEventRecord(e0, st);
+      if (R == 2)
+        k_csr_stream<2><<<stream_grid(n, 2), kThreads, 0, st>>>(A->nrows, A->ia, A->ja,
+                                                                (const double *)A->a, x, epi);
+      else
+        k_csr_stream<1><<<stream_grid(n, 1), kThreads, 0, st>>>(A->nrows, A->ia, A->ja,
+                                                                (const double *)A->a, x, epi);
+    }
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(&ms[R], e0, e1);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (fail(cudaGetLastError(), "stream_tune")) return PEVSL_ERR_CUDA;
+  ctx().launches += 12;
+  if (ms[2] > 0.f && ms[2] < 0.97f * ms[1]) A->stream_r = 2;
+  if (getenv("PEVSL_B200_VERBOSE"))
+    fprintf(stderr, "stream_tune n=%ld: 1 row/lane %.2f us, 2 rows/lane %.2f us -> %d\n", n,
+            ms[1] * 200.f, ms[2] * 200.f, A->stream_r);
+  return 0;
+}
+
+/* one CSR-stream launch with the matrix's rows per lane (tuned on first use
+ * when the stream is not being captured) */
 template <class T, class Epi>
 static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const Epi &epi) {
-  if (stream_r() == 2)
+  if (!A->stream_r) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx().stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone)
+      stream_tune(const_cast<pevsl_devcsr *>(A));
+  }
+  if (stream_r(A) == 2)
     k_csr_stream<2><<<stream_grid(A->nrows, 2), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja,
                                                                              a, x, epi);
   else
@@ -664,7 +845,9 @@ static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const E
 template <class T, class Epi, int CAP, class Make>
 static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const char *what) {
   static StreamBatch<T, Epi, CAP> b; /* host staging: the launch copies it */
-  const int R = stream_r();
+  bool one = true;
+  for (int i = 1; i < nb && one; i++) one = en[i].A == en[0].A;
+  const int R = one ? stream_r(en[0].A) : 1;
   const long rows_per_block = (kThreads / 32) * 32L * R;
   b.nb = nb;
   b.shared = 1;
@@ -688,7 +871,9 @@ static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const cha
   const int *ia0 = b.ia[0], *ja0 = b.ja[0];
   const T *a0 = b.a[0];
   if (b.shared) {
-    if (R == 2)
+    if (batch_kernel() == 1 && nb > 1)
+      launch_group<T, Epi, CAP>(b, n0, ia0, ja0, a0);
+    else if (R == 2)
       k_csr_stream_batch<2, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
     else
       k_csr_stream_batch<1, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);

@@ -48,6 +48,7 @@ typedef struct pevsl_devcsr {
   int max_row_nnz;
   double avg_row_nnz;
   int lanes; /* threads per row in the row-group SpMV kernels */
+  int stream_r; /* rows per lane of the CSR-stream kernels, 0 until tuned */
   size_t bytes; /* size of the one device block holding a, ja, ia */
 } pevsl_devcsr;
 

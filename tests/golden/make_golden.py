@@ -158,5 +158,58 @@ def main():
                                      lam=fl(out["lam"]), res=fl(out["res"])))
 
 
+def mm_case(refdir="/root/reference"):
+    """The reference's Matrix Market driver (TESTS/MM/MMPLanN.c, built by
+    `make -C oracle drivers` against the reference build) on its own
+    MATRICES/A.mtx (stiff1) with the first two intervals of TESTS/MM/matfile.
+    Writes mm_stiff1.npz: the matrix's coordinate entries exactly as the
+    file lists them (one triangle, 1-based), and the driver's output."""
+    import subprocess
+    import tempfile
+    root = os.path.dirname(os.path.dirname(HERE))
+    exe = os.path.join(root, "oracle", "_ref", "MMPLanN")
+    src = os.path.join(refdir, "MATRICES", "A.mtx")
+    with open(src) as f:
+        lines = [ln for ln in f if not ln.startswith("%")]
+    nr, nc, nz = (int(x) for x in lines[0].split())
+    ent = np.array([ln.split() for ln in lines[1:1 + nz]])
+    I, J = ent[:, 0].astype(np.int32), ent[:, 1].astype(np.int32)
+    V = ent[:, 2].astype(np.float64)
+    intervals = [(0.10, 0.12, 3), (0.12, 0.14, 2)]
+    with tempfile.TemporaryDirectory() as d:
+        write_mm(os.path.join(d, "stiff1.mtx"), nr, I, J, V)
+        write_matfile(os.path.join(d, "matfile"), "stiff1.mtx", intervals)
+        os.makedirs(os.path.join(d, "OUT"))
+        subprocess.run([exe, "-matfile", "matfile", "-ngroups", "1"], cwd=d, check=True,
+                       capture_output=True, env=dict(os.environ, OPENBLAS_NUM_THREADS="1"))
+        with open(os.path.join(d, "OUT", "LapPLanN_G0.out")) as f:
+            out = f.read()
+    path = os.path.join(HERE, "mm_stiff1.npz")
+    np.savez_compressed(path, n=nr, i=I, j=J, v=V, intervals=np.array(intervals),
+                        output=np.array(out))
+    print("wrote", path, os.path.getsize(path), "bytes")
+
+
+def write_mm(path, n, I, J, V):
+    """A symmetric Matrix Market file with the given entries (repr floats:
+    they read back to the same doubles)."""
+    with open(path, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate real symmetric\n")
+        f.write(f"{n} {n} {len(V)}\n")
+        f.writelines(f"{i} {j} {v!r}\n" for i, j, v in zip(I.tolist(), J.tolist(), V.tolist()))
+
+
+def write_matfile(path, mtx, intervals):
+    """TESTS/MM/matfile's format: the count, then one line per problem."""
+    with open(path, "w") as f:
+        f.write(f"{len(intervals)}\n")
+        for a, b, ns in intervals:
+            f.write(f"{mtx} stiff1 MM1 {a} {b} {ns}\n")
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["mm"]:
+        mm_case()
+    else:
+        main()
+        mm_case()

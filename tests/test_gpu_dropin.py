@@ -63,3 +63,43 @@ def test_reference_matvec_driver(gpu):
     m = re.search(r"Matvec \|\|SEQ-PARA\|\| = ([-\d.e+]+)", r.stdout)
     assert m, r.stdout
     assert float(m.group(1)) == 0.0
+
+
+def _driver_report(out):
+    """Slices, filter degrees, per-slice counts and listed eigenvalues of an
+    OUT/LapPLanN_G0.out written by the reference's drivers."""
+    sl = [tuple(float(x) for x in m) for m in
+          re.findall(r"^\s*\d+: \[\s*([-\d.e+]+)\s*,\s*([-\d.e+]+)\]", out, re.M)]
+    degs = [int(x) for x in re.findall(r"polynomial \[type \d\] deg (\d+)", out)]
+    counts = [int(x) for x in re.findall(r"number of eigenvalues found: (\d+)", out)]
+    lams = [float(x) for x in re.findall(r"^\s*(-?\d\.\d{15}e[-+]\d+)\s+\d\.\de[-+]\d+\s*$", out, re.M)]
+    return sl, degs, counts, lams
+
+
+def test_reference_matrix_market_driver(gpu, tmp_path):
+    """TESTS/MM/MMPLanN.c with the reference's Matrix Market reader
+    (TESTS/COMMON/parmm.c, mmio.c), unchanged, on this library: the
+    reference's stiff1 matrix (MATRICES/A.mtx, n = 5795) and the first two
+    intervals of TESTS/MM/matfile give the reference driver's slices,
+    degrees and per-slice counts, and its listed eigenvalues to 1e-10
+    (fixture: tests/golden/mm_stiff1.npz, from the reference build)."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_golden import write_matfile, write_mm
+    exe = binary("MMPLanN")
+    g = np.load(os.path.join(HERE, "golden", "mm_stiff1.npz"))
+    write_mm(tmp_path / "stiff1.mtx", int(g["n"]), g["i"], g["j"], g["v"])
+    write_matfile(tmp_path / "matfile", "stiff1.mtx",
+                  [(float(a), float(b), int(c)) for a, b, c in g["intervals"]])
+    os.makedirs(tmp_path / "OUT")
+    r = subprocess.run([exe, "-matfile", "matfile", "-ngroups", "1"], cwd=tmp_path,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    got = _driver_report((tmp_path / "OUT" / "LapPLanN_G0.out").read_text())
+    ref = _driver_report(str(g["output"]))
+    assert got[2] == ref[2] == [45, 55, 61, 85, 66]
+    assert got[1] == ref[1]
+    assert len(got[0]) == len(ref[0]) == 5
+    assert np.max(np.abs(np.array(got[0]) - np.array(ref[0]))) <= 1e-12 * 0.14
+    assert len(got[3]) == len(ref[3]) > 0
+    assert np.max(np.abs(np.array(got[3]) - ref[3]) / np.abs(ref[3])) <= 1e-10

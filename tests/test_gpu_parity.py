@@ -451,14 +451,15 @@ def _lap_slices(grid, a, b, ns, seed=3):
 
 
 def test_filter_forms_bit_identical(gpu):
-    """One launch per degree and one persistent launch for all degrees give
-    the same bits (same per-row arithmetic, any schedule)."""
+    """One launch per degree, one persistent launch for all degrees, and the
+    launches replayed from a CUDA graph give the same bits (same per-row
+    arithmetic, any schedule)."""
     lib = pv.load()
     M, intvs, fl = _lap_slices((14, 13, 12), 0.5, 1.3, 4)
     v = np.cos(np.arange(M.n) * 0.37)
     outs = []
     try:
-        for form in (0, 1):
+        for form in (0, 1, 2):
             assert lib.pEVSL_B200_SetFilterForm(form) == 0
             with pv.Instance(M) as ev:
                 r, o = pv.cheblannr_batch(ev, intvs, [150] * 4, 1e-8, v, fl)
@@ -466,9 +467,10 @@ def test_filter_forms_bit_identical(gpu):
             outs.append(o)
     finally:
         lib.pEVSL_B200_SetFilterForm(-1)
-    for a, b in zip(*outs):
-        assert a["nev"] == b["nev"] and a["its"] == b["its"]
-        assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
+    for other in outs[1:]:
+        for a, b in zip(outs[0], other):
+            assert a["nev"] == b["nev"] and a["its"] == b["its"]
+            assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
 
 
 def test_multi_problem_equals_separate(gpu):

@@ -139,3 +139,20 @@ def test_findpol_too_narrow_is_an_error(lib):
     r, f = pv.findpol([0.4845065036442954, 0.4850594098995861, 0.4435124791600489,
                        8.445429558871442], max_deg=3000, deg_in=100)
     assert r == pv.ERR_ARG
+
+
+def test_copy_eigenvectors_rejects_bad_arguments(lib):
+    """pEVSL_B200_CopyEigenvectors checks its arguments before touching the
+    GPU: more vectors than the Parvecs holds, or a leading dimension below
+    the vector length, is PEVSL_ERR_ARG; zero vectors is a no-op."""
+    import ctypes as C
+    import pevsl_b200 as pv
+    W = pv.Parvecs()
+    W.n_vecs, W.n_local, W.ld = 2, 10, 16
+    out = np.zeros(64)
+    p = out.ctypes.data_as(C.POINTER(C.c_double))
+    f = pv.load().pEVSL_B200_CopyEigenvectors
+    assert f(C.byref(W), 3, p, 10) == pv.ERR_ARG
+    assert f(C.byref(W), 2, p, 9) == pv.ERR_ARG
+    assert f(C.byref(W), -1, p, 10) == pv.ERR_ARG
+    assert f(C.byref(W), 0, p, 10) == 0
