@@ -24,8 +24,12 @@
  *     being called through the pointer.
  *   - Nothing aborts the process: errors come back as return codes (the
  *     reference's codes where it has them, PEVSL_ERR_* below otherwise).
- *   - The generalized problem (SetGenEig with B-solves) is declared for
- *     source compatibility; solver calls on it return PEVSL_NOT_IMPLEMENT.
+ *   - The generalized problem (SetGenEig): B-solve and L^{-T}-solve
+ *     callbacks (SetBSol, SetLTSol) receive device (managed) pointers like
+ *     a user matvec.  The library's own solvers -- least-squares
+ *     polynomials (pEVSL_LSPolSol) and Chebyshev iterations
+ *     (pevsl_itsol.h) -- run on the device; direct solvers (MUMPS, PARDISO)
+ *     are not provided.
  */
 #ifndef PEVSL_H
 #define PEVSL_H
@@ -300,6 +304,20 @@ void pEVSL_SpslicerLan(double *xi, double *yi, int n_int, int npts, double *sli)
 /* Spectrum bounds — SRC/lantrbnd.c:31 (INC/pevsl.h:28-30). */
 int pEVSL_LanTrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pevsl_Parvec *vinit,
                       int bndtype, double *lammin, double *lammax, FILE *fstats);
+
+/* Least-squares polynomial approximation of B^{-1/2} (or B^{-1}) applied
+ * as a solve callback — SRC/lspolapprox.c (INC/pevsl.h:31-37).  B must be
+ * a parcsr set up by this library; *vdata is NULL on failure.
+ * pEVSL_SetupLSPol / pEVSL_SetupLSPolRec are exported by the reference's
+ * library (SRC/lspolapprox.c:171,207) without a declaration in its header. */
+void pEVSL_SetupLSPolSqrt(int max_deg, double tol, double lmin, double lmax, pevsl_Parcsr *B,
+                          void **vdata);                        /* lspolapprox.c:221 */
+void pEVSL_SetupLSPolRec(int max_deg, double tol, double lmin, double lmax, pevsl_Parcsr *B,
+                         void **vdata);                         /* lspolapprox.c:207 */
+void pEVSL_SetupLSPol(int max_deg, double tol, double lmin, double lmax, pevsl_Parcsr *B,
+                      double (*ffun)(double), void **vdata);    /* lspolapprox.c:171 */
+void pEVSL_LSPolSol(double *db, double *dx, void *data);        /* lspolapprox.c:296 */
+void pEVSL_LSPolFree(void *vdata);                              /* lspolapprox.c:314 */
 
 /* Instance — SRC/pevsl.c (INC/pevsl.h:41-52). */
 int pEVSL_Start(MPI_Comm comm, pevsl_Data **data);                 /* pevsl.c:13  */

@@ -107,6 +107,20 @@ int pEVSL_B200_LastError(void);
  * vectors of length pevsl->n. */
 int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y);
 
+/* The same for the generalized problem: y = p(A B^{-1}) v, each degree a
+ * solve with the instance's B-solve callback (SRC/chebpol.c:543-546). */
+int pEVSL_B200_ChebAvGen(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y);
+
+/* Host only (no device needed): the least-squares Chebyshev coefficients
+ * that pEVSL_SetupLSPolRec (kind 0, f = 1/x) or pEVSL_SetupLSPolSqrt
+ * (kind 1, f = 1/sqrt(x)) computes for [lmin, lmax]: mu[0..*deg] (mu holds
+ * max_deg entries), centre *cc and half-width *dd. */
+int pEVSL_B200_LSPolCoefs(int kind, int max_deg, double tol, double lmin, double lmax, double *mu,
+                          int *deg, double *cc, double *dd);
+/* degree of a set-up least-squares solver; its coefficients into
+ * mu_out[0..min(deg, cap-1)] when mu_out is not NULL */
+int pEVSL_B200_LSPolDegree(const void *vdata, double *mu_out, int cap);
+
 /* pEVSL_ChebLanNr for nslices slices at once.  The slices advance in
  * lockstep (up to 256 per group): one fused filter launch per polynomial
  * degree serves every slice still filtering (the matrix is read once per

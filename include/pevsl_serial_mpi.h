@@ -20,6 +20,7 @@
 #include <time.h>
 
 typedef int MPI_Comm;
+typedef int MPI_Fint; /* Fortran handle: the same int as the C handle here */
 typedef int MPI_Datatype; /* element size in bytes */
 typedef int MPI_Op;
 typedef int MPI_Request;
@@ -43,6 +44,8 @@ static inline int pevsl_serial_mpi_copy(const void *s, void *r, int n, MPI_Datat
   if (n > 0 && s != r) memmove(r, s, (size_t)n * (size_t)t);
   return MPI_SUCCESS;
 }
+static inline MPI_Comm MPI_Comm_f2c(MPI_Fint c) { return (MPI_Comm)c; }
+static inline MPI_Fint MPI_Comm_c2f(MPI_Comm c) { return (MPI_Fint)c; }
 static inline int MPI_Init(int *argc, char ***argv) { (void)argc; (void)argv; return 0; }
 static inline int MPI_Finalize(void) { return 0; }
 static inline int MPI_Comm_rank(MPI_Comm c, int *r) { (void)c; *r = 0; return 0; }

@@ -404,3 +404,68 @@ int oref_pipeline(const orc_spec *s, orc_out *o) {
   o->t_total = pEVSL_Wtime() - t0;
   return o->status;
 }
+
+/* ------------------------------------------------------------ B-solvers */
+
+/* exported by SRC/lspolapprox.c:207 without a declaration in INC/ */
+void pEVSL_SetupLSPolRec(int max_deg, double tol, double lmin, double lmax, pevsl_Parcsr *B,
+                         void **vdata);
+int pEVSL_ChebIterSetup(double lmin, double lmax, int deg, pevsl_Parcsr *A, void **data);
+void pEVSL_ChebIterSolv1(double *db, double *dx, void *data);
+void pEVSL_ChebIterSolv2(double *db, double *dx, void *data);
+void pEVSL_ChebIterFree(void *vdata);
+
+/* The leading members of the private LSPol_Data of SRC/lspolapprox.c:10-22,
+ * in their order, to read the degree and coefficients it computed. */
+typedef struct {
+  int N, n, nfirst, max_deg, deg;
+  double intv[2];
+  double cc, dd, tol;
+  double *mu;
+} oref_lspol_view;
+
+/* pEVSL_SetupLSPolRec (kind 0) / pEVSL_SetupLSPolSqrt (kind 1) on B, then
+ * x = pEVSL_LSPolSol(b); mu receives the max_deg coefficients. */
+int oref_lspol(int kind, int max_deg, double tol, double lmin, double lmax, int n, const int *ia,
+               const int *ja, const double *a, double *mu, int *deg, double *cc, double *dd,
+               const double *b, double *x) {
+  pevsl_Parcsr B;
+  void *data = NULL;
+  build_parcsr(n, ia, ja, a, &B);
+  if (kind == 0)
+    pEVSL_SetupLSPolRec(max_deg, tol, lmin, lmax, &B, &data);
+  else
+    pEVSL_SetupLSPolSqrt(max_deg, tol, lmin, lmax, &B, &data);
+  const oref_lspol_view *L = (const oref_lspol_view *)data;
+  *deg = L->deg;
+  *cc = L->cc;
+  *dd = L->dd;
+  memcpy(mu, L->mu, (size_t)max_deg * sizeof(double));
+  double *bb = (double *)malloc((size_t)n * sizeof(double));
+  memcpy(bb, b, (size_t)n * sizeof(double));
+  pEVSL_LSPolSol(bb, x, data);
+  free(bb);
+  pEVSL_LSPolFree(data);
+  pEVSL_ParcsrFree(&B);
+  return 0;
+}
+
+/* x = pEVSL_ChebIterSolv1 (kind 1) or Solv2 (kind 2) of b on A */
+int oref_chebiter(int kind, double lmin, double lmax, int deg, int n, const int *ia, const int *ja,
+                  const double *a, const double *b, double *x) {
+  pevsl_Parcsr A;
+  void *data = NULL;
+  build_parcsr(n, ia, ja, a, &A);
+  pEVSL_ChebIterSetup(lmin, lmax, deg, &A, &data);
+  double *bb = (double *)malloc((size_t)n * sizeof(double));
+  memcpy(bb, b, (size_t)n * sizeof(double));
+  memset(x, 0, (size_t)n * sizeof(double));
+  if (kind == 1)
+    pEVSL_ChebIterSolv1(bb, x, data);
+  else
+    pEVSL_ChebIterSolv2(bb, x, data);
+  free(bb);
+  pEVSL_ChebIterFree(data);
+  pEVSL_ParcsrFree(&A);
+  return 0;
+}

@@ -155,6 +155,22 @@ SIGNATURES = [
     ("pEVSL_B200_Sync", _I, []),
     ("pEVSL_B200_LastError", _I, []),
     ("pEVSL_B200_ChebAv", _I, [C.POINTER(PevslData), C.POINTER(Polparams), _vp, _vp]),
+    ("pEVSL_B200_ChebAvGen", _I, [C.POINTER(PevslData), C.POINTER(Polparams), _vp, _vp]),
+    ("pEVSL_SetBParcsr", _I, [C.POINTER(PevslData), C.POINTER(Parcsr)]),
+    ("pEVSL_SetBSol", _I, [C.POINTER(PevslData), _vp, _vp]),
+    ("pEVSL_SetLTSol", _I, [C.POINTER(PevslData), _vp, _vp]),
+    ("pEVSL_SetupLSPolRec", None, [_I, _D, _D, _D, C.POINTER(Parcsr), C.POINTER(_vp)]),
+    ("pEVSL_SetupLSPolSqrt", None, [_I, _D, _D, _D, C.POINTER(Parcsr), C.POINTER(_vp)]),
+    ("pEVSL_LSPolSol", None, [_vp, _vp, _vp]),
+    ("pEVSL_LSPolFree", None, [_vp]),
+    ("pEVSL_B200_LSPolCoefs", _I, [_I, _I, _D, _D, _D, _dp, _ip, _dp, _dp]),
+    ("pEVSL_B200_LSPolDegree", _I, [_vp, _dp, _I]),
+    ("pEVSL_ChebIterSetup", _I, [_D, _D, _I, C.POINTER(Parcsr), C.POINTER(_vp)]),
+    ("pEVSL_ChebIterSolv1", None, [_vp, _vp, _vp]),
+    ("pEVSL_ChebIterSolv2", None, [_vp, _vp, _vp]),
+    ("pEVSL_ChebIterFree", None, [_vp]),
+    ("pEVSL_ChebIterGetRes", _dp, [_vp]),
+    ("pEVSL_ChebIterStatsPrint", None, [_vp, _vp]),
     ("pEVSL_B200_ReleaseWorkspace", None, []),
     ("pEVSL_B200_Info", _I, [C.c_char_p, _I]),
     ("pEVSL_B200_SetDevice", _I, [_I]),
@@ -387,6 +403,79 @@ def spslicer_lan(xi, yi, n_int):
 
 
 # ---------------------------------------------------------------- instance
+class BSolver:
+    """A B-solver of the library on a parcsr B, usable as the B-solve or
+    L^{-T}-solve of a generalized instance: kind "lsrec" (least-squares
+    polynomial for 1/x, pEVSL_SetupLSPolRec), "lssqrt" (1/sqrt(x),
+    pEVSL_SetupLSPolSqrt), "cheb1" / "cheb2" (Chebyshev iteration of the
+    first / second kind, pEVSL_ChebIterSetup) on the spectrum enclosure
+    [lmin, lmax] of B; `deg` is max_deg for the polynomials, the number of
+    iterations for the Chebyshev iterations."""
+
+    def __init__(self, B: Matrix, kind: str, lmin: float, lmax: float, deg: int, tol: float = 1e-6):
+        self.lib, self.B, self.kind = load(), B, kind
+        self.h = C.c_void_p()
+        if kind in ("lsrec", "lssqrt"):
+            f = self.lib.pEVSL_SetupLSPolRec if kind == "lsrec" else self.lib.pEVSL_SetupLSPolSqrt
+            f(deg, tol, lmin, lmax, C.byref(B.A), C.byref(self.h))
+            if not self.h.value:
+                raise PevslError(f"pEVSL_SetupLSPol ({kind}) failed")
+            self.func = C.cast(self.lib.pEVSL_LSPolSol, C.c_void_p)
+        elif kind in ("cheb1", "cheb2"):
+            _check(self.lib.pEVSL_ChebIterSetup(lmin, lmax, deg, C.byref(B.A), C.byref(self.h)),
+                   "ChebIterSetup")
+            self.func = C.cast(self.lib.pEVSL_ChebIterSolv1 if kind == "cheb1"
+                               else self.lib.pEVSL_ChebIterSolv2, C.c_void_p)
+        else:
+            raise ValueError(kind)
+
+    @property
+    def degree(self) -> int:
+        """degree of a least-squares polynomial"""
+        return self.lib.pEVSL_B200_LSPolDegree(self.h, None, 0)
+
+    def coefficients(self) -> np.ndarray:
+        d = self.degree
+        mu = np.zeros(d + 1)
+        self.lib.pEVSL_B200_LSPolDegree(self.h, _ptr(mu), d + 1)
+        return mu
+
+    def solve(self, b: np.ndarray) -> np.ndarray:
+        """x = the solver applied to b (called as a user would call it)"""
+        bv, xv = Vector(self.B.n, b), Vector(self.B.n)
+        fn = C.CFUNCTYPE(None, _vp, _vp, _vp)(self.func.value)
+        fn(bv.pv.data, xv.pv.data, self.h)
+        _check(self.lib.pEVSL_B200_LastError(), "B-solve")
+        x = xv.get()
+        bv.free()
+        xv.free()
+        return x
+
+    def free(self):
+        if self.h.value:
+            if self.kind.startswith("ls"):
+                self.lib.pEVSL_LSPolFree(self.h)
+            else:
+                self.lib.pEVSL_ChebIterFree(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def lspol_coefs(kind: int, max_deg: int, tol: float, lmin: float, lmax: float):
+    """Host-only least-squares coefficients of 1/x (kind 0) or 1/sqrt(x)
+    (kind 1) on [lmin, lmax]: (deg, mu[0..deg], cc, dd)."""
+    mu = np.zeros(max_deg)
+    deg, cc, dd = C.c_int(), C.c_double(), C.c_double()
+    _check(load().pEVSL_B200_LSPolCoefs(kind, max_deg, tol, lmin, lmax, _ptr(mu), C.byref(deg),
+                                        C.byref(cc), C.byref(dd)), "LSPolCoefs")
+    return deg.value, mu[:deg.value + 1].copy(), cc.value, dd.value
+
+
 class Instance:
     """One pEVSL instance (pEVSL_Start ... pEVSL_Finish) bound to a matrix."""
 
@@ -401,6 +490,16 @@ class Instance:
     @property
     def n(self) -> int:
         return self.p.contents.n
+
+    def set_generalized(self, B: Matrix, bsol: BSolver, ltsol: BSolver | None = None) -> None:
+        """A x = lambda B x: B as the parcsr B matvec, bsol as the B-solve,
+        ltsol (B^{-1/2} or another L^{-T}) for the DOS start vectors."""
+        _check(self.lib.pEVSL_SetBParcsr(self.p, C.byref(B.A)), "SetBParcsr")
+        _check(self.lib.pEVSL_SetBSol(self.p, bsol.func, bsol.h), "SetBSol")
+        if ltsol is not None:
+            _check(self.lib.pEVSL_SetLTSol(self.p, ltsol.func, ltsol.h), "SetLTSol")
+        _check(self.lib.pEVSL_SetGenEig(self.p), "SetGenEig")
+        self._gen = (B, bsol, ltsol)
 
     def set_precision(self, precision: int) -> None:
         """PREC_FP64 (default) or PREC_MIXED (FP32 filter and KPM moments,

@@ -71,6 +71,8 @@ enum Ws {
   WS_FILT,      /* batched filter work vectors                */
   WS_MU,        /* filter coefficients on the device          */
   WS_GROUP,     /* per-entry coefficient vectors of a group   */
+  WS_ZBASIS,    /* generalized problem: Z = B V               */
+  WS_GEN,       /* generalized problem: filter / KPM vectors  */
   WS_COUNT
 };
 
@@ -153,6 +155,19 @@ int spmv(const pevsl_devcsr *A, const double *x, double *y);
  *   vkp1 = w;  y = first ? mu0 * vk + muk * w : y + muk * w            */
 int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1,
               double *y, double cc, double t, double mu0, double muk, int first);
+/* The degree of the generalized filter (SRC/chebpol.c:543-546): the SpMV
+ * reads x = B^{-1} vk, the recurrence uses vk; tmp (n doubles) is used
+ * only by the row-group kernels. */
+int cheb_step_x(const pevsl_devcsr *A, const double *x, const double *vk, const double *vkm1,
+                double *vkp1, double *y, double cc, double t, double mu0, double muk, int first,
+                double *tmp);
+/* Fused steps of the Chebyshev iterations for B x = b
+ * (EXTERNAL/ITERSOL/chebiter.c): first kind r = b - B x; p = bet p + r;
+ * xnew = x + alp p.  Second kind x += d; r -= B d; dnew = c1 d + c2 r. */
+int chebiter1_step(const pevsl_devcsr *B, const double *b, const double *x, double *p, double *xnew,
+                   double bet, double alp, double *tmp);
+int chebiter2_step(const pevsl_devcsr *B, const double *d, double *x, double *r, double *dnew,
+                   double c1, double c2, double *tmp);
 /* Same recurrence when A x is computed by a user callback: ax = A vk. */
 int cheb_combine(long n, const double *ax, const double *vk, const double *vkm1, double *vkp1,
                  double *y, double cc, double t, double mu0, double muk, int first);

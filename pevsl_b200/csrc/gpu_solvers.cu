@@ -449,7 +449,6 @@ int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, 
 int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *intv, int ngroups,
                  int groupid, MPI_Comm gl_comm, double *mu, double *ecnt) {
   const double t0 = pevsl_now();
-  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   if (ensure()) return PEVSL_ERR_CUDA;
   if (pevsl_check_intv(intv, stdout) < 0) return -1;
   const long n = pevsl->n;
@@ -481,9 +480,15 @@ int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *int
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   cudaEventRecord(e0, ctx().stream);
-  const bool mixed = A && pevsl_inst_of(pevsl)->precision == PEVSL_PREC_MIXED;
+  const bool gen = pevsl->ifGenEv != 0;
+  const bool mixed = !gen && A && pevsl_inst_of(pevsl)->precision == PEVSL_PREC_MIXED;
   if (mixed) st = csr_make_fp32(A);
-  if (A && mixed && !st) {
+  if (gen) {
+    /* generalized problem: one vector at a time with B-solves */
+    if (!st)
+      st = pevsl_gen_kpm_moments(pevsl, Mdeg, jac, ctr, wid, beta1, beta2, vec_start, vec_end, mu,
+                                 &tcnt);
+  } else if (A && mixed && !st) {
     /* FP32 moments: blocks of up to 64 vectors drawn and normalised in FP64,
      * then rounded to FP32; FP32 recurrence and dots, one launch per degree */
     const int smax = 64;
@@ -655,10 +660,54 @@ int pEVSL_Kpmdos(pevsl_Data *pevsl, int Mdeg, int damping, int nvec, double *int
 
 /* ================================================================ Lanczos DOS */
 
+/* one Lanczos run of pEVSL_LanDosG (SRC/landos.c:134-262): v_0 = vinit
+ * normalised, maxit steps with full reorthogonalisation; the tridiagonal
+ * matrix into dT, eT */
+static int landos_lanczos(pevsl_Data *pevsl, int maxit, double *V, long ld, const double *vinit,
+                          long n, double *dT, double *eT) {
+  Ctx &c = ctx();
+  int st = vnrm2(n, vinit, c.dscal + S_TMP0);
+  const double *h = st ? nullptr : fetch_scalars(S_TMP0, 1);
+  if (!h) return st ? st : PEVSL_ERR_CUDA;
+  const double tinv = 1.0 / h[0];
+  if (!st) st = vcopy(vinit, V, n);
+  if (!st) st = vscal(V, n, tinv);
+  double wn = 0.0, beta = 0.0;
+  int nwn = 0;
+  for (int k = 0; k < maxit && !st; k++) {
+    double *v = V + (size_t)k * ld, *vnew = V + (size_t)(k + 1) * ld;
+    st = apply_A(pevsl, v, vnew);
+    if (!st && k > 0) st = vaxpy(n, -beta, V + (size_t)(k - 1) * ld, vnew);
+    if (!st) st = vdot(n, v, vnew, c.dscal + S_ALPHA);
+    if (!st) st = vaxpy_dev_nrm2(n, c.dscal + S_ALPHA, v, vnew, c.dscal + S_NRM0);
+    if (!st) st = cgs_dgks(V, ld, k + 1, vnew, n);
+    if (!st) st = memcpy_async(c.hscal + S_ALPHA, c.dscal + S_ALPHA, sizeof(double) * 4);
+    if (!st) st = sync();
+    if (st) break;
+    const double alpha = c.hscal[S_ALPHA];
+    beta = c.hscal[S_NRM];
+    dT[k] = alpha;
+    wn += fabs(alpha) + 2.0 * beta;
+    nwn += 3;
+    if (beta * nwn < orthTol * wn) {
+      st = pevsl_rand_vector_dev(vnew, (int)n);
+      if (!st) st = vnrm2(n, vnew, c.dscal + S_NRM0);
+      if (!st) st = cgs_dgks(V, ld, k + 1, vnew, n);
+      const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
+      if (!hb) return st ? st : PEVSL_ERR_CUDA;
+      st = vscal(vnew, n, 1.0 / hb[0]);
+      beta = 0.0;
+    } else {
+      st = vscal(vnew, n, 1.0 / beta);
+    }
+    eT[k] = beta;
+  }
+  return st;
+}
+
 int pEVSL_LanDosG(pevsl_Data *pevsl, const int nvec, int msteps, int npts, double *xdos,
                   double *ydos, double *neig, double *intv, int ngroups, int groupid,
                   MPI_Comm gl_comm) {
-  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   if (ensure()) return PEVSL_ERR_CUDA;
   const double t0 = pevsl_now();
   const long n = pevsl->n, ld = round_ld(n);
@@ -682,51 +731,10 @@ int pEVSL_LanDosG(pevsl_Data *pevsl, const int nvec, int msteps, int npts, doubl
   if (!st) linspace(aa, bb, npts, xdos);
   int vec_start = 0, vec_end = nvec;
   if (ngroups > 1) pEVSL_Part1d(nvec, ngroups, &groupid, &vec_start, &vec_end, 1);
-  Ctx &c = ctx();
   for (int m = vec_start; m < vec_end && !st; m++) {
     st = pevsl_rand_vector_dev(vinit, (int)n);
-    if (!st) st = vnrm2(n, vinit, c.dscal + S_TMP0);
-    const double *h = st ? nullptr : fetch_scalars(S_TMP0, 1);
-    if (!h) {
-      st = st ? st : PEVSL_ERR_CUDA;
-      break;
-    }
-    const double tinv = 1.0 / h[0];
-    if (!st) st = vcopy(vinit, V, n);
-    if (!st) st = vscal(V, n, tinv);
-    double wn = 0.0, beta = 0.0;
-    int nwn = 0;
-    for (int k = 0; k < maxit && !st; k++) {
-      double *v = V + (size_t)k * ld, *vnew = V + (size_t)(k + 1) * ld;
-      st = apply_A(pevsl, v, vnew);
-      if (!st && k > 0) st = vaxpy(n, -beta, V + (size_t)(k - 1) * ld, vnew);
-      if (!st) st = vdot(n, v, vnew, c.dscal + S_ALPHA);
-      if (!st) st = vaxpy_dev_nrm2(n, c.dscal + S_ALPHA, v, vnew, c.dscal + S_NRM0);
-      if (!st) st = cgs_dgks(V, ld, k + 1, vnew, n);
-      if (!st) st = memcpy_async(c.hscal + S_ALPHA, c.dscal + S_ALPHA, sizeof(double) * 4);
-      if (!st) st = sync();
-      if (st) break;
-      const double alpha = c.hscal[S_ALPHA];
-      beta = c.hscal[S_NRM];
-      dT[k] = alpha;
-      wn += fabs(alpha) + 2.0 * beta;
-      nwn += 3;
-      if (beta * nwn < orthTol * wn) {
-        st = pevsl_rand_vector_dev(vnew, (int)n);
-        if (!st) st = vnrm2(n, vnew, c.dscal + S_NRM0);
-        if (!st) st = cgs_dgks(V, ld, k + 1, vnew, n);
-        const double *hb = st ? nullptr : fetch_scalars(S_NRM, 1);
-        if (!hb) {
-          st = st ? st : PEVSL_ERR_CUDA;
-          break;
-        }
-        st = vscal(vnew, n, 1.0 / hb[0]);
-        beta = 0.0;
-      } else {
-        st = vscal(vnew, n, 1.0 / beta);
-      }
-      eT[k] = beta;
-    }
+    if (!st) st = pevsl->ifGenEv ? pevsl_gen_landos_lanczos(pevsl, maxit, vinit, dT, eT)
+                                 : landos_lanczos(pevsl, maxit, V, ld, vinit, n, dT, eT);
     if (st) break;
     if (pevsl_tridiag_eig(maxit, dT, eT, EvalT, EvecT)) {
       st = PEVSL_ERR_EIG;
@@ -769,9 +777,15 @@ int pEVSL_LanDosG(pevsl_Data *pevsl, const int nvec, int msteps, int npts, doubl
 
 int pEVSL_LanTrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pevsl_Parvec *vinit,
                       int bndtype, double *lammin, double *lammax, FILE *fstats) {
-  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   if (ensure()) return PEVSL_ERR_CUDA;
   const double t0 = pevsl_now();
+  if (pevsl->ifGenEv) {
+    const int st = pevsl_gen_lantrbounds(pevsl, lanm, maxit, tol, vinit, bndtype, lammin, lammax,
+                                         fstats);
+    pevsl->stats->t_eigbounds += pevsl_now() - t0;
+    pevsl_inst_of(pevsl)->phase_ms[0] = 1e3 * (pevsl_now() - t0);
+    return st;
+  }
   const int N = pevsl->N;
   const long n = pevsl->n, ld = round_ld(n);
   lanm = PEVSL_MIN(lanm, N);
@@ -1699,8 +1713,15 @@ int pEVSL_ChebLanNr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevs
   *lamo = nullptr;
   *Wo = nullptr;
   *reso = nullptr;
-  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   if (ensure()) return PEVSL_ERR_CUDA;
+  if (pevsl->ifGenEv) {
+    int its = 0;
+    const int st = pevsl_gen_cheblannr(pevsl, intv, maxit, tol, vinit, pol, nevOut, lamo, Wo, reso,
+                                       &its, fstats);
+    pevsl_inst_of(pevsl)->last_its = its;
+    pevsl->stats->t_iter = pevsl_now() - tall;
+    return st;
+  }
   SliceState S;
   memset(&S, 0, sizeof S);
   memcpy(S.intv, intv, sizeof S.intv);
@@ -1759,10 +1780,21 @@ int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intv
                               pevsl_Parvecs **Wo, double **reso, int *its, int *status,
                               FILE *fstats) {
   const double tall = pevsl_now();
-  if (pevsl->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   if (ensure()) return PEVSL_ERR_CUDA;
   if (nslices < 0) return PEVSL_ERR_ARG;
   int first_err = 0;
+  if (pevsl->ifGenEv) {
+    /* generalized problem: the slices one after the other */
+    for (int s = 0; s < nslices; s++) {
+      double iv[4];
+      memcpy(iv, intvs + 4 * (size_t)s, sizeof iv);
+      status[s] = pevsl_gen_cheblannr(pevsl, iv, maxits[s], tol, vinit, &pols[s], &nevOut[s],
+                                      &lamo[s], &Wo[s], &reso[s], &its[s], fstats);
+      if (status[s] && !first_err) first_err = status[s];
+    }
+    pevsl->stats->t_iter = pevsl_now() - tall;
+    return first_err;
+  }
   g_t_pol.init();
   g_t_orth.init();
   g_fallbacks = 0;
@@ -1802,7 +1834,6 @@ int pEVSL_B200_ChebLanNrMulti(int nprob, pevsl_Data **pevsls, const int *nslices
   if (nprob < 0 || (nprob > 0 && (!pevsls || !nslices || !vinits))) return PEVSL_ERR_ARG;
   for (int p = 0; p < nprob; p++) {
     if (!pevsls[p] || nslices[p] < 0) return PEVSL_ERR_ARG;
-    if (pevsls[p]->ifGenEv) return PEVSL_NOT_IMPLEMENT;
   }
   g_t_pol.init();
   g_t_orth.init();
@@ -1822,6 +1853,19 @@ int pEVSL_B200_ChebLanNrMulti(int nprob, pevsl_Data **pevsls, const int *nslices
     SL.clear();
   };
   for (int p = 0; p < nprob; p++) {
+    if (pevsls[p]->ifGenEv) {
+      /* a generalized problem: its slices one after the other */
+      flush();
+      for (int s = 0; s < nslices[p]; s++, o++) {
+        double iv[4];
+        memcpy(iv, intvs + 4 * (size_t)o, sizeof iv);
+        status[o] = pevsl_gen_cheblannr(pevsls[p], iv, maxits[o], tol, vinits[p], &pols[o],
+                                        &nevOut[o], &lamo[o], &Wo[o], &reso[o], &its[o], fstats);
+        if (status[o] && !first_err) first_err = status[o];
+      }
+      o0 = o;
+      continue;
+    }
     if (!SL.empty() && (int)SL.size() + nslices[p] > kMaxEntries) flush();
     for (int s = 0; s < nslices[p]; s++, o++) {
       if ((int)SL.size() == kMaxEntries) flush();

@@ -101,6 +101,27 @@ __global__ void k_cheb_combine(long n, const double *__restrict__ ax, const doub
   }
 }
 
+__global__ void k_chebiter1_combine(long n, const double *__restrict__ w, const double *__restrict__ b,
+                                    const double *__restrict__ x, double *__restrict__ p,
+                                    double *__restrict__ xnew, double bet, double alp) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    const double pn = __dadd_rn(__dmul_rn(p[i], bet), __dsub_rn(b[i], w[i]));
+    p[i] = pn;
+    xnew[i] = __fma_rn(alp, pn, x[i]);
+  }
+}
+
+__global__ void k_chebiter2_combine(long n, const double *__restrict__ w, const double *__restrict__ d,
+                                    double *__restrict__ x, double *__restrict__ r,
+                                    double *__restrict__ dnew, double c1, double c2) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+    x[i] = __dadd_rn(x[i], d[i]);
+    const double rn = __dsub_rn(r[i], w[i]);
+    r[i] = rn;
+    dnew[i] = __fma_rn(c2, rn, __dmul_rn(d[i], c1));
+  }
+}
+
 /* ---------------------------------------------------------------- CSR-stream
  * Short rows (the stencil matrices of this path have 5-16 entries): a warp
  * owns 32 consecutive rows.  Its lanes stream the rows' entries in
@@ -170,6 +191,45 @@ struct EpiCheb32 {
       yout[row] = (double)yv;
     else
       y[row] = yv;
+  }
+};
+
+/* One step of the Chebyshev iteration for B x = b of
+ * EXTERNAL/ITERSOL/chebiter.c:121-197 (first kind): with w = B x_i,
+ *   r = b - w;  p = bet p + r;  x_{i+1} = x_i + alp p.
+ * x_i is the gathered vector, so x_{i+1} goes to another buffer. */
+struct EpiChebIter1 {
+  const double *b, *x;
+  double *p, *xnew;
+  double bet, alp;
+  struct Pre {
+    double b, p, x;
+  };
+  __device__ __forceinline__ Pre pre(int row) const { return Pre{b[row], p[row], x[row]}; }
+  __device__ __forceinline__ void operator()(int row, double w, const Pre &q) const {
+    const double r = __dsub_rn(q.b, w);
+    const double pn = __dadd_rn(__dmul_rn(q.p, bet), r);
+    p[row] = pn;
+    xnew[row] = __fma_rn(alp, pn, q.x);
+  }
+};
+
+/* One step of EXTERNAL/ITERSOL/chebiter.c:204-262 (second kind): with
+ * w = B d, x += d;  r -= w;  d_new = c1 d + c2 r  (c1 = rho1 rho,
+ * c2 = 2 rho1 / delta).  d is the gathered vector: d_new goes to dnew. */
+struct EpiChebIter2 {
+  const double *d;
+  double *x, *r, *dnew;
+  double c1, c2;
+  struct Pre {
+    double d, x, r;
+  };
+  __device__ __forceinline__ Pre pre(int row) const { return Pre{d[row], x[row], r[row]}; }
+  __device__ __forceinline__ void operator()(int row, double w, const Pre &q) const {
+    x[row] = __dadd_rn(q.x, q.d);
+    const double rn = __dsub_rn(q.r, w);
+    r[row] = rn;
+    dnew[row] = __fma_rn(c2, rn, __dmul_rn(q.d, c1));
   }
 };
 
@@ -293,131 +353,6 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
     stream_rows<R>(b.n[lo], b.ia[lo], b.ja[lo], b.a[lo], (const T *)b.epi[lo].vk, b.epi[lo],
                    (long)blockIdx.x - b.off[lo], prod);
   }
-}
-
-/* Grouped form of the shared-matrix batch: block b serves row block
- * b / ngroups for the G slices of group b % ngroups.  A warp loads its rows'
- * column indices and values once, prefetches every slice's epilogue
- * operands, issues every slice's gathers x_s[col] together as asynchronous
- * copies into shared memory (cp.async: no registers held while they fly),
- * then forms the products and sums each slice's rows in index order -- the
- * arithmetic of stream_rows, bit for bit.  The matrix stretch is read once
- * per group instead of once per slice. */
-template <class T>
-__device__ __forceinline__ void gather_async(T *dst, const T *src) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(sizeof(T))
-               : "memory");
-}
-
-template <class T, class Epi, int CAP, int G>
-__global__ void __launch_bounds__(kThreads, 3)
-    k_csr_stream_group(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-                       const T *__restrict__ a, const __grid_constant__ StreamBatch<T, Epi, CAP> b,
-                       int ngroups) {
-  extern __shared__ __align__(16) unsigned char dyn_raw[];
-  T(*xs)[G][kStreamChunk] = reinterpret_cast<T(*)[G][kStreamChunk]>(dyn_raw);
-  constexpr int PL = kStreamChunk / 32;
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const long rblk = blockIdx.x / (unsigned)ngroups;
-  const int g0 = (int)(blockIdx.x % (unsigned)ngroups) * G;
-  const int ng = b.nb - g0 < G ? b.nb - g0 : G;
-  const long r0l = (rblk * (kThreads / 32) + w) * 32;
-  if (r0l >= n) return;
-  const int r0 = (int)r0l;
-  const int nr = n - r0 < 32 ? n - r0 : 32;
-  const int row = r0 + lane;
-  typename Epi::Pre pre[G];
-  int rs = 0, re = 0;
-  if (lane < nr) {
-#pragma unroll
-    for (int j = 0; j < G; j++)
-      if (j < ng) pre[j] = b.epi[g0 + j].pre(row);
-    rs = __ldg(ia + row);
-    re = __ldg(ia + row + 1);
-  }
-  const int base = __ldg(ia + r0), len = __ldg(ia + r0 + nr) - base;
-  rs -= base;
-  re -= base;
-  T acc[G];
-#pragma unroll
-  for (int j = 0; j < G; j++) acc[j] = T(0);
-  for (int c0 = 0; c0 < len; c0 += kStreamChunk) {
-    int col[PL];
-    T val[PL];
-#pragma unroll
-    for (int q = 0; q < PL; q++) {
-      const int t = c0 + q * 32 + lane;
-      col[q] = t < len ? __ldg(ja + base + t) : -1;
-      val[q] = t < len ? __ldg(a + base + t) : T(0);
-    }
-#pragma unroll
-    for (int j = 0; j < G; j++) {
-      if (j >= ng) break;
-      const T *x = (const T *)b.epi[g0 + j].vk;
-#pragma unroll
-      for (int q = 0; q < PL; q++) {
-        T *d = &xs[w][j][q * 32 + lane];
-        if (col[q] >= 0)
-          gather_async(d, x + col[q]);
-        else
-          *d = T(0);
-      }
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < G; j++) {
-      if (j >= ng) break;
-#pragma unroll
-      for (int q = 0; q < PL; q++) {
-        T *d = &xs[w][j][q * 32 + lane];
-        *d = mul_rn(val[q], *d);
-      }
-    }
-    __syncwarp();
-    const int lo = rs > c0 ? rs : c0;
-    const int hi = re < c0 + kStreamChunk ? re : c0 + kStreamChunk;
-#pragma unroll
-    for (int j = 0; j < G; j++) {
-      if (j >= ng) break;
-      for (int t = lo; t < hi; t++) acc[j] = add_rn(acc[j], xs[w][j][t - c0]);
-    }
-    __syncwarp();
-  }
-  if (lane < nr) {
-#pragma unroll
-    for (int j = 0; j < G; j++)
-      if (j < ng) b.epi[g0 + j](row, acc[j], pre[j]);
-  }
-}
-
-/* 0: grid-interleaved blocks (k_csr_stream_batch), 1: grouped blocks
- * (k_csr_stream_group); PEVSL_B200_BATCH_KERNEL */
-static int batch_kernel() {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("PEVSL_B200_BATCH_KERNEL");
-    v = e ? (atoi(e) == 1) : 0;
-  }
-  return v;
-}
-
-template <class T, class Epi, int CAP>
-static void launch_group(const StreamBatch<T, Epi, CAP> &b, int n0, const int *ia0, const int *ja0,
-                         const T *a0) {
-  constexpr int G = 4;
-  const size_t smem = sizeof(T) * (kThreads / 32) * G * kStreamChunk;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_csr_stream_group<T, Epi, CAP, G>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
-  const int ngroups = (b.nb + G - 1) / G;
-  const unsigned g = (unsigned)(((n0 + kThreads - 1) / kThreads) * (long)ngroups);
-  k_csr_stream_group<T, Epi, CAP, G><<<g, kThreads, smem, ctx().stream>>>(n0, ia0, ja0, a0, b,
-                                                                          ngroups);
 }
 
 /* ---------------------------------------------------------------- persistent filter */
@@ -871,9 +806,7 @@ static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const cha
   const int *ia0 = b.ia[0], *ja0 = b.ja[0];
   const T *a0 = b.a[0];
   if (b.shared) {
-    if (batch_kernel() == 1 && nb > 1)
-      launch_group<T, Epi, CAP>(b, n0, ia0, ja0, a0);
-    else if (R == 2)
+    if (R == 2)
       k_csr_stream_batch<2, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
     else
       k_csr_stream_batch<1, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
@@ -906,6 +839,44 @@ int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, doubl
   PV_LANE_SWITCH(k_cheb_step, A->lanes, A->nrows, A->nrows, A->ia, A->ja, A->a, vk, vkm1, vkp1, y,
                  cc, t, mu0, muk, first);
   return launched("cheb_step");
+}
+
+int cheb_step_x(const pevsl_devcsr *A, const double *x, const double *vk, const double *vkm1,
+                double *vkp1, double *y, double cc, double t, double mu0, double muk, int first,
+                double *tmp) {
+  if (A->nrows <= 0) return 0;
+  if (A->lanes == 0) {
+    launch_stream(A, (const double *)A->a, x, EpiCheb{vk, vkm1, vkp1, y, cc, t, mu0, muk, first});
+    return launched("cheb_step_x");
+  }
+  if (spmv(A, x, tmp)) return PEVSL_ERR_CUDA;
+  return cheb_combine(A->nrows, tmp, vk, vkm1, vkp1, y, cc, t, mu0, muk, first);
+}
+
+int chebiter1_step(const pevsl_devcsr *B, const double *b, const double *x, double *p, double *xnew,
+                   double bet, double alp, double *tmp) {
+  const long n = B->nrows;
+  if (n <= 0) return 0;
+  if (B->lanes == 0) {
+    launch_stream(B, (const double *)B->a, x, EpiChebIter1{b, x, p, xnew, bet, alp});
+    return launched("chebiter1_step");
+  }
+  if (spmv(B, x, tmp)) return PEVSL_ERR_CUDA;
+  k_chebiter1_combine<<<grid_for(n, 4), kThreads, 0, ctx().stream>>>(n, tmp, b, x, p, xnew, bet, alp);
+  return launched("chebiter1_combine");
+}
+
+int chebiter2_step(const pevsl_devcsr *B, const double *d, double *x, double *r, double *dnew,
+                   double c1, double c2, double *tmp) {
+  const long n = B->nrows;
+  if (n <= 0) return 0;
+  if (B->lanes == 0) {
+    launch_stream(B, (const double *)B->a, d, EpiChebIter2{d, x, r, dnew, c1, c2});
+    return launched("chebiter2_step");
+  }
+  if (spmv(B, d, tmp)) return PEVSL_ERR_CUDA;
+  k_chebiter2_combine<<<grid_for(n, 4), kThreads, 0, ctx().stream>>>(n, tmp, d, x, r, dnew, c1, c2);
+  return launched("chebiter2_combine");
 }
 
 int cheb_step_batch(int nb, const ChebEntry *e, bool fp32) {

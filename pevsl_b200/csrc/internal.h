@@ -82,6 +82,29 @@ int pevsl_dense_symeig_range(int n, const double *H, int ldh, double lo, double 
 int pevsl_gen_symeig_range(int m, const double *H, const double *G, int ld, double lo, double hi,
                            int *nout, double *lam, double *Z, int ldz);
 void pevsl_simpson(const double *xi, double *yi, int npts);
+/* least-squares Chebyshev coefficients of ffun on [a, b] (mu has max_deg
+ * entries; the polynomial has degree *deg) */
+int pevsl_lspol_coefs(double (*ffun)(double), int max_deg, double tol, double a, double b,
+                      double *mu, int *deg, double *cc, double *dd);
+double (*pevsl_lspol_rec(void))(double);
+double (*pevsl_lspol_isqrt(void))(double);
+
+/* local vector length of a least-squares / Chebyshev-iteration B-solver */
+int pevsl_lspol_size(const void *lspol);
+int pevsl_chebiter_size(const void *cheb);
+
+/* ------------------------------------------------------------------ generalized
+ * problem (gpu_gen.cu): the ifGenEv branches of the solvers */
+int pevsl_gen_kpm_moments(pevsl_Data *pevsl, int Mdeg, const double *jac, double ctr, double wid,
+                          double beta1, double beta2, int vec_start, int vec_end, double *mu,
+                          double *tcnt);
+int pevsl_gen_landos_lanczos(pevsl_Data *pevsl, int maxit, const double *vinit, double *dT,
+                             double *eT);
+int pevsl_gen_lantrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pevsl_Parvec *vinit,
+                          int bndtype, double *lammin, double *lammax, FILE *fstats);
+int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
+                        pevsl_Polparams *pol, int *nevOut, double **lamo, pevsl_Parvecs **Wo,
+                        double **reso, int *its, FILE *fstats);
 
 /* RNG state (host side; rng.cu owns the device generator) */
 int pevsl_rng_mode(void);

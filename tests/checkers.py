@@ -193,6 +193,26 @@ class Checker:
                          C.c_double(pol["cc"]), C.c_double(pol["dd"]), _ptr(mu), _ptr(v), _ptr(y))
         return y
 
+    # -- B-solvers of the generalized problem (reference build only) ----
+    def lspol(self, kind, max_deg, tol, lmin, lmax, B: Csr, b):
+        """pEVSL_SetupLSPolRec (kind 0) / Sqrt (kind 1) on B: the degree,
+        coefficients mu[0..deg], cc, dd, and pEVSL_LSPolSol(b)."""
+        mu, x = np.zeros(max_deg), np.zeros(B.n)
+        deg, cc, dd = C.c_int(), C.c_double(), C.c_double()
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        self.f("lspol")(kind, max_deg, C.c_double(tol), C.c_double(lmin), C.c_double(lmax), B.n,
+                        _ptr(B.ia), _ptr(B.ja), _ptr(B.a), _ptr(mu), C.byref(deg), C.byref(cc),
+                        C.byref(dd), _ptr(bb), _ptr(x))
+        return deg.value, mu[:deg.value + 1].copy(), cc.value, dd.value, x
+
+    def chebiter(self, kind, lmin, lmax, deg, B: Csr, b):
+        """pEVSL_ChebIterSolv1 (kind 1) / Solv2 (kind 2) of b on B"""
+        x = np.zeros(B.n)
+        bb = np.ascontiguousarray(b, dtype=np.float64)
+        self.f("chebiter")(kind, C.c_double(lmin), C.c_double(lmax), deg, B.n, _ptr(B.ia),
+                           _ptr(B.ja), _ptr(B.a), _ptr(bb), _ptr(x))
+        return x
+
     def lantrbounds(self, A: Csr, lanm, maxit, tol, vinit, bndtype=1):
         lo, hi = C.c_double(), C.c_double()
         v = np.ascontiguousarray(vinit, dtype=np.float64)

@@ -6,7 +6,7 @@ reference is mounted, never on a GPU box) and writes small JSON files that
 the CPU tests use to pin the oracle restatement and the GPU tests use as
 known answers.  Floats are written with repr() so they round-trip exactly.
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [mm | gen]
 """
 from __future__ import annotations
 
@@ -190,6 +190,44 @@ def mm_case(refdir="/root/reference"):
     print("wrote", path, os.path.getsize(path), "bytes")
 
 
+def gen_case():
+    """The generalized problem.  (1) The reference's B-solvers on the 1D
+    Laplacian B of TESTS/Gen_Lap/LapPLanN.c (n = 512, diagonal 4): the
+    least-squares coefficients of 1/x and 1/sqrt(x) and one solve each, and
+    Chebyshev-iteration solves -> gen_bsolve.json.  (2) That driver, built
+    against the reference with the Chebyshev B-solver of tests/dropin/shim
+    (`make -C oracle drivers`), with KPM and with Lanczos DOS -> genlap8.json
+    (its screen output and OUT/LapPLanN_G0.out)."""
+    import subprocess
+    import tempfile
+    ref = Checker("ref")
+    B = laplacian(512, 1, 1)
+    b = np.cos(0.1 * np.arange(B.n, dtype=np.float64)) + 0.5
+    ls = []
+    for kind, max_deg, tol in ((0, 50, 1e-6), (1, 50, 1e-6), (0, 80, 1e-10), (1, 120, 1e-12)):
+        deg, mu, cc, dd, x = ref.lspol(kind, max_deg, tol, 2.0, 6.0, B, b)
+        ls.append(dict(kind=kind, max_deg=max_deg, tol=tol, lmin=2.0, lmax=6.0, deg=deg,
+                       mu=fl(mu), cc=cc, dd=dd, x=fl(x)))
+    ci = []
+    for kind, deg in ((1, 1), (1, 12), (2, 0), (2, 12), (2, 40)):
+        ci.append(dict(kind=kind, deg=deg, lmin=2.0, lmax=6.0,
+                       x=fl(ref.chebiter(kind, 2.0, 6.0, deg, B, b))))
+    dump("gen_bsolve.json", dict(B="laplacian(512,1,1)", b="cos(0.1 i) + 0.5", lspol=ls,
+                                 chebiter=ci))
+    root = os.path.dirname(os.path.dirname(HERE))
+    exe = os.path.join(root, "oracle", "_ref", "GenLapPLanN")
+    runs = {}
+    for name, args in (("kpm", ["-ngroups", "1"]),
+                       ("landos", ["-ngroups", "1", "-dostype", "1", "-nslices", "3"])):
+        with tempfile.TemporaryDirectory() as d:
+            os.makedirs(os.path.join(d, "OUT"))
+            r = subprocess.run([exe] + args, cwd=d, check=True, capture_output=True, text=True,
+                               env=dict(os.environ, OPENBLAS_NUM_THREADS="1"))
+            with open(os.path.join(d, "OUT", "LapPLanN_G0.out")) as f:
+                runs[name] = dict(args=args, stdout=r.stdout, out=f.read())
+    dump("genlap8.json", runs)
+
+
 def write_mm(path, n, I, J, V):
     """A symmetric Matrix Market file with the given entries (repr floats:
     they read back to the same doubles)."""
@@ -210,6 +248,9 @@ def write_matfile(path, mtx, intervals):
 if __name__ == "__main__":
     if sys.argv[1:] == ["mm"]:
         mm_case()
+    elif sys.argv[1:] == ["gen"]:
+        gen_case()
     else:
         main()
         mm_case()
+        gen_case()

@@ -25,7 +25,7 @@ def rel(a, b):
 
 def declared_functions():
     names = set()
-    for h in ("pevsl.h", "pevsl_b200.h"):
+    for h in ("pevsl.h", "pevsl_b200.h", "pevsl_itsol.h", "pevsl_f90.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         kept, cont = [], False
