@@ -44,6 +44,12 @@ WORKLOADS = {
     # 32 shifted 2D/3D Laplacians, n 1e4..5e5, 2..8 slices each (a count
     # interpretation of "~2% of the spectrum": 20 eigenvalues per slice)
     "lap_multi_32": dict(multi=True, count=32, seed=2024, per_slice=20),
+    # the generalized problem of TESTS/Gen_Lap/LapPLanN.c scaled up: A the 3D
+    # Laplacian, B the 1D Laplacian (diagonal 4) of the same size; B-solve
+    # by the least-squares 1/x on [2, 6] (degree 24 at tol 1e-10, rounding
+    # level), L^{-T} by the least-squares 1/sqrt(x) (max degree 50, 1e-6)
+    "genlap24": dict(gen=True, grid=(24, 24, 24), a=1.0, b=1.0094, nslices=2, Mdeg=100, nvec=30,
+                     bsol=("lsrec", 80, 1e-10), ltsol=("lssqrt", 50, 1e-6), brange=(2.0, 6.0)),
 }
 DEFAULT_WORKLOAD = "lap100_4slices"
 METRIC = "eigenpairs/s at residual <= 1e-8 (3D Laplacian 100^3, [0.80,0.82], 4 slices, FP64)"
@@ -52,8 +58,40 @@ METRIC = "eigenpairs/s at residual <= 1e-8 (3D Laplacian 100^3, [0.80,0.82], 4 s
 def metric_of(w):
     """The metric string of a single-problem workload."""
     g = w["grid"]
+    if w.get("gen"):
+        return (f"eigenpairs/s at ||A x - lam B x|| <= 1e-8 (A x = lam B x: A 3D Laplacian "
+                f"{g[0]}^3, B 1D Laplacian, [{w['a']:.4f},{w['b']:.4f}], {w['nslices']} slices, "
+                f"FP64)")
     return (f"eigenpairs/s at residual <= 1e-8 (3D Laplacian {g[0]}^3, [{w['a']:.2f},{w['b']:.2f}], "
             f"{w['nslices']} slices, FP64)")
+
+
+class GenSetup:
+    """B (1D Laplacian of the same size as A) on the device and the
+    B-solvers of a generalized workload; install(ev) makes an instance
+    generalized (pEVSL_SetBParcsr, SetBSol, SetLTSol, SetGenEig)."""
+
+    def __init__(self, w, n, pinned=None):
+        import pevsl_b200 as pv
+        from pevsl_b200.problems import laplacian
+        if pinned is None:
+            _, ib, jb, b = laplacian(n, 1, 1)
+        else:
+            ib, jb, b = pinned
+        self.B = pv.Matrix.from_csr(n, ib, jb, b)
+        lo, hi = w["brange"]
+        k, deg, tol = w["bsol"]
+        self.bsol = pv.BSolver(self.B, k, lo, hi, deg, tol)
+        k, deg, tol = w["ltsol"]
+        self.ltsol = pv.BSolver(self.B, k, lo, hi, deg, tol)
+
+    def install(self, ev):
+        ev.set_generalized(self.B, self.bsol, self.ltsol)
+
+    def free(self):
+        self.bsol.free()
+        self.ltsol.free()
+        self.B.free()
 
 
 def slice_run(w, seed):
@@ -193,6 +231,31 @@ def cpu_reference_sample(n, ia, ja, a, fil, seconds_budget=30.0):
     return (time.perf_counter() - t) / d, d
 
 
+def cpu_reference_gen_sample(w, n, ia, ja, a, fil, seconds_budget=30.0):
+    """Time the reference's generalized pEVSL_ChebAv (oracle/_ref): per
+    degree one B-solve (its least-squares polynomial, pEVSL_LSPolSol) and
+    one A matvec, on one core.  Returns seconds per degree."""
+    from pevsl_b200.problems import laplacian
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so"))
+    _, ib, jb, b = laplacian(n, 1, 1)
+    mu = np.ascontiguousarray(fil.mu[: fil.deg + 1])
+    v = np.cos(np.arange(n) * 0.1)
+    y = np.zeros(n)
+    P = lambda x: x.ctypes.data_as(C.c_void_p)  # noqa: E731
+    k, lsdeg, lstol = w["bsol"]
+    lo, hi = w["brange"]
+
+    def run(d):
+        t = time.perf_counter()
+        lib.oref_gen_chebav(n, P(ia), P(ja), P(a), P(ib), P(jb), P(b), lsdeg, C.c_double(lstol),
+                            C.c_double(lo), C.c_double(hi), d, C.c_double(fil.cc),
+                            C.c_double(fil.dd), P(mu), P(v), P(y))
+        return time.perf_counter() - t
+    per = run(10) / 10
+    d = int(max(10, min(fil.deg, seconds_budget / max(per, 1e-9))))
+    return run(d) / d, d
+
+
 # ---------------------------------------------------------------- our arm
 def run_b200(args, dist):
     import pevsl_b200 as pv
@@ -211,11 +274,19 @@ def run_b200(args, dist):
     a_p, p3 = pv.pinned_empty(nnz, np.float64)
     ia_p[:], ja_p[:], a_p[:] = ia, ja, a
     M = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
+    gen = bool(w.get("gen"))
+    gs, bpins = None, []
+    if gen:
+        _, ib, jb, bv = laplacian(n, 1, 1)
+        bpins = [pv.pinned_empty(n + 1, np.int32), pv.pinned_empty(len(jb), np.int32),
+                 pv.pinned_empty(len(jb), np.float64)]
+        bpins[0][0][:], bpins[1][0][:], bpins[2][0][:] = ib, jb, bv
+        gs = GenSetup(w, n, (bpins[0][0], bpins[1][0], bpins[2][0]))
 
     batched = args.path == "batched"
 
     def step():
-        return pv.solve_interval(M, spec, batched=batched)
+        return pv.solve_interval(M, spec, batched=batched, setup=gs.install if gen else None)
 
     for _ in range(args.warmup):
         r = step()
@@ -224,19 +295,27 @@ def run_b200(args, dist):
     clocks.start()
     pv.load().pEVSL_B200_Sync()
     pv.load().pEVSL_B200_ResetFilterCounters()
+    pv.load().pEVSL_B200_ResetGenCounters()
     l0 = pv.launch_count()
-    lib.pEVSL_B200_EventRecord(0)
     eig = 0
     results = []
+    ms = 0.0
     for _ in range(args.steps):
+        lib.pEVSL_B200_FlushL2(0)  # L2 flushed between timed steps (outside the events)
+        lib.pEVSL_B200_EventRecord(0)
         r = step()
+        lib.pEVSL_B200_EventRecord(1)
+        ms += lib.pEVSL_B200_EventElapsedMs(0, 1)
         results.append(r)
         eig += sum(r.nev)
-    lib.pEVSL_B200_EventRecord(1)
-    ms = lib.pEVSL_B200_EventElapsedMs(0, 1)
     clk = clocks.stop()
     launches = pv.launch_count() - l0
     f_launch, f_bytes, f_ms = pv.filter_counters()
+    if gen:
+        # the generalized filter: one "launch" is one filter degree (the
+        # B-solve's fused degrees on B and the fused A step), timed per
+        # application (CUDA graph replays)
+        _, f_launch, f_bytes, f_ms = pv.gen_counters()
     dist.barrier()
     t_max = dist.max(ms / 1e3)
     eig_all = dist.sum(float(eig))
@@ -249,7 +328,10 @@ def run_b200(args, dist):
     d2h = 0
     for _ in range(args.steps):
         M2 = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
-        r2 = pv.solve_interval(M2, spec, batched=batched)
+        gs2 = GenSetup(w, n, (bpins[0][0], bpins[1][0], bpins[2][0])) if gen else None
+        r2 = pv.solve_interval(M2, spec, batched=batched, setup=gs2.install if gen else None)
+        if gs2:
+            gs2.free()
         M2.free()
         e2e_eig += sum(r2.nev)
         d2h += sum(len(x) for x in r2.lam) * 16
@@ -277,9 +359,14 @@ def run_b200(args, dist):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic: 3D Dirichlet Laplacian generated on the host, seeded Philox Gaussian "
-                "random vectors (seed 1000*rank)",
+        "data": ("synthetic: 3D Dirichlet Laplacian A" + (" and 1D Laplacian B (diagonal 4)"
+                 if gen else "") + " generated on the host, seeded Philox Gaussian random "
+                 "vectors (seed 1000*rank)"),
         "config": {"workload": args.workload, "n": n, "nnz": nnz, "interval": [w["a"], w["b"]],
+                   **({"problem": "generalized A x = lam B x (pEVSL_SetGenEig)",
+                       "b_solve": "least-squares 1/x on [2, 6], pEVSL_SetupLSPolRec(80, 1e-10)",
+                       "lt_solve": "least-squares 1/sqrt(x), pEVSL_SetupLSPolSqrt(50, 1e-6)"}
+                      if gen else {}),
                    "nslices": w["nslices"], "kpm_mdeg": w["Mdeg"], "kpm_nvec": w["nvec"],
                    "bounds": "thick-restart Lanczos (50, 200, 1e-8)", "tol": 1e-8,
                    "precision": "fp64",
@@ -288,24 +375,41 @@ def run_b200(args, dist):
                             "slice by slice (pEVSL_ChebLanNr, the drop-in path)"),
                    "eigenpairs_per_step": sum(r0.nev), "nev_per_slice": r0.nev,
                    "lanczos_steps_per_slice": r0.its, "filter_degree_per_slice": r0.deg,
-                   "l2": "matrix + vectors ~120 MB per filter degree against a 126 MB L2; "
-                         "no flush between steps (each step streams the working set "
-                         "thousands of times)",
+                   "l2": "256 MiB written between timed steps (L2 flush); within a step the "
+                         "working set streams thousands of times",
                    "parallelism": f"replicas x{dist.world}"},
         "gpu_launches": int(launches),
         "clocks": clk,
         "roofline": {
-            "kernel": ("cheb_step_batch (fused SpMV + Chebyshev recurrence, CSR-stream, all slices per launch)"
+            "kernel": ("generalized filter degree (B-solve: fused Chebyshev degrees on B; A step "
+                       "fused with the recurrence), CUDA-graph replays; one launch = one degree"
+                       if gen else
+                       "cheb_step_batch (fused SpMV + Chebyshev recurrence, CSR-stream, all slices per launch)"
                        if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream)"),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
             "bytes_per_launch": per_launch_bytes, "launches": f_launch,
             "avg_launch_us": per_launch_ms * 1e3, "traffic": ncu_traffic(args.workload)},
         "e2e": {"value": e2e_val, "unit": "eigenpairs/s",
-                "h2d_bytes_per_step": int(4 * (n + 1) + 12 * nnz),
+                "h2d_bytes_per_step": int(4 * (n + 1) + 12 * nnz +
+                                          (4 * (n + 1) + 12 * (3 * n - 2) if gen else 0)),
                 "d2h_bytes_per_step": int(d2h // max(args.steps, 1))},
     }
-    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and gen:
+        try:
+            r, fil = pv.findpol([r0.sli[0], r0.sli[1], r0.lmin, r0.lmax], 3000, 2, 0.8, 0.2)
+            per, d = cpu_reference_gen_sample(w, n, ia, ja, a, fil)
+            degs = sum(dg * (it + 1) for dg, it in zip(r0.deg, r0.its)) + w["Mdeg"] * w["nvec"] + 200
+            out["cpu_baseline"] = {
+                "value": sum(r0.nev) / (per * degs), "unit": "eigenpairs/s", "cores": 1,
+                "kind": "reference",
+                "sample": f"reference generalized pEVSL_ChebAv (oracle/_ref, least-squares B-solve, "
+                          f"OpenBLAS 1 thread) of degree {d} with slice 0's filter: "
+                          f"{per*1e3:.2f} ms per degree; extrapolated to this run's "
+                          f"{degs} degrees (filters x Lanczos steps, KPM, <=200 bounds steps)"}
+        except Exception as e:
+            out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
+    elif dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         try:
             r, fil = pv.findpol([r0.sli[0], r0.sli[1], r0.lmin, r0.lmax], 3000, 2, 0.8, 0.2)
             per, d = cpu_reference_sample(n, ia, ja, a, fil)
@@ -324,7 +428,9 @@ def run_b200(args, dist):
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
     M.free()
-    for p in (p1, p2, p3):
+    if gs:
+        gs.free()
+    for p in [p1, p2, p3] + [bp[1] for bp in bpins]:
         pv.free_pinned(p)
     return out
 
@@ -380,10 +486,13 @@ def run_b200_multi(args, dist):
     lib.pEVSL_B200_Sync()
     lib.pEVSL_B200_ResetFilterCounters()
     l0 = pv.launch_count()
-    lib.pEVSL_B200_EventRecord(0)
-    eig = sum(solve(mats) for _ in range(args.steps))
-    lib.pEVSL_B200_EventRecord(1)
-    ms = lib.pEVSL_B200_EventElapsedMs(0, 1)
+    eig, ms = 0, 0.0
+    for _ in range(args.steps):
+        lib.pEVSL_B200_FlushL2(0)  # L2 flushed between timed steps (outside the events)
+        lib.pEVSL_B200_EventRecord(0)
+        eig += solve(mats)
+        lib.pEVSL_B200_EventRecord(1)
+        ms += lib.pEVSL_B200_EventElapsedMs(0, 1)
     clk = clocks.stop()
     launches = pv.launch_count() - l0
     f_launch, f_bytes, f_ms = pv.filter_counters()
@@ -446,14 +555,17 @@ def run_b200_multi(args, dist):
 
 
 # ---------------------------------------------------------------- reference arm
-def _ref_slice_worker(q, n, ia, ja, a, deg, cc, dd, mu, budget):
+def _ref_slice_worker(q, n, ia, ja, a, deg, cc, dd, mu, budget, gen_w=None):
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
 
     class F:
         pass
     f = F()
     f.deg, f.cc, f.dd, f.mu = deg, cc, dd, mu
-    q.put(cpu_reference_sample(n, ia, ja, a, f, budget))
+    if gen_w:
+        q.put(cpu_reference_gen_sample(gen_w, n, ia, ja, a, f, budget))
+    else:
+        q.put(cpu_reference_sample(n, ia, ja, a, f, budget))
 
 
 def run_reference(args, dist):
@@ -462,6 +574,8 @@ def run_reference(args, dist):
     per slice as the reference's MPI groups, each step a bounded sample."""
     if dist.rank != 0:
         return None
+    if WORKLOADS[args.workload].get("gen") and args.workload not in REF_COUNTS:
+        return {"impl": "reference", "unavailable": "per-slice counts of this workload not recorded"}
     if WORKLOADS[args.workload].get("multi"):
         return {"impl": "reference", "unavailable": "the reference arm times the single-problem "
                 "workloads (lap100_4slices, lap20_5slices)"}
@@ -473,17 +587,22 @@ def run_reference(args, dist):
     n, ia, ja, a = laplacian(*w["grid"])
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so"))
     P = lambda x: x.ctypes.data_as(C.c_void_p)  # noqa: E731
-    # bounds with the reference's thick-restart Lanczos (real run)
-    lib.oref_set_unit_rng(1, C.c_uint64(0))
-    v0 = np.cos(np.arange(n) * 0.37)
+    counts = REF_COUNTS.get(args.workload)
+    gen = bool(w.get("gen"))
     lo, hi = C.c_double(), C.c_double()
-    lib.oref_lantrbounds(n, P(ia), P(ja), P(a), 50, 200, C.c_double(1e-8), P(v0), 1, C.byref(lo),
-                         C.byref(hi))
+    if gen:
+        # spectrum bounds of B^{-1} A recorded with the counts below
+        lo.value, hi.value = counts["bounds"]
+    else:
+        # bounds with the reference's thick-restart Lanczos (real run)
+        lib.oref_set_unit_rng(1, C.c_uint64(0))
+        v0 = np.cos(np.arange(n) * 0.37)
+        lib.oref_lantrbounds(n, P(ia), P(ja), P(a), 50, 200, C.c_double(1e-8), P(v0), 1,
+                             C.byref(lo), C.byref(hi))
     nsl = w["nslices"]
     cores = min(os.cpu_count() or 1, nsl)
     ctx = mp.get_context("spawn")
     times = []
-    counts = REF_COUNTS.get(args.workload)
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         q = ctx.Queue()
@@ -492,7 +611,8 @@ def run_reference(args, dist):
         for s in range(nsl):
             r, fil = pv.findpol([edges[s], edges[s + 1], lo.value, hi.value], 3000, 2, 0.8, 0.2)
             p = ctx.Process(target=_ref_slice_worker,
-                            args=(q, n, ia, ja, a, fil.deg, fil.cc, fil.dd, fil.mu, 20.0))
+                            args=(q, n, ia, ja, a, fil.deg, fil.cc, fil.dd, fil.mu, 20.0,
+                                  w if gen else None))
             p.start()
             procs.append(p)
         per = [q.get() for _ in procs]
@@ -519,7 +639,8 @@ def run_reference(args, dist):
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * float(np.mean(times)) if times else None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: 3D Dirichlet Laplacian", "impl": "reference",
+            "data": "synthetic: 3D Dirichlet Laplacian" + (" A, 1D Laplacian B" if gen else ""),
+            "impl": "reference",
             "config": {"workload": args.workload, "n": n, "nnz": int(ia[-1])},
             "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": cores,
                              "kind": "reference", "sample": how},

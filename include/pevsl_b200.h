@@ -197,6 +197,18 @@ void pEVSL_B200_ManagedFree(void *p);
 void pEVSL_B200_FilterCounters(uint64_t *launches, double *bytes, double *ms);
 void pEVSL_B200_ResetFilterCounters(void);
 
+/* The generalized filter's counters since the last reset: filter
+ * applications and degrees inside pEVSL_ChebLanNr with ifGenEv, their
+ * algorithmic HBM bytes (per degree: the B-solve's matrix passes and
+ * vectors, and the fused A step) and the device time of the applications
+ * (CUDA events around each). */
+void pEVSL_B200_GenCounters(uint64_t *filters, uint64_t *degrees, double *bytes, double *ms);
+
+/* Benchmark helper: write `bytes` (0: 256 MiB, twice the L2) of a scratch
+ * device buffer on the library stream, evicting earlier data from L2. */
+int pEVSL_B200_FlushL2(size_t bytes);
+void pEVSL_B200_ResetGenCounters(void);
+
 /* Short build/device description into buf (NUL-terminated). */
 int pEVSL_B200_Info(char *buf, int len);
 

@@ -469,3 +469,44 @@ int oref_chebiter(int kind, double lmin, double lmax, int deg, int n, const int 
   pEVSL_ParcsrFree(&A);
   return 0;
 }
+
+/* y = p(A B^{-1}) v through the reference's pEVSL_ChebAv with ifGenEv
+ * (SRC/chebpol.c:538-546), B-solve pEVSL_LSPolSol of the least-squares
+ * 1/x on [blo, bhi] (max degree lsdeg, tolerance lstol): the CPU sample of
+ * the generalized filter. */
+int oref_gen_chebav(int n, const int *ia, const int *ja, const double *a, const int *ib,
+                    const int *jb, const double *b, int lsdeg, double lstol, double blo, double bhi,
+                    int deg, double cc, double dd, const double *mu, const double *v, double *y) {
+  pevsl_Parcsr A, B;
+  pevsl_Data *pevsl;
+  pevsl_Parvec vv, yv, w[4];
+  pevsl_Polparams pol;
+  void *bsol = NULL;
+  build_parcsr(n, ia, ja, a, &A);
+  build_parcsr(n, ib, jb, b, &B);
+  pEVSL_SetupLSPolRec(lsdeg, lstol, blo, bhi, &B, &bsol);
+  pEVSL_Start(MPI_COMM_WORLD, &pevsl);
+  pEVSL_SetAParcsr(pevsl, &A);
+  pEVSL_SetBParcsr(pevsl, &B);
+  pEVSL_SetBSol(pevsl, pEVSL_LSPolSol, bsol);
+  pEVSL_SetGenEig(pevsl);
+  pEVSL_SetPolDef(&pol);
+  pol.deg = deg;
+  pol.cc = cc;
+  pol.dd = dd;
+  pol.mu = (double *)mu;
+  pEVSL_ParvecCreate(n, n, 0, MPI_COMM_WORLD, &vv);
+  pEVSL_ParvecDupl(&vv, &yv);
+  for (int i = 0; i < 4; i++) pEVSL_ParvecDupl(&vv, &w[i]);
+  memcpy(vv.data, v, (size_t)n * sizeof(double));
+  pEVSL_ChebAv(pevsl, &pol, &vv, &yv, w);
+  memcpy(y, yv.data, (size_t)n * sizeof(double));
+  for (int i = 0; i < 4; i++) pEVSL_ParvecFree(&w[i]);
+  pEVSL_ParvecFree(&vv);
+  pEVSL_ParvecFree(&yv);
+  pEVSL_Finish(pevsl);
+  pEVSL_LSPolFree(bsol);
+  pEVSL_ParcsrFree(&A);
+  pEVSL_ParcsrFree(&B);
+  return 0;
+}

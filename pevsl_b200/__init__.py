@@ -157,6 +157,9 @@ SIGNATURES = [
     ("pEVSL_B200_ChebAv", _I, [C.POINTER(PevslData), C.POINTER(Polparams), _vp, _vp]),
     ("pEVSL_B200_ChebAvGen", _I, [C.POINTER(PevslData), C.POINTER(Polparams), _vp, _vp]),
     ("pEVSL_SetBParcsr", _I, [C.POINTER(PevslData), C.POINTER(Parcsr)]),
+    ("pEVSL_B200_GenCounters", None, [C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), _dp, _dp]),
+    ("pEVSL_B200_ResetGenCounters", None, []),
+    ("pEVSL_B200_FlushL2", _I, [C.c_size_t]),
     ("pEVSL_SetBSol", _I, [C.POINTER(PevslData), _vp, _vp]),
     ("pEVSL_SetLTSol", _I, [C.POINTER(PevslData), _vp, _vp]),
     ("pEVSL_SetupLSPolRec", None, [_I, _D, _D, _D, C.POINTER(Parcsr), C.POINTER(_vp)]),
@@ -838,12 +841,22 @@ class SliceResult:
     fallbacks: int = 0            # mixed form: slices solved again in FP64
 
 
+def gen_counters():
+    """(filters, degrees, bytes, ms) of the generalized filter since the
+    last reset (pEVSL_B200_GenCounters)."""
+    f, d = C.c_uint64(), C.c_uint64()
+    b, ms = C.c_double(), C.c_double()
+    load().pEVSL_B200_GenCounters(C.byref(f), C.byref(d), C.byref(b), C.byref(ms))
+    return f.value, d.value, b.value, ms.value
+
+
 def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
-                   precision: int = PREC_FP64) -> SliceResult:
+                   precision: int = PREC_FP64, setup=None) -> SliceResult:
     """Run the whole slicing path through the C API, in the reference
     drivers' order: start vector, bounds, DOS, slicer, then each slice
     (one pEVSL_ChebLanNr per slice, or all slices in lockstep through
-    pEVSL_B200_ChebLanNrBatch when batched)."""
+    pEVSL_B200_ChebLanNrBatch when batched).  setup(instance), if given,
+    runs right after pEVSL_Start (e.g. Instance.set_generalized)."""
     import time
     lib = load()
     t_all = time.perf_counter()
@@ -852,6 +865,8 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
         # pEVSL_Start reseeds rand() with srand(0); restart the chosen stream
         set_rng(s.rng_mode, s.seed)
         ev.set_precision(precision)
+        if setup is not None:
+            setup(ev)
         vinit = Vector(A.n)
         lib.pEVSL_ParvecRand(C.byref(vinit.pv))
         times = {}

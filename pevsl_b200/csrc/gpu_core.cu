@@ -480,6 +480,27 @@ double pEVSL_B200_EventElapsedMs(int a, int b) {
   return (double)ms;
 }
 
+/* write `bytes` (0: 256 MiB, twice the L2) of a scratch device buffer on
+ * the library stream, so that the next timed work finds nothing of its own
+ * in L2 */
+int pEVSL_B200_FlushL2(size_t bytes) {
+  static void *buf = nullptr;
+  static size_t cap = 0;
+  static int val = 0;
+  if (ensure()) return PEVSL_ERR_CUDA;
+  if (!bytes) bytes = (size_t)256 << 20;
+  if (bytes > cap) {
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    cap = 0;
+    if (fail(cudaMalloc(&buf, bytes), "cudaMalloc flush")) return PEVSL_ERR_NOMEM;
+    cap = bytes;
+  }
+  val = (val + 1) & 0xff;
+  if (fail(cudaMemsetAsync(buf, val, bytes, g_ctx.stream), "cudaMemsetAsync flush")) return PEVSL_ERR_CUDA;
+  return 0;
+}
+
 void *pEVSL_B200_HostAlloc(size_t bytes) {
   void *p = nullptr;
   if (ensure() || fail(cudaMallocHost(&p, bytes ? bytes : 1), "cudaMallocHost")) return nullptr;

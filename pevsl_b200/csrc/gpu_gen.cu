@@ -152,14 +152,23 @@ void chebiter_flush(pevsl_chebiter *C) {
   C->used = 0;
 }
 
+bool capturing() {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  return cudaStreamIsCapturing(ctx().stream, &cs) == cudaSuccess &&
+         cs != cudaStreamCaptureStatusNone;
+}
+
+/* a solve inside a captured graph is not timed (its events would belong to
+ * the capture) */
 int chebiter_time(pevsl_chebiter *C, int (*f)(pevsl_chebiter *, const double *, double *),
                   const double *b, double *x) {
-  if (C->ev_ok) {
+  const bool timed = C->ev_ok && !capturing();
+  if (timed) {
     if (C->used == 32) chebiter_flush(C);
     cudaEventRecord(C->ev[2 * C->used], ctx().stream);
   }
   const int st = f(C, b, x);
-  if (C->ev_ok) cudaEventRecord(C->ev[2 * C->used++ + 1], ctx().stream);
+  if (timed) cudaEventRecord(C->ev[2 * C->used++ + 1], ctx().stream);
   return st;
 }
 
@@ -247,6 +256,67 @@ int nrm_host(long n, const double *x, double *out) {
 
 long gen_ld(long n) { return (n + 31) / 32 * 32; }
 
+/* ------------------------------------------------ generalized filter counters
+ * applications, algorithmic HBM bytes and device time (CUDA events around
+ * each application) of the generalized filter: pEVSL_B200_GenCounters */
+uint64_t g_gen_filters = 0, g_gen_degrees = 0;
+double g_gen_bytes = 0.0, g_gen_ms = 0.0;
+
+struct EvPool {
+  static constexpr int kPairs = 64;
+  cudaEvent_t ev[2 * kPairs];
+  int used = 0;
+  bool ok = false, init = false;
+  void begin() {
+    if (!init) {
+      init = ok = true;
+      for (int i = 0; i < 2 * kPairs && ok; i++) ok = cudaEventCreate(&ev[i]) == cudaSuccess;
+    }
+    if (!ok) return;
+    if (used == kPairs) flush();
+    cudaEventRecord(ev[2 * used], ctx().stream);
+  }
+  void end() {
+    if (ok) cudaEventRecord(ev[2 * used++ + 1], ctx().stream);
+  }
+  void flush() {
+    if (!ok || !used) return;
+    cudaEventSynchronize(ev[2 * used - 1]);
+    for (int i = 0; i < used; i++) {
+      float ms = 0.f;
+      if (cudaEventElapsedTime(&ms, ev[2 * i], ev[2 * i + 1]) == cudaSuccess) g_gen_ms += ms;
+    }
+    used = 0;
+  }
+};
+EvPool g_gen_ev;
+
+/* algorithmic bytes: a matrix pass is entry_bytes (3 packed, 12 plain) per
+ * entry + 4 (n + 1); a fused
+ * Chebyshev degree adds v_k, v_{k-1}, y read and v_{k+1}, y written (the
+ * first degree reads neither v_{k-1} nor y); a second-kind Chebyshev-
+ * iteration step gathers d and reads/writes x and r, writes d_new */
+double mat_bytes(const pevsl_devcsr *M) {
+  return entry_bytes(M, false) * (double)M->nnz + 4.0 * (M->nrows + 1.0);
+}
+
+double solve_bytes(pevsl_Data *pevsl) {
+  const SVFunc f = pevsl->Bsol ? pevsl->Bsol->func : nullptr;
+  if (f == pEVSL_LSPolSol) {
+    const pevsl_lspol *L = (const pevsl_lspol *)pevsl->Bsol->data;
+    const double n = L->B->nrows;
+    double b = 0.0;
+    for (int k = 1; k <= L->deg; k++) b += mat_bytes(L->B) + (k == 1 ? 24.0 : 40.0) * n;
+    return b;
+  }
+  if (f == pEVSL_ChebIterSolv1 || f == pEVSL_ChebIterSolv2) {
+    const pevsl_chebiter *C = (const pevsl_chebiter *)pevsl->Bsol->data;
+    const double n = C->A->nrows;
+    return C->deg * (mat_bytes(C->A) + 48.0 * n) + 32.0 * n;
+  }
+  return 0.0;
+}
+
 /* The generalized filter (pEVSL_ChebAv with ifGenEv, SRC/chebpol.c:509-574):
  * y = p(A B^{-1}) v, each degree a B-solve then the fused degree kernel
  * whose SpMV reads B^{-1} v_k.  w holds 4 n doubles. */
@@ -262,6 +332,12 @@ int gen_filter(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, d
     return vscal(y, n, mu[0]);
   }
   if (!A && (!pevsl->Amv || !pevsl->Amv->func)) return PEVSL_ERR_NOMATVEC;
+  if (A) {
+    const double sb = solve_bytes(pevsl);
+    for (int k = 1; k <= m; k++) g_gen_bytes += sb + mat_bytes(A) + (k == 1 ? 32.0 : 48.0) * n;
+  }
+  g_gen_degrees += (uint64_t)m;
+  g_gen_filters++;
   double *buf[2] = {w, w + n}, *w2 = w + 2 * n, *tmp = w + 3 * n;
   const double *vk = v, *vkm1 = nullptr;
   int st = 0;
@@ -282,6 +358,110 @@ int gen_filter(pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v, d
   return st;
 }
 
+/* The library's own B-solvers enqueue a fixed sequence of launches with
+ * no host synchronisation, so a generalized filter application (or a KPM
+ * vector's degree loop) that uses one can be captured once in a CUDA graph
+ * and replayed: at n ~ 10^5 a degree is 40+ short launches whose gaps would
+ * otherwise cost as much as the kernels. */
+bool graphable(pevsl_Data *pevsl) {
+  if (!pevsl_builtin_A(pevsl) || !pevsl->Bsol) return false;
+  const SVFunc f = pevsl->Bsol->func;
+  if (f != pEVSL_LSPolSol && f != pEVSL_ChebIterSolv1 && f != pEVSL_ChebIterSolv2) return false;
+  return !capturing() && getenv("PEVSL_B200_GEN_GRAPH") == nullptr;
+}
+
+/* choose the row kernels of A and of the B-solver's matrix before a
+ * capture (the tuning times launches, which a capture cannot) */
+void pretune(pevsl_Data *pevsl) {
+  stream_tune(pevsl_builtin_A(pevsl));
+  const SVFunc f = pevsl->Bsol->func;
+  if (f == pEVSL_LSPolSol)
+    stream_tune(((pevsl_lspol *)pevsl->Bsol->data)->B);
+  else
+    stream_tune(((pevsl_chebiter *)pevsl->Bsol->data)->A);
+}
+
+/* a captured launch sequence and the statistics one replay stands for */
+struct GenGraph {
+  cudaGraphExec_t exec = nullptr;
+  size_t d_mvA = 0, d_svB = 0, d_polAv = 0, d_chebmv = 0;
+  uint64_t d_launches = 0, d_filters = 0, d_degrees = 0;
+  double d_bytes = 0.0;
+  ~GenGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+pevsl_chebiter *bsol_chebiter(pevsl_Data *pevsl) {
+  const SVFunc f = pevsl->Bsol->func;
+  return (f == pEVSL_ChebIterSolv1 || f == pEVSL_ChebIterSolv2) ? (pevsl_chebiter *)pevsl->Bsol->data
+                                                                : nullptr;
+}
+
+/* capture body() into g (first call) and replay it */
+template <class Body>
+int graph_run(GenGraph &g, pevsl_Data *pevsl, Body body) {
+  Ctx &c = ctx();
+  pevsl_chebiter *C = bsol_chebiter(pevsl);
+  if (!g.exec) {
+    const size_t m0 = pevsl->stats->n_mvA, s0 = pevsl->stats->n_svB, p0 = pevsl->stats->n_polAv;
+    const size_t c0 = C ? C->n_chebmv : 0;
+    const uint64_t l0 = c.launches, f0 = g_gen_filters, dg0 = g_gen_degrees;
+    const double b0 = g_gen_bytes;
+    if (fail(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal), "BeginCapture"))
+      return PEVSL_ERR_CUDA;
+    const int st = body();
+    cudaGraph_t gr = nullptr;
+    const cudaError_t ec = cudaStreamEndCapture(c.stream, &gr);
+    if (st || fail(ec, "EndCapture")) {
+      if (gr) cudaGraphDestroy(gr);
+      return st ? st : PEVSL_ERR_CUDA;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&g.exec, gr, 0);
+    cudaGraphDestroy(gr);
+    if (fail(ei, "cudaGraphInstantiate")) {
+      g.exec = nullptr;
+      return PEVSL_ERR_CUDA;
+    }
+    /* the capture counted the statistics once; each replay adds them */
+    g.d_mvA = pevsl->stats->n_mvA - m0;
+    g.d_svB = pevsl->stats->n_svB - s0;
+    g.d_polAv = pevsl->stats->n_polAv - p0;
+    g.d_chebmv = C ? C->n_chebmv - c0 : 0;
+    g.d_launches = c.launches - l0;
+    g.d_filters = g_gen_filters - f0;
+    g.d_degrees = g_gen_degrees - dg0;
+    g.d_bytes = g_gen_bytes - b0;
+    g_gen_filters = f0;
+    g_gen_degrees = dg0;
+    g_gen_bytes = b0;
+    pevsl->stats->n_mvA = m0;
+    pevsl->stats->n_svB = s0;
+    pevsl->stats->n_polAv = p0;
+    if (C) C->n_chebmv = c0;
+    c.launches = l0;
+  }
+  pevsl->stats->n_mvA += g.d_mvA;
+  pevsl->stats->n_svB += g.d_svB;
+  pevsl->stats->n_polAv += g.d_polAv;
+  if (C) C->n_chebmv += g.d_chebmv;
+  c.launches += g.d_launches;
+  g_gen_filters += g.d_filters;
+  g_gen_degrees += g.d_degrees;
+  g_gen_bytes += g.d_bytes;
+  return fail(cudaGraphLaunch(g.exec, c.stream), "cudaGraphLaunch");
+}
+
+/* the generalized filter through a graph over the staging vectors xs, ys
+ * (fixed addresses), with one copy in and one copy out */
+int gen_filter_graphed(GenGraph &g, pevsl_Data *pevsl, const pevsl_Polparams *pol, const double *v,
+                       double *y, double *w, double *xs, double *ys, long n) {
+  if (memcpy_async(xs, v, sizeof(double) * (size_t)n)) return PEVSL_ERR_CUDA;
+  const int st = graph_run(g, pevsl, [&]() { return gen_filter(pevsl, pol, xs, ys, w, n); });
+  if (st) return st;
+  return memcpy_async(y, ys, sizeof(double) * (size_t)n);
+}
+
 }  // namespace
 
 /* ====================================================== generalized solvers */
@@ -298,6 +478,9 @@ int pevsl_gen_kpm_moments(pevsl_Data *pevsl, int Mdeg, const double *jac, double
   double *ddot_ = (double *)ws(WS_MOM, sizeof(double) * (size_t)(Mdeg + 1));
   double *hdot = (double *)malloc(sizeof(double) * (size_t)(Mdeg + 1));
   int st = (!buf || !ddot_ || !hdot) ? PEVSL_ERR_NOMEM : 0;
+  const bool use_graph = graphable(pevsl);
+  if (use_graph) pretune(pevsl);
+  GenGraph kg;
   for (int m = vec_start; m < vec_end && !st; m++) {
     double *v = buf, *vkm1 = buf + n, *vk = buf + 2 * n, *vkp1 = buf + 3 * n, *w = buf + 4 * n;
     double t = 0.0;
@@ -308,19 +491,26 @@ int pevsl_gen_kpm_moments(pevsl_Data *pevsl, int Mdeg, const double *jac, double
     if (!st) st = apply_B(pevsl, w, v);
     if (!st) st = vcopy(w, vk, n);
     if (!st) st = vfill(vkm1, n, 0.0);
-    for (int k = 0; k < Mdeg && !st; k++) {
-      const double sc = (k == 0 ? 1.0 : 2.0) / wid;
-      st = apply_Ag(pevsl, vk, w);
-      if (!st) st = solve_B(pevsl, w, vkp1);
-      if (!st) st = vaxpy(n, -ctr, vk, vkp1);
-      if (!st) st = vscal(vkp1, n, sc);
-      if (!st) st = vaxpy(n, -1.0, vkm1, vkp1);
-      double *tmp = vkm1;
-      vkm1 = vk;
-      vk = vkp1;
-      vkp1 = tmp;
-      if (!st) st = vdot(n, vk, v, ddot_ + k);
-    }
+    /* the degree loop touches only fixed buffers: one graph for every vector */
+    auto degrees = [&]() -> int {
+      double *a = vkm1, *bk = vk, *c = vkp1;
+      int s2 = 0;
+      for (int k = 0; k < Mdeg && !s2; k++) {
+        const double sc = (k == 0 ? 1.0 : 2.0) / wid;
+        s2 = apply_Ag(pevsl, bk, w);
+        if (!s2) s2 = solve_B(pevsl, w, c);
+        if (!s2) s2 = vaxpy(n, -ctr, bk, c);
+        if (!s2) s2 = vscal(c, n, sc);
+        if (!s2) s2 = vaxpy(n, -1.0, a, c);
+        double *tmp = a;
+        a = bk;
+        bk = c;
+        c = tmp;
+        if (!s2) s2 = vdot(n, bk, v, ddot_ + k);
+      }
+      return s2;
+    };
+    if (!st) st = use_graph ? graph_run(kg, pevsl, degrees) : degrees();
     if (!st) st = memcpy_async(hdot, ddot_, sizeof(double) * (size_t)Mdeg);
     if (!st) st = sync();
     if (st) break;
@@ -611,15 +801,25 @@ int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, 
   if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
   double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
   double *Z = (double *)ws(WS_ZBASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
-  double *wf = (double *)ws(WS_GEN, sizeof(double) * 5 * (size_t)ld);
+  double *wf = (double *)ws(WS_GEN, sizeof(double) * 7 * (size_t)ld);
   std::vector<double> dT(maxit + 1), eT(maxit + 1), EvalT(maxit + 1);
   if (!V || !Z || !wf) return PEVSL_ERR_NOMEM;
-  double *vrand = wf + 4 * ld;
+  double *vrand = wf + 4 * ld, *xs = wf + 5 * ld, *ys = wf + 6 * ld;
+  const bool use_graph = graphable(pevsl);
+  if (use_graph) pretune(pevsl);
+  GenGraph fg;
+  auto filter = [&](const double *in, double *out) -> int {
+    g_gen_ev.begin();
+    const int r = use_graph ? gen_filter_graphed(fg, pevsl, pol, in, out, wf, xs, ys, n)
+                            : gen_filter(pevsl, pol, in, out, wf, n);
+    g_gen_ev.end();
+    return r;
+  };
   int st = 0, k = 0, kdim = 0, count = 0, nconv = 0;
   double t = 0.0, tr0 = 0.0, wn = 0.0, beta = 0.0;
   int nwn = 0;
   /* filtered initial vector, unit B-norm */
-  st = gen_filter(pevsl, pol, vinit->data, V, wf, n);
+  st = filter(vinit->data, V);
   if (!st) st = apply_B(pevsl, V, Z);
   if (!st) st = dot_host(n, V, Z, &t);
   if (!st) {
@@ -631,7 +831,7 @@ int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, 
     double *v = V + (size_t)k * ld, *z = Z + (size_t)k * ld;
     double *vnew = v + ld, *znew = z + ld;
     double alpha = 0.0;
-    st = gen_filter(pevsl, pol, z, znew, wf, n);
+    st = filter(z, znew);
     if (!st && k > 0) st = vaxpy(n, -beta, z - ld, znew);
     if (!st) st = dot_host(n, v, znew, &alpha);
     if (st) break;
@@ -648,7 +848,7 @@ int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, 
     if (beta * nwn < orthTol * wn) {
       if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
       st = pevsl_rand_vector_dev(vrand, (int)n);
-      if (!st) st = gen_filter(pevsl, pol, vrand, vnew, wf, n);
+      if (!st) st = filter(vrand, vnew);
       if (!st) st = cgs2(n, ld, k + 1, V, Z, vnew);
       if (!st) st = apply_B(pevsl, vnew, znew);
       if (!st) st = dot_host(n, vnew, znew, &beta);
@@ -899,6 +1099,20 @@ void pEVSL_ChebIterStatsPrint(void *data, FILE *fstats) {
     fprintf(fstats, "   Matvec in ChebIter        :  %f (%8ld, avg %f)\n", C->t_chebmv,
             (long)C->n_chebmv, C->t_chebmv / C->n_chebmv);
   fprintf(fstats, "= = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = = =\n");
+}
+
+void pEVSL_B200_GenCounters(uint64_t *filters, uint64_t *degrees, double *bytes, double *ms) {
+  g_gen_ev.flush();
+  if (filters) *filters = g_gen_filters;
+  if (degrees) *degrees = g_gen_degrees;
+  if (bytes) *bytes = g_gen_bytes;
+  if (ms) *ms = g_gen_ms;
+}
+
+void pEVSL_B200_ResetGenCounters(void) {
+  g_gen_ev.flush();
+  g_gen_filters = g_gen_degrees = 0;
+  g_gen_bytes = g_gen_ms = 0.0;
 }
 
 /* y = p(A B^{-1}) v for the generalized problem (the filter of

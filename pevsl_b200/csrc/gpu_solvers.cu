@@ -86,7 +86,7 @@ double g_filter_ms = 0.0;
  * written) */
 double cheb_step_bytes(const pevsl_devcsr *A, int first) {
   const double n = A->nrows;
-  return 12.0 * (double)A->nnz + 4.0 * (n + 1) + (first ? 24.0 : 40.0) * n;
+  return entry_bytes(A, false) * (double)A->nnz + 4.0 * (n + 1) + (first ? 24.0 : 40.0) * n;
 }
 
 /* matvec through the installed operator: fused kernels use the device CSR
@@ -218,7 +218,7 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     int dmax = 0;
     for (int t = i; t < nlive; t++)
       if (jobs[live[t]].A == A) dmax = PEVSL_MAX(dmax, jobs[live[t]].pol->deg);
-    mat_bytes += (double)dmax * ((fp32 ? 8.0 : 12.0) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
+    mat_bytes += (double)dmax * (entry_bytes(A, fp32) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
   }
   const int form = filter_form();
   if (form == 1) {

@@ -19,6 +19,7 @@
  */
 #include <ctype.h>
 #include <cuda_runtime.h>
+#include <vector>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -240,11 +241,33 @@ struct EpiChebIter2 {
  * a[j] * x[ja[j]] (unfused) into shared memory; each lane adds its rows'
  * products in index order -- the summation order of the reference's row
  * loop (SRC/spmat.c:188-193), so the result matches it to the last bit. */
-template <int R, class T, class Epi, bool NC = true>
-__device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
-                                            const int *__restrict__ ja, const T *__restrict__ a,
-                                            const T *x, const Epi &epi, long rblk,
-                                            T (*prod)[kStreamChunk * R]) {
+/* Entry accessors of stream_rows: the plain CSR arrays, or the packed form
+ * (int16 column offset from the row's 32-row group, uint8 index into a
+ * table of the distinct values held in shared memory).  Both give the same
+ * column and the same double (or float) for every entry. */
+template <class T>
+struct EntriesCSR {
+  const int *__restrict__ ja;
+  const T *__restrict__ a;
+  __device__ __forceinline__ int col(long t, int) const { return __ldg(ja + t); }
+  __device__ __forceinline__ T val(long t) const { return __ldg(a + t); }
+};
+
+template <class T>
+struct EntriesPacked {
+  const short *__restrict__ dj;
+  const unsigned char *__restrict__ vi;
+  const T *vt; /* shared memory */
+  __device__ __forceinline__ int col(long t, int g0) const { return g0 + (int)__ldg(dj + t); }
+  __device__ __forceinline__ T val(long t) const { return vt[__ldg(vi + t)]; }
+};
+
+/* R == 1 for the packed accessor: the column offsets are relative to the
+ * warp's one 32-row group */
+template <int R, class T, class Epi, bool NC, class Ent>
+__device__ __forceinline__ void stream_rows_e(int n, const int *__restrict__ ia, const Ent &ent,
+                                              const T *x, const Epi &epi, long rblk,
+                                              T (*prod)[kStreamChunk * R]) {
   constexpr int CH = kStreamChunk * R, PL = CH / 32;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const long r0l = (rblk * (kThreads / 32) + w) * 32 * R;
@@ -279,8 +302,8 @@ __device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
 #pragma unroll
     for (int q = 0; q < PL; q++) {
       const int t = c0 + q * 32 + lane;
-      col[q] = t < len ? __ldg(ja + base + t) : -1;
-      val[q] = t < len ? __ldg(a + base + t) : T(0);
+      col[q] = t < len ? ent.col(base + t, r0) : -1;
+      val[q] = t < len ? ent.val(base + t) : T(0);
     }
 #pragma unroll
     for (int q = 0; q < PL; q++) {
@@ -301,6 +324,27 @@ __device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
 #pragma unroll
   for (int j = 0; j < R; j++)
     if (lane + 32 * j < nr) epi(r0 + lane + 32 * j, acc[j], pre[j]);
+}
+
+template <int R, class T, class Epi, bool NC = true>
+__device__ __forceinline__ void stream_rows(int n, const int *__restrict__ ia,
+                                            const int *__restrict__ ja, const T *__restrict__ a,
+                                            const T *x, const Epi &epi, long rblk,
+                                            T (*prod)[kStreamChunk * R]) {
+  stream_rows_e<R, T, Epi, NC>(n, ia, EntriesCSR<T>{ja, a}, x, epi, rblk, prod);
+}
+
+/* the packed form: the block stages the value table in shared memory */
+template <class T, class Epi>
+__global__ void __launch_bounds__(kThreads, 5)
+    k_csr_stream_packed(int n, const int *__restrict__ ia, const short *__restrict__ dj,
+                        const unsigned char *__restrict__ vi, const T *__restrict__ vtab, int nv,
+                        const T *__restrict__ x, Epi epi) {
+  __shared__ T prod[kThreads / 32][kStreamChunk];
+  __shared__ T vt[256];
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
+  __syncthreads();
+  stream_rows_e<1, T, Epi, true>(n, ia, EntriesPacked<T>{dj, vi, vt}, x, epi, blockIdx.x, prod);
 }
 
 /* R = 1 fits 48 registers (5 blocks per SM) without spilling */
@@ -353,6 +397,21 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
     stream_rows<R>(b.n[lo], b.ia[lo], b.ja[lo], b.a[lo], (const T *)b.epi[lo].vk, b.epi[lo],
                    (long)blockIdx.x - b.off[lo], prod);
   }
+}
+
+/* the shared-matrix batch on the packed form */
+template <class T, class Epi, int CAP>
+__global__ void __launch_bounds__(kThreads, 4)
+    k_csr_stream_batch_packed(int n0, const int *__restrict__ ia0, const short *__restrict__ dj,
+                              const unsigned char *__restrict__ vi, const T *__restrict__ vtab,
+                              int nv, const __grid_constant__ StreamBatch<T, Epi, CAP> b) {
+  __shared__ T prod[kThreads / 32][kStreamChunk];
+  __shared__ T vt[256];
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
+  __syncthreads();
+  const int e = (int)(blockIdx.x % (unsigned)b.nb);
+  stream_rows_e<1, T, Epi, true>(n0, ia0, EntriesPacked<T>{dj, vi, vt}, (const T *)b.epi[e].vk,
+                                 b.epi[e], (long)(blockIdx.x / (unsigned)b.nb), prod);
 }
 
 /* ---------------------------------------------------------------- persistent filter */
@@ -761,8 +820,31 @@ int stream_tune(pevsl_devcsr *A) {
 
 /* one CSR-stream launch with the matrix's rows per lane (tuned on first use
  * when the stream is not being captured) */
+static bool use_packed(const pevsl_devcsr *A) {
+  static int on = -1;
+  if (on < 0) {
+    const char *e = getenv("PEVSL_B200_PACKED");
+    on = e ? atoi(e) != 0 : 0;
+  }
+  return on && A->pdj != nullptr;
+}
+
+double entry_bytes(const pevsl_devcsr *A, bool fp32) {
+  return use_packed(A) ? 3.0 : (fp32 ? 8.0 : 12.0);
+}
+
+template <class T>
+static const T *packed_table(const pevsl_devcsr *A) {
+  return sizeof(T) == 4 ? (const T *)(const void *)A->pvtab32 : (const T *)(const void *)A->pvtab;
+}
+
 template <class T, class Epi>
 static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const Epi &epi) {
+  if (use_packed(A)) {
+    k_csr_stream_packed<T, Epi><<<stream_grid(A->nrows, 1), kThreads, 0, ctx().stream>>>(
+        A->nrows, A->ia, A->pdj, A->pvi, packed_table<T>(A), A->pnv, x, epi);
+    return;
+  }
   if (!A->stream_r) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(ctx().stream, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone)
@@ -805,7 +887,14 @@ static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const cha
   const int n0 = b.n[0];
   const int *ia0 = b.ia[0], *ja0 = b.ja[0];
   const T *a0 = b.a[0];
-  if (b.shared) {
+  if (b.shared && use_packed(en[0].A)) {
+    /* packed rows are grouped by 32 (one row group per warp) */
+    const pevsl_devcsr *A = en[0].A;
+    const long rb = (n0 + kThreads - 1) / kThreads;
+    const unsigned gp = (unsigned)(rb * nb);
+    k_csr_stream_batch_packed<T, Epi, CAP><<<gp, kThreads, 0, ctx().stream>>>(
+        n0, ia0, A->pdj, A->pvi, packed_table<T>(A), A->pnv, b);
+  } else if (b.shared) {
     if (R == 2)
       k_csr_stream_batch<2, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
     else
@@ -1019,6 +1108,65 @@ int pEVSL_ParcsrCreate(int nrow, int ncol, int *row_starts, int *col_starts, pev
 
 /* Upload the caller's host CSR (the local rows, global column indices) as
  * one device CSR (SRC/parcsr.c:70-283 without the split and halo plan). */
+/* The packed copy of a matrix's entries, when every column lies within
+ * int16 range of its row's 32-row group start and the matrix has at most
+ * 256 distinct values (compared bit for bit, so each entry decodes to the
+ * exact double it was): 3 bytes per entry instead of 12.  Stencil and
+ * finite-element matrices with few coefficients qualify; the filter and SpMV
+ * kernels then read a quarter of the bytes for the matrix, and the result is
+ * bit-identical.  Returns 0 also when the matrix does not qualify. */
+static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
+  const int nr = d->nrows;
+  const long long nnz = d->nnz;
+  if (nnz <= 0) return 0;
+  std::vector<short> dj((size_t)nnz);
+  std::vector<unsigned char> vi((size_t)nnz);
+  std::vector<double> tab;
+  tab.reserve(256);
+  /* value bits -> table index: open addressing in 1024 slots */
+  constexpr int kSlots = 1024;
+  std::vector<uint64_t> hkey(kSlots);
+  std::vector<int> hval(kSlots, -1);
+  for (int i = 0; i < nr; i++) {
+    const long g0 = (long)(i & ~31);
+    for (int k = Ai->ia[i]; k < Ai->ia[i + 1]; k++) {
+      const long off = (long)Ai->ja[k] - g0;
+      if (off < -32768 || off > 32767) return 0;
+      dj[(size_t)k] = (short)off;
+      uint64_t key;
+      memcpy(&key, &Ai->a[k], sizeof key);
+      unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 54) & (kSlots - 1);
+      while (hval[h] >= 0 && hkey[h] != key) h = (h + 1) & (kSlots - 1);
+      if (hval[h] < 0) {
+        if (tab.size() == 256) return 0;
+        hkey[h] = key;
+        hval[h] = (int)tab.size();
+        tab.push_back(Ai->a[k]);
+      }
+      vi[(size_t)k] = (unsigned char)hval[h];
+    }
+  }
+  const size_t b_dj = ((sizeof(short) * (size_t)nnz + 255) / 256) * 256;
+  const size_t b_vi = ((size_t)nnz + 255) / 256 * 256;
+  const size_t b_tab = 256 * sizeof(double) + 256 * sizeof(float);
+  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab);
+  if (!base) return PEVSL_ERR_NOMEM;
+  std::vector<float> tab32(tab.size());
+  for (size_t t = 0; t < tab.size(); t++) tab32[t] = (float)tab[t];
+  d->pdj = (short *)base;
+  d->pvi = (unsigned char *)(base + b_dj);
+  d->pvtab = (double *)(base + b_dj + b_vi);
+  d->pvtab32 = (float *)(base + b_dj + b_vi + 256 * sizeof(double));
+  d->pnv = (int)tab.size();
+  d->pbytes = b_dj + b_vi + b_tab;
+  int st = memcpy_async(d->pdj, dj.data(), sizeof(short) * (size_t)nnz);
+  if (!st) st = memcpy_async(d->pvi, vi.data(), (size_t)nnz);
+  if (!st) st = memcpy_async(d->pvtab, tab.data(), sizeof(double) * tab.size());
+  if (!st) st = memcpy_async(d->pvtab32, tab32.data(), sizeof(float) * tab.size());
+  if (!st) st = sync();
+  return st;
+}
+
 int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
   if (ensure()) return PEVSL_ERR_CUDA;
   const int nr = A->nrow_local;
@@ -1062,6 +1210,8 @@ int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
   if (!st) st = memcpy_async(d->a, Ai->a, sizeof(double) * (size_t)nnz);
   if (!st) st = sync();
   if (st) return st;
+  st = pack_entries(d, Ai);
+  if (st) return st;
   A->comm_handle = (commHandle *)d;
   A->diag = (pevsl_Csr *)calloc(1, sizeof(pevsl_Csr));
   A->offd = (pevsl_Csr *)calloc(1, sizeof(pevsl_Csr));
@@ -1081,6 +1231,7 @@ void pEVSL_ParcsrFree(pevsl_Parcsr *A) {
     cudaStreamSynchronize(ctx().stream);
     cudaFree(d->a); /* the whole [values | indices | pointers] block */
     if (d->a32) cudaFree(d->a32);
+    if (d->pdj) cudaFree(d->pdj); /* the packed block */
     d->magic = 0;
     free(d);
   }

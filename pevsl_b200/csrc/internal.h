@@ -50,6 +50,16 @@ typedef struct pevsl_devcsr {
   int lanes; /* threads per row in the row-group SpMV kernels */
   int stream_r; /* rows per lane of the CSR-stream kernels, 0 until tuned */
   size_t bytes; /* size of the one device block holding a, ja, ia */
+  /* packed copy of the entries (NULL when the matrix does not qualify):
+   * pdj = column - 32 * (row / 32) as int16, pvi = index of the value in
+   * pvtab (at most 256 distinct values, exact doubles; pvtab32 their FP32
+   * roundings), all in one device block of pbytes bytes */
+  short *pdj;
+  unsigned char *pvi;
+  double *pvtab;
+  float *pvtab32;
+  int pnv;
+  size_t pbytes;
 } pevsl_devcsr;
 
 /* The device matrix behind a Parcsr, or NULL if it was never set up here. */
