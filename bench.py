@@ -667,6 +667,9 @@ def kernel_case(args):
                  lockstep, 3 Lanczos steps (32 batched filter-degree
                  launches);
       kpm_step   8 KPM degrees for 16 vectors;
+      gen_filter two degree-8 generalized filter applications on the
+                 genlap24 problem scaled to --grid (B-solve: least-squares
+                 1/x of degree 24, 25 launches per degree);
       pipeline   one whole batched solve of --workload (for launch lists)."""
     import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian
@@ -682,6 +685,21 @@ def kernel_case(args):
     n, ia, ja, a = laplacian(g, g, g)
     M = pv.Matrix.from_csr(n, ia, ja, a)
     pv.set_rng(pv.RNG_GAUSS, 0)
+    if args.kernel_case == "gen_filter":
+        gs = GenSetup(WORKLOADS["genlap24"], n)
+        r, f = pv.findpol([1.0, 1.0094, 0.02, 4.1], deg_in=8)
+        v = np.cos(np.arange(n) * 0.1)
+        with pv.Instance(M) as ev:
+            gs.install(ev)
+            pol, keep = pv._polparams(f)
+            vv, yv = pv.Vector(n, v), pv.Vector(n)
+            for _ in range(2):
+                st = ev.lib.pEVSL_B200_ChebAvGen(ev.p, C.byref(pol), vv.pv.data, yv.pv.data)
+            vv.free()
+            yv.free()
+        gs.free()
+        print(json.dumps({"kernel_case": "gen_filter", "n": n, "status": st}))
+        return
     with pv.Instance(M) as ev:
         if args.kernel_case == "cheb_step":
             r, f = pv.findpol([0.80, 0.82, 0.0, 12.0], deg_in=8)
@@ -710,7 +728,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--path", default="batched", choices=["batched", "plain"],
                     help="batched: slices in lockstep; plain: one pEVSL_ChebLanNr per slice")
-    ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "pipeline"],
+    ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "gen_filter",
+                                              "pipeline"],
                     help="run a few launches of one kernel (for ncu) and exit")
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--batch", type=int, default=4)

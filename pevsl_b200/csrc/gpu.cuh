@@ -227,7 +227,7 @@ int cheb_step_batch(int nb, const ChebEntry *e, bool fp32);
 /* bytes per stored entry that the CSR-stream kernels read for A: 3 for the
  * packed form (int16 column offset + uint8 value index), else 12 (int32
  * column + FP64 value) or 8 (FP32 value) */
-double entry_bytes(const pevsl_devcsr *A, bool fp32);
+double entry_bytes(const pevsl_devcsr *A, bool fp32, bool batch = false);
 /* choose the CSR-stream rows per lane of a matrix by timing (once) */
 int stream_tune(pevsl_devcsr *A);
 

@@ -218,7 +218,7 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     int dmax = 0;
     for (int t = i; t < nlive; t++)
       if (jobs[live[t]].A == A) dmax = PEVSL_MAX(dmax, jobs[live[t]].pol->deg);
-    mat_bytes += (double)dmax * (entry_bytes(A, fp32) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
+    mat_bytes += (double)dmax * (entry_bytes(A, fp32, true) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
   }
   const int form = filter_form();
   if (form == 1) {

@@ -820,17 +820,29 @@ int stream_tune(pevsl_devcsr *A) {
 
 /* one CSR-stream launch with the matrix's rows per lane (tuned on first use
  * when the stream is not being captured) */
-static bool use_packed(const pevsl_devcsr *A) {
+/* Which kernels read the packed entries (PEVSL_B200_PACKED): 0 none, 1 the
+ * one-vector kernels (default), 2 also the shared-matrix batch.  Measured
+ * per filter degree at 100^3: one vector 22.3 vs 28.1 us, but 4 slices
+ * 89.5 vs 79.9 us, and at 160^3 one vector 98.1 vs 99.4 us -- the kernels
+ * are bound by the gathers and the vector streams more than by the matrix
+ * bytes, so the packed form pays only where the working set nears L2. */
+static int packed_mode() {
   static int on = -1;
   if (on < 0) {
     const char *e = getenv("PEVSL_B200_PACKED");
-    on = e ? atoi(e) != 0 : 0;
+    on = e ? atoi(e) : 1;
+    if (on < 0 || on > 2) on = 1;
   }
-  return on && A->pdj != nullptr;
+  return on;
 }
 
-double entry_bytes(const pevsl_devcsr *A, bool fp32) {
-  return use_packed(A) ? 3.0 : (fp32 ? 8.0 : 12.0);
+static bool use_packed(const pevsl_devcsr *A) { return packed_mode() >= 1 && A->pdj != nullptr; }
+static bool use_packed_batch(const pevsl_devcsr *A) {
+  return packed_mode() == 2 && A->pdj != nullptr;
+}
+
+double entry_bytes(const pevsl_devcsr *A, bool fp32, bool batch) {
+  return (batch ? use_packed_batch(A) : use_packed(A)) ? 3.0 : (fp32 ? 8.0 : 12.0);
 }
 
 template <class T>
@@ -887,7 +899,7 @@ static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const cha
   const int n0 = b.n[0];
   const int *ia0 = b.ia[0], *ja0 = b.ja[0];
   const T *a0 = b.a[0];
-  if (b.shared && use_packed(en[0].A)) {
+  if (b.shared && use_packed_batch(en[0].A)) {
     /* packed rows are grouped by 32 (one row group per warp) */
     const pevsl_devcsr *A = en[0].A;
     const long rb = (n0 + kThreads - 1) / kThreads;
