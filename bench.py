@@ -413,17 +413,20 @@ def run_b200(args, dist):
         try:
             r, fil = pv.findpol([r0.sli[0], r0.sli[1], r0.lmin, r0.lmax], 3000, 2, 0.8, 0.2)
             per, d = cpu_reference_sample(n, ia, ja, a, fil)
-            # whole-run CPU time: every filter degree and every KPM / bounds
-            # SpMV at the measured per-degree cost (reorthogonalisation, ~1-2%
-            # of the reference's time on this workload, not counted)
+            # whole-run CPU time: every slice's filter degrees (degree x
+            # (Lanczos steps + 1), the reference's pEVSL_ChebAv calls) and every
+            # KPM / bounds SpMV at the measured per-degree cost
+            # (reorthogonalisation, ~1-2% of the reference's time on this
+            # workload, not counted)
             kpm = w["Mdeg"] * w["nvec"]
-            cpu_t = per * (f_launch / args.steps + kpm + 200)
+            slice_degs = sum(dg * (it + 1) for dg, it in zip(r0.deg, r0.its))
+            cpu_t = per * (slice_degs + kpm + 200)
             out["cpu_baseline"] = {
                 "value": sum(r0.nev) / cpu_t, "unit": "eigenpairs/s", "cores": 1,
                 "kind": "reference",
                 "sample": f"reference pEVSL_ChebAv (oracle/_ref, OpenBLAS 1 thread) of degree {d} "
                           f"with slice 0's filter on this matrix: {per*1e3:.2f} ms per degree; "
-                          f"extrapolated to the run's {int(f_launch/args.steps)} filter degrees + "
+                          f"extrapolated to the run's {slice_degs} slice filter degrees + "
                           f"{kpm} KPM + <=200 bounds matvecs"}
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
@@ -661,15 +664,17 @@ REF_COUNTS = {
 def kernel_case(args):
     """A few launches of one kernel on a matrix larger than L2, for ncu, on
     the 3D Laplacian of side --grid:
-      cheb_step  two degree-8 filter applications (16 fused filter-degree
+      cheb_step  two degree-16 filter applications (32 fused filter-degree
                  launches, one vector);
-      cheb_batch --batch slices of [0.80, 0.82] with degree-8 filters in
-                 lockstep, 3 Lanczos steps (32 batched filter-degree
+      cheb_batch --batch slices of [0.8, 4.0] with degree-16 filters in
+                 lockstep, 3 Lanczos steps (64 batched filter-degree
                  launches);
       kpm_step   8 KPM degrees for 16 vectors;
-      gen_filter two degree-8 generalized filter applications on the
+      gen_filter two degree-16 generalized filter applications on the
                  genlap24 problem scaled to --grid (B-solve: least-squares
                  1/x of degree 24, 25 launches per degree);
+    (the filters are forced to a small degree on wide intervals: a forced
+    degree below a slice's starting degree is an error)
       pipeline   one whole batched solve of --workload (for launch lists)."""
     import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian
@@ -687,7 +692,7 @@ def kernel_case(args):
     pv.set_rng(pv.RNG_GAUSS, 0)
     if args.kernel_case == "gen_filter":
         gs = GenSetup(WORKLOADS["genlap24"], n)
-        r, f = pv.findpol([1.0, 1.0094, 0.02, 4.1], deg_in=8)
+        r, f = pv.findpol([0.5, 2.0, 0.02, 4.1], deg_in=16)
         v = np.cos(np.arange(n) * 0.1)
         with pv.Instance(M) as ev:
             gs.install(ev)
@@ -702,15 +707,15 @@ def kernel_case(args):
         return
     with pv.Instance(M) as ev:
         if args.kernel_case == "cheb_step":
-            r, f = pv.findpol([0.80, 0.82, 0.0, 12.0], deg_in=8)
+            r, f = pv.findpol([0.8, 4.0, 0.0, 12.0], deg_in=16)
             v = np.cos(np.arange(n) * 0.1)
             for _ in range(2):
                 ev.chebav(f, v)
         elif args.kernel_case == "cheb_batch":
             S = args.batch
-            edges = np.linspace(0.80, 0.82, S + 1)
+            edges = np.linspace(0.8, 4.0, S + 1)
             intvs = [[edges[i], edges[i + 1], 0.0, 12.0] for i in range(S)]
-            fl = [pv.findpol(iv, deg_in=8)[1] for iv in intvs]
+            fl = [pv.findpol(iv, deg_in=16)[1] for iv in intvs]
             v = np.cos(np.arange(n) * 0.1)
             pv.cheblannr_batch(ev, intvs, [3] * S, 1e-8, v, fl)
         else:

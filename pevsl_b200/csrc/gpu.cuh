@@ -228,6 +228,8 @@ int cheb_step_batch(int nb, const ChebEntry *e, bool fp32);
  * packed form (int16 column offset + uint8 value index), else 12 (int32
  * column + FP64 value) or 8 (FP32 value) */
 double entry_bytes(const pevsl_devcsr *A, bool fp32, bool batch = false);
+/* L2 persistence window over the part of A the kernels read (if enabled) */
+void matrix_window(const pevsl_devcsr *A);
 /* choose the CSR-stream rows per lane of a matrix by timing (once) */
 int stream_tune(pevsl_devcsr *A);
 

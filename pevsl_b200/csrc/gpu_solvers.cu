@@ -218,7 +218,7 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     int dmax = 0;
     for (int t = i; t < nlive; t++)
       if (jobs[live[t]].A == A) dmax = PEVSL_MAX(dmax, jobs[live[t]].pol->deg);
-    mat_bytes += (double)dmax * (entry_bytes(A, fp32, true) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
+    mat_bytes += (double)dmax * ((fp32 ? 8.0 : 12.0) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
   }
   const int form = filter_form();
   if (form == 1) {
@@ -294,7 +294,6 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     }
     vkm1[i] = nullptr;
   }
-  g_filter_bytes += mat_bytes;
   std::vector<ChebEntry> en(nlive);
   for (int k = 1; k <= maxdeg && !st; k++) {
     int nb = 0;
@@ -313,7 +312,23 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
       vkm1[i] = vk[i];
       vk[i] = vkp1;
     }
-    st = cheb_step_batch(nb, en.data(), fp32);
+    /* matrix bytes: each distinct matrix of this degree's entries once */
+    for (int i = 0; i < nb; i++) {
+      bool seen = false;
+      for (int t = 0; t < i && !seen; t++) seen = en[t].A == en[i].A;
+      if (!seen)
+        bytes += entry_bytes(en[i].A, fp32, nb > 1) * (double)en[i].A->nnz +
+                 4.0 * (en[i].A->nrows + 1.0);
+    }
+    if (nb == 1 && !fp32 && en[0].A->lanes == 0) {
+      /* one live slice: the one-vector kernel (packed entries when the
+       * matrix has them); the same arithmetic as the batch */
+      const ChebEntry &c = en[0];
+      st = cheb_step(c.A, (const double *)c.vk, (const double *)c.vkm1, (double *)c.vkp1,
+                     (double *)c.y, c.cc, c.t, c.mu0, c.muk, c.first);
+    } else {
+      st = cheb_step_batch(nb, en.data(), fp32);
+    }
     g_filter_launches++;
     g_filter_bytes += bytes;
   }
@@ -435,7 +450,7 @@ void pEVSL_B200_ResetFilterCounters(void) {
  * ChebAv internal. */
 int pEVSL_B200_ChebAv(pevsl_Data *pevsl, pevsl_Polparams *pol, const double *v, double *y) {
   if (ensure()) return PEVSL_ERR_CUDA;
-  if (pevsl_builtin_A(pevsl)) l2_window(pevsl_builtin_A(pevsl)->a, pevsl_builtin_A(pevsl)->bytes);
+  matrix_window(pevsl_builtin_A(pevsl));
   const long n = pevsl->n;
   double *w3 = (double *)ws(WS_CHEB, sizeof(double) * 3 * (size_t)n);
   if (!w3) return PEVSL_ERR_NOMEM;
@@ -1295,7 +1310,9 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
     all_builtin = all_builtin && SL[s].A != nullptr;
     nmax = PEVSL_MAX(nmax, SL[s].n);
   }
-  const bool batched = all_builtin && (ns > 1 || mixed);
+  /* the lockstep machinery also serves one slice when the filter is
+   * graph-replayed (one captured launch sequence per filter application) */
+  const bool batched = all_builtin && (ns > 1 || mixed || filter_graph_enabled());
   /* mixed form: trace tolerance per converged value, and the guard of the
    * refinement sweep (PEVSL_B200_MIXED_TRTOL / PEVSL_B200_MIXED_GUARD) */
   double trtol_mixed = 1e-9, guard = 0.3;
@@ -1438,7 +1455,7 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
   double *dW = (double *)ws(WS_GROUP, sizeof(double) * (size_t)ns * (size_t)ldw);
   if (!dW) return PEVSL_ERR_NOMEM;
   for (int s = 0; s < ns; s++)
-    if (act[s] && SL[s].A) l2_window(SL[s].A->a, SL[s].A->bytes);
+    if (act[s] && SL[s].A) matrix_window(SL[s].A);
   cudaEvent_t e_all0, e_all1;
   cudaEventCreate(&e_all0);
   cudaEventCreate(&e_all1);
