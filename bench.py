@@ -389,7 +389,8 @@ def run_b200(args, dist):
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
             "bytes_per_launch": per_launch_bytes, "launches": f_launch,
-            "avg_launch_us": per_launch_ms * 1e3, "traffic": ncu_traffic(args.workload)},
+            "avg_launch_us": per_launch_ms * 1e3,
+            "traffic": ncu_traffic(args.workload) if batched and not gen else None},
         "e2e": {"value": e2e_val, "unit": "eigenpairs/s",
                 "h2d_bytes_per_step": int(4 * (n + 1) + 12 * nnz +
                                           (4 * (n + 1) + 12 * (3 * n - 2) if gen else 0)),
