@@ -674,11 +674,47 @@ def kernel_case(args):
       gen_filter two degree-16 generalized filter applications on the
                  genlap24 problem scaled to --grid (B-solve: least-squares
                  1/x of degree 24, 25 launches per degree);
+      c4_filter  the C4 matrix (random symmetric, n = 2e6, ~17 entries per
+                 row, offsets within +-5000; seed 1): 3 Lanczos steps with
+                 a degree-16 filter on one slice, then on 16 interior slices
+                 in lockstep; prints the filter's live timing (CUDA events)
+                 and HBM fraction per degree;
     (the filters are forced to a small degree on wide intervals: a forced
     degree below a slice's starting degree is an error)
       pipeline   one whole batched solve of --workload (for launch lists)."""
     import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian
+    if args.kernel_case == "c4_filter":
+        from pevsl_b200.problems import random_sparse_symmetric
+        n, ia, ja, a = random_sparse_symmetric(2000000, 16, 5000, 1)
+        # Gershgorin enclosure of the spectrum
+        rows = np.repeat(np.arange(n), np.diff(ia))
+        diag = np.zeros(n)
+        np.add.at(diag, rows[ja == rows], a[ja == rows])
+        rad = np.bincount(rows, weights=np.abs(a), minlength=n) - np.abs(diag)
+        lmin, lmax = float(np.min(diag - rad)), float(np.max(diag + rad))
+        M = pv.Matrix.from_csr(n, ia, ja, a)
+        wdt = lmax - lmin
+        edges = np.linspace(lmin + 0.1 * wdt, lmax - 0.1 * wdt, 17)
+        intvs = [[edges[i], edges[i + 1], lmin, lmax] for i in range(16)]
+        fl = [pv.findpol(iv, deg_in=16)[1] for iv in intvs]
+        v = np.cos(np.arange(n) * 0.1)
+        peak, kind = measured_peak()
+        out = {"kernel_case": "c4_filter", "n": n, "nnz": int(ia[-1]), "bounds": [lmin, lmax]}
+        with pv.Instance(M) as ev:
+            for label, k in (("one_slice", 1), ("16_slices", 16)):
+                pv.load().pEVSL_B200_ResetFilterCounters()
+                if k == 1:
+                    ev.cheblannr(intvs[0], 3, 1e-8, v, fl[0])
+                else:
+                    pv.cheblannr_batch(ev, intvs, [3] * 16, 1e-8, v, fl)
+                l, b, ms = pv.filter_counters()
+                out[label] = {"launches": l, "us_per_launch": 1e3 * ms / l,
+                              "bytes_per_launch": b / l, "GBps": b / ms / 1e6,
+                              "frac": b / ms / 1e6 / peak, "peak": peak, "peak_source": kind}
+        M.free()
+        print(json.dumps(out))
+        return
     if args.kernel_case == "pipeline":
         w = WORKLOADS[args.workload]
         n, ia, ja, a = laplacian(*w["grid"])
@@ -735,7 +771,7 @@ def main():
     ap.add_argument("--path", default="batched", choices=["batched", "plain"],
                     help="batched: slices in lockstep; plain: one pEVSL_ChebLanNr per slice")
     ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "gen_filter",
-                                              "pipeline"],
+                                              "c4_filter", "pipeline"],
                     help="run a few launches of one kernel (for ncu) and exit")
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--batch", type=int, default=4)

@@ -73,6 +73,8 @@ enum Ws {
   WS_GROUP,     /* per-entry coefficient vectors of a group   */
   WS_ZBASIS,    /* generalized problem: Z = B V               */
   WS_GEN,       /* generalized problem: filter / KPM vectors  */
+  WS_IL,        /* interleaved filter: three n x S blocks     */
+  WS_ILMU,      /* interleaved filter: per-degree coefficients */
   WS_COUNT
 };
 
@@ -224,6 +226,15 @@ struct ChebEntry {
   int first;
 };
 int cheb_step_batch(int nb, const ChebEntry *e, bool fp32);
+/* the same degree for S in {2,4,8,16} vectors of one problem held
+ * row-interleaved (X[i*S + s]); mu0[s], muk[s] on the device; Xkp1 may
+ * alias Xkm1 */
+int cheb_step_il(const pevsl_devcsr *A, int S, const double *Xk, const double *Xkm1, double *Xkp1,
+                 double *Y, double cc, double t, const double *mu0, const double *muk, int first);
+/* X[i*S + s] = xs[s][i] (S <= kMaxBatch), and ys[s][i] = X[i*S + s] for
+ * the first cols columns */
+int il_pack(long n, int S, const double *const *xs, double *X);
+int il_unpack(long n, int S, int cols, const double *X, double *const *ys);
 /* bytes per stored entry that the CSR-stream kernels read for A: 3 for the
  * packed form (int16 column offset + uint8 value index), else 12 (int32
  * column + FP64 value) or 8 (FP32 value) */

@@ -992,6 +992,107 @@ int chebiter2_step(const pevsl_devcsr *B, const double *d, double *x, double *r,
   return launched("chebiter2_combine");
 }
 
+/* ---------------------------------------------------------------- interleaved
+ * One filter degree for S (2..16) vectors of one problem held row-interleaved
+ * (X[i*S + s]): S lanes serve one row, lane s its vector s.  For each entry
+ * the S lanes read x[col*S .. col*S+S-1] -- one contiguous segment -- so a
+ * scattered column costs one L1/L2 access for all S vectors instead of one
+ * per vector.  Lane s adds its row's products in entry order and applies
+ * the recurrence of its own column (cheb_update_v with its own mu), which is
+ * the arithmetic of the one-vector kernel, bit for bit.  X_{k+1} may alias
+ * X_{k-1} (each lane reads its own element first). */
+template <int S>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb_il(int n, const int *__restrict__ ia, const int *__restrict__ ja,
+              const double *__restrict__ a, const double *__restrict__ Xk, const double *Xkm1,
+              double *Xkp1, double *Y, double cc, double t, const double *__restrict__ mu0,
+              const double *__restrict__ muk, int first) {
+  constexpr int RPW = 32 / S; /* rows per warp */
+  const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, s = lane % S;
+  const long row = gw * RPW + lane / S;
+  if (row >= n) return;
+  const size_t me = (size_t)row * S + s;
+  const double x = Xk[me];
+  const double xm1 = Xkm1 ? Xkm1[me] : 0.0;
+  const double yold = first ? 0.0 : Y[me];
+  const int e = __ldg(ia + row + 1);
+  double r = 0.0;
+  int j = __ldg(ia + row);
+  for (; j + 3 < e; j += 4) {
+    const int c0 = __ldg(ja + j), c1 = __ldg(ja + j + 1), c2 = __ldg(ja + j + 2), c3 = __ldg(ja + j + 3);
+    const double a0 = __ldg(a + j), a1 = __ldg(a + j + 1), a2 = __ldg(a + j + 2), a3 = __ldg(a + j + 3);
+    const double x0 = __ldg(Xk + (size_t)c0 * S + s), x1 = __ldg(Xk + (size_t)c1 * S + s);
+    const double x2 = __ldg(Xk + (size_t)c2 * S + s), x3 = __ldg(Xk + (size_t)c3 * S + s);
+    r = __dadd_rn(r, __dmul_rn(a0, x0));
+    r = __dadd_rn(r, __dmul_rn(a1, x1));
+    r = __dadd_rn(r, __dmul_rn(a2, x2));
+    r = __dadd_rn(r, __dmul_rn(a3, x3));
+  }
+  for (; j < e; j++) r = __dadd_rn(r, __dmul_rn(__ldg(a + j), __ldg(Xk + (size_t)__ldg(ja + j) * S + s)));
+  double w, yv;
+  cheb_update_v(r, x, xm1, Xkm1 != nullptr, cc, t, mu0[s], muk[s], first, yold, &w, &yv);
+  Xkp1[me] = w;
+  Y[me] = yv;
+}
+
+/* X[i*S + s] = x_s[i] and back */
+__global__ void k_il_pack(long n, int S, CPtrs xs, double *X) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n * S;
+       i += (long)gridDim.x * blockDim.x)
+    X[i] = xs.p[i % S][i / S];
+}
+
+__global__ void k_il_unpack(long n, int S, int cols, const double *X, VPtrs ys) {
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n * S;
+       i += (long)gridDim.x * blockDim.x)
+    if ((int)(i % S) < cols) ys.p[i % S][i / S] = X[i];
+}
+
+int il_pack(long n, int S, const double *const *xs, double *X) {
+  if (S < 1 || S > kMaxBatch) return PEVSL_ERR_ARG;
+  CPtrs p{};
+  for (int s = 0; s < S; s++) p.p[s] = xs[s];
+  k_il_pack<<<grid_for(n * S, 4), kThreads, 0, ctx().stream>>>(n, S, p, X);
+  return launched("il_pack");
+}
+
+int il_unpack(long n, int S, int cols, const double *X, double *const *ys) {
+  if (S < 1 || S > kMaxBatch || cols < 1 || cols > S) return PEVSL_ERR_ARG;
+  VPtrs p{};
+  for (int s = 0; s < cols; s++) p.p[s] = ys[s];
+  k_il_unpack<<<grid_for(n * S, 4), kThreads, 0, ctx().stream>>>(n, S, cols, X, p);
+  return launched("il_unpack");
+}
+
+/* S is padded up to 2, 4, 8 or 16 by the caller (unused columns are zero) */
+int cheb_step_il(const pevsl_devcsr *A, int S, const double *Xk, const double *Xkm1, double *Xkp1,
+                 double *Y, double cc, double t, const double *mu0, const double *muk, int first) {
+  const long rows_per_block = (kThreads / 32) * (32 / S);
+  const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
+  switch (S) {
+    case 2:
+      k_cheb_il<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1, Xkp1,
+                                                     Y, cc, t, mu0, muk, first);
+      break;
+    case 4:
+      k_cheb_il<4><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1, Xkp1,
+                                                     Y, cc, t, mu0, muk, first);
+      break;
+    case 8:
+      k_cheb_il<8><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1, Xkp1,
+                                                     Y, cc, t, mu0, muk, first);
+      break;
+    case 16:
+      k_cheb_il<16><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1,
+                                                      Xkp1, Y, cc, t, mu0, muk, first);
+      break;
+    default:
+      return PEVSL_ERR_ARG;
+  }
+  return launched("cheb_step_il");
+}
+
 int cheb_step_batch(int nb, const ChebEntry *e, bool fp32) {
   if (nb <= 0) return 0;
   if (nb > kMaxEntries) return PEVSL_ERR_ARG;

@@ -149,15 +149,16 @@ def random_coef_laplacian(nx: int, ny: int, nz: int, seed: int, lo: float = 0.5,
 def random_sparse_symmetric(n: int, per_row: int, bandwidth: int, seed: int):
     """Symmetric sparse matrix of the general-sparse family: per_row/2
     off-diagonal entries drawn per row at column offsets uniform in
-    [1, bandwidth] (either side, clipped to the matrix), values N(0,1),
-    symmetrised as (B + B^T), duplicates summed, plus the diagonal
-    4 + U[0, 1].  About per_row nonzeros per row.  Returns (n, ia, ja, a)."""
+    [1, bandwidth] (either side; draws that fall outside the matrix are
+    dropped, so no row collects the overflow), values N(0,1), symmetrised
+    as (B + B^T), duplicates summed, plus the diagonal 4 + U[0, 1].  About
+    per_row nonzeros per row.  Returns (n, ia, ja, a)."""
     rng = np.random.default_rng(seed)
     h = max(1, per_row // 2)
     i = np.repeat(np.arange(n), h)
     off = rng.integers(1, bandwidth + 1, size=i.size) * np.where(rng.random(i.size) < 0.5, -1, 1)
-    j = np.clip(i + off, 0, n - 1)
-    keep = j != i
+    j = i + off
+    keep = (j >= 0) & (j < n)
     i, j = i[keep], j[keep]
     v = rng.standard_normal(i.size)
     # sum duplicates on the upper triangle, then mirror: exactly symmetric
