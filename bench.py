@@ -384,8 +384,10 @@ def run_b200(args, dist):
             "kernel": ("generalized filter degree (B-solve: fused Chebyshev degrees on B; A step "
                        "fused with the recurrence), CUDA-graph replays; one launch = one degree"
                        if gen else
-                       "cheb_step_batch (fused SpMV + Chebyshev recurrence, CSR-stream, all slices per launch)"
-                       if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream)"),
+                       "cheb_step_il (fused SpMV + Chebyshev recurrence, all slices per launch with "
+                       "row-interleaved vectors; one live slice: the packed one-vector kernel)"
+                       if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream, "
+                       "packed entries)"),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
             "bytes_per_launch": per_launch_bytes, "launches": f_launch,

@@ -179,7 +179,8 @@ static int filter_form() { return filter_form_setting() == 1 ? 1 : 0; }
  * their vectors row-interleaved, so one gather serves every slice
  * (cheb_step_il); the input is packed once and the result unpacked once per
  * filter application.  Applies to 2..16 FP64 slices on a short-row matrix
- * whose polynomials share the spectrum bounds (cc, dd).  Measured per
+ * of at least 2^16 rows whose polynomials share the spectrum bounds
+ * (cc, dd).  Measured per
  * degree against the grid-interleaved batch kernel: 100^3, 4 slices 52.6
  * vs 80.1 us (2 slices 34.0 vs 44.6, 16 slices 182 vs 310); random sparse
  * n = 2e6 with ~17 entries per row, 16 slices 758 vs 2160 us. */
@@ -205,7 +206,10 @@ static bool il_applies(int ne, const FilterJob *jobs, bool fp32) {
       return false;
     nlive++;
   }
-  return nlive >= 2 && nlive <= kMaxBatch && f0->A->lanes == 0;
+  /* below 2^16 rows the problem sits in L2 and the launch is latency-bound:
+   * the grid-interleaved batch kernel is faster there (20^3, 5 slices: the
+   * whole run 0.115 vs 0.125 s) */
+  return nlive >= 2 && nlive <= kMaxBatch && f0->A->lanes == 0 && f0->A->nrows >= 65536;
 }
 
 /* workspace and per-degree coefficient table of the interleaved form,
