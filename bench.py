@@ -543,7 +543,8 @@ def run_b200_multi(args, dist):
                    "l2": "working set far above the 126 MB L2 (25 GB of Lanczos bases)",
                    "parallelism": f"replicas x{dist.world}"},
         "gpu_launches": int(launches), "clocks": clk,
-        "roofline": {"kernel": "cheb_step_batch / cheb_step (fused SpMV + Chebyshev recurrence)",
+        "roofline": {"kernel": "one filter degree for every live slice: cheb_step_il per problem "
+                               "(interleaved slices, n >= 2^16), cheb_step_batch for the rest",
                      "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "peak_source": peak_kind,
                      "bytes_per_launch": per_launch_bytes, "launches": f_launch,

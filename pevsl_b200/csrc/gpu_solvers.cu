@@ -22,6 +22,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <array>
 #include <vector>
 
 #include "gpu.cuh"
@@ -195,87 +196,100 @@ static int interleave_setting() {
 
 static int il_width(int nlive) { return nlive <= 2 ? 2 : nlive <= 4 ? 4 : nlive <= 8 ? 8 : 16; }
 
-static bool il_applies(int ne, const FilterJob *jobs, bool fp32) {
-  if (fp32 || !interleave_setting()) return false;
-  int nlive = 0;
-  const FilterJob *f0 = nullptr;
+/* a set of slices the interleaved form serves together */
+struct IlGroup {
+  const pevsl_devcsr *A;
+  int idx[kMaxBatch]; /* job indices, in job order */
+  int cnt, S, maxdeg;
+  double cc, dd;
+  size_t ws_off, mu_off; /* in doubles, into WS_IL / WS_ILMU */
+};
+
+/* The entries the interleaved form takes: groups of 2..16 live FP64
+ * entries on one short-row matrix of at least 2^16 rows with the same
+ * spectrum bounds (cc, dd), in job order; the other entries stay with the
+ * grid-interleaved batch kernel.  Below 2^16 rows the problem sits in L2
+ * and the launch is latency-bound, where the batch kernel is faster (20^3,
+ * 5 slices: the whole run 0.115 vs 0.125 s). */
+static void il_partition(int ne, const FilterJob *jobs, bool fp32, std::vector<IlGroup> &g,
+                         std::vector<char> &taken) {
+  g.clear();
+  taken.assign((size_t)ne, 0);
+  if (fp32 || !interleave_setting()) return;
+  std::vector<char> seen((size_t)ne, 0);
+  size_t ws_off = 0, mu_off = 0;
   for (int e = 0; e < ne; e++) {
-    if (jobs[e].pol->deg <= 0) continue;
-    if (!f0) f0 = &jobs[e];
-    if (jobs[e].A != f0->A || jobs[e].pol->cc != f0->pol->cc || jobs[e].pol->dd != f0->pol->dd)
-      return false;
-    nlive++;
+    const FilterJob &J = jobs[e];
+    if (seen[e] || J.pol->deg <= 0) continue;
+    const pevsl_devcsr *A = J.A;
+    if (A->lanes != 0 || A->nrows < 65536) continue;
+    std::vector<int> L;
+    for (int f = e; f < ne; f++)
+      if (!seen[f] && jobs[f].pol->deg > 0 && jobs[f].A == A && jobs[f].pol->cc == J.pol->cc &&
+          jobs[f].pol->dd == J.pol->dd) {
+        seen[f] = 1;
+        L.push_back(f);
+      }
+    for (size_t c0 = 0; c0 < L.size(); c0 += kMaxBatch) {
+      const int cnt = (int)PEVSL_MIN((size_t)kMaxBatch, L.size() - c0);
+      if (cnt < 2) continue;
+      IlGroup G;
+      G.A = A;
+      G.cnt = cnt;
+      G.S = il_width(cnt);
+      G.maxdeg = 0;
+      G.cc = J.pol->cc;
+      G.dd = J.pol->dd;
+      for (int i = 0; i < cnt; i++) {
+        G.idx[i] = L[c0 + i];
+        taken[(size_t)G.idx[i]] = 1;
+        G.maxdeg = PEVSL_MAX(G.maxdeg, jobs[G.idx[i]].pol->deg);
+      }
+      G.ws_off = ws_off;
+      G.mu_off = mu_off;
+      ws_off += 4 * (size_t)A->nrows * (size_t)G.S;
+      mu_off += (size_t)(G.maxdeg + 1) * (size_t)G.S;
+      g.push_back(G);
+    }
   }
-  /* below 2^16 rows the problem sits in L2 and the launch is latency-bound:
-   * the grid-interleaved batch kernel is faster there (20^3, 5 slices: the
-   * whole run 0.115 vs 0.125 s) */
-  return nlive >= 2 && nlive <= kMaxBatch && f0->A->lanes == 0 && f0->A->nrows >= 65536;
 }
 
-/* workspace and per-degree coefficient table of the interleaved form,
- * prepared outside any stream capture: mu row k holds mu_k of every live
- * slice (0 past a slice's degree, where its y then stays unchanged) */
-static int il_prepare(int ne, const FilterJob *jobs) {
-  int nlive = 0, maxdeg = 0;
-  for (int e = 0; e < ne; e++)
-    if (jobs[e].pol->deg > 0) {
-      nlive++;
-      maxdeg = PEVSL_MAX(maxdeg, jobs[e].pol->deg);
-    }
-  const int S = il_width(nlive);
-  long n = 0;
-  for (int e = 0; e < ne; e++)
-    if (jobs[e].pol->deg > 0) n = jobs[e].A->nrows;
-  if (!ws(WS_IL, sizeof(double) * 4 * (size_t)n * (size_t)S)) return PEVSL_ERR_NOMEM;
-  double *dmu = (double *)ws(WS_ILMU, sizeof(double) * (size_t)(maxdeg + 1) * (size_t)S);
+static size_t il_ws_doubles(const std::vector<IlGroup> &g) {
+  return g.empty() ? 0 : g.back().ws_off + 4 * (size_t)g.back().A->nrows * (size_t)g.back().S;
+}
+static size_t il_mu_doubles(const std::vector<IlGroup> &g) {
+  return g.empty() ? 0 : g.back().mu_off + (size_t)(g.back().maxdeg + 1) * (size_t)g.back().S;
+}
+
+/* workspace and per-degree coefficient tables of the interleaved groups,
+ * prepared outside any stream capture: row k of a group's table holds mu_k
+ * of each of its slices (0 past a slice's degree, where its y then stays
+ * unchanged) */
+static int il_prepare(int ne, const FilterJob *jobs, bool fp32) {
+  std::vector<IlGroup> g;
+  std::vector<char> taken;
+  il_partition(ne, jobs, fp32, g, taken);
+  if (g.empty()) return 0;
+  if (!ws(WS_IL, sizeof(double) * il_ws_doubles(g))) return PEVSL_ERR_NOMEM;
+  double *dmu = (double *)ws(WS_ILMU, sizeof(double) * il_mu_doubles(g));
   if (!dmu) return PEVSL_ERR_NOMEM;
-  std::vector<double> tab((size_t)(maxdeg + 1) * S, 0.0);
-  int c = 0;
-  for (int e = 0; e < ne; e++) {
-    const pevsl_Polparams *pol = jobs[e].pol;
-    if (pol->deg <= 0) continue;
-    for (int k = 0; k <= pol->deg; k++) tab[(size_t)k * S + c] = pol->mu[k];
-    c++;
-  }
+  std::vector<double> tab(il_mu_doubles(g), 0.0);
+  for (const IlGroup &G : g)
+    for (int c = 0; c < G.cnt; c++) {
+      const pevsl_Polparams *pol = jobs[G.idx[c]].pol;
+      for (int k = 0; k <= pol->deg; k++) tab[G.mu_off + (size_t)k * G.S + c] = pol->mu[k];
+    }
   if (memcpy_async(dmu, tab.data(), sizeof(double) * tab.size())) return PEVSL_ERR_CUDA;
   return sync();
 }
 
-static int cheb_filter_il(int ne, const FilterJob *jobs) {
-  std::vector<const double *> xs;
-  std::vector<double *> ys;
-  int maxdeg = 0;
-  const FilterJob *f0 = nullptr;
-  for (int e = 0; e < ne; e++) {
-    if (jobs[e].pol->deg <= 0) continue;
-    if (!f0) f0 = &jobs[e];
-    xs.push_back(jobs[e].x);
-    ys.push_back(jobs[e].y);
-    maxdeg = PEVSL_MAX(maxdeg, jobs[e].pol->deg);
-  }
-  const int nlive = (int)xs.size(), S = il_width(nlive);
-  while ((int)xs.size() < S) xs.push_back(xs[0]); /* padding columns: mu 0, never read back */
-  const pevsl_devcsr *A = f0->A;
-  const long n = A->nrows;
-  double *X0 = (double *)ctx().ws[WS_IL], *dmu = (double *)ctx().ws[WS_ILMU];
-  if (!X0 || !dmu || ctx().wsz[WS_IL] < sizeof(double) * 4 * (size_t)n * (size_t)S)
-    return PEVSL_ERR_ARG; /* il_prepare not run */
-  double *B0 = X0 + (size_t)n * S, *B1 = B0 + (size_t)n * S, *Y = B1 + (size_t)n * S;
-  int st = il_pack(n, S, xs.data(), X0);
-  const double cc = f0->pol->cc, dd = f0->pol->dd;
-  const double *vk = X0, *vkm1 = nullptr;
-  const double mb = 12.0 * (double)A->nnz + 4.0 * (n + 1.0);
-  for (int k = 1; k <= maxdeg && !st; k++) {
-    double *vkp1 = k == 1 ? B0 : k == 2 ? B1 : const_cast<double *>(vkm1);
-    st = cheb_step_il(A, S, vk, vkm1, vkp1, Y, cc, (k == 1 ? 1.0 : 2.0) / dd, dmu,
-                      dmu + (size_t)k * S, k == 1);
-    g_filter_launches++;
-    g_filter_bytes += mb + (k == 1 ? 24.0 : 40.0) * (double)n * S;
-    vkm1 = vk;
-    vk = vkp1;
-  }
-  if (!st) st = il_unpack(n, S, nlive, Y, ys.data());
-  return st;
+/* buffers of group G: packed input, two recurrence blocks, accumulator */
+static void il_buffers(const IlGroup &G, double **X0, double **B0, double **B1, double **Y) {
+  const size_t blk = (size_t)G.A->nrows * (size_t)G.S;
+  *X0 = (double *)ctx().ws[WS_IL] + G.ws_off;
+  *B0 = *X0 + blk;
+  *B1 = *B0 + blk;
+  *Y = *B1 + blk;
 }
 
 static double filter_bytes_degree(const pevsl_devcsr *A, int deg_k, bool fp32, bool last) {
@@ -325,13 +339,6 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     mat_bytes += (double)dmax * ((fp32 ? 8.0 : 12.0) * (double)A->nnz + 4.0 * (A->nrows + 1.0));
   }
   const int form = filter_form();
-  if (form == 0 && il_applies(ne, jobs, fp32)) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(ctx().stream, &cs);
-    /* inside a capture the caller prepared the workspace and coefficients */
-    if (cs == cudaStreamCaptureStatusNone) st = il_prepare(ne, jobs);
-    return st ? st : cheb_filter_il(ne, jobs);
-  }
   if (form == 1) {
     /* table sorted by non-increasing degree (stable: ties keep their order) */
     FiltDev tab[kMaxEntries];
@@ -385,7 +392,31 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     return st;
   }
   /* one launch per degree for all live entries; a matrix is read once per
-   * launch for all entries on it */
+   * launch for all entries on it.  Entries taken by interleaved groups run
+   * as one interleaved launch per group and degree instead. */
+  std::vector<IlGroup> ig;
+  std::vector<char> taken;
+  il_partition(ne, jobs, fp32, ig, taken);
+  std::vector<std::array<const double *, 3>> ilv(ig.size()); /* vk, vkm1 per group */
+  if (!ig.empty()) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx().stream, &cs);
+    /* inside a capture the caller prepared the workspace and coefficients */
+    if (cs == cudaStreamCaptureStatusNone) st = il_prepare(ne, jobs, fp32);
+    if (!st && (!ctx().ws[WS_IL] || ctx().wsz[WS_IL] < sizeof(double) * il_ws_doubles(ig) ||
+                !ctx().ws[WS_ILMU] || ctx().wsz[WS_ILMU] < sizeof(double) * il_mu_doubles(ig)))
+      st = PEVSL_ERR_ARG; /* il_prepare not run before the capture */
+    for (size_t gi = 0; gi < ig.size() && !st; gi++) {
+      const IlGroup &G = ig[gi];
+      const double *xs[kMaxBatch];
+      for (int c = 0; c < G.S; c++) xs[c] = jobs[G.idx[c < G.cnt ? c : 0]].x; /* padding: mu 0 */
+      double *X0, *B0, *B1, *Y;
+      il_buffers(G, &X0, &B0, &B1, &Y);
+      st = il_pack(G.A->nrows, G.S, xs, X0);
+      ilv[gi] = {X0, nullptr, nullptr};
+    }
+    if (st) return st;
+  }
   std::vector<const void *> vk(nlive), vkm1(nlive);
   std::vector<void *> b0(nlive), b1(nlive), acc(nlive);
   for (int i = 0; i < nlive; i++) {
@@ -409,9 +440,25 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
   for (int k = 1; k <= maxdeg && !st; k++) {
     int nb = 0;
     double bytes = 0.0;
+    for (size_t gi = 0; gi < ig.size() && !st; gi++) {
+      const IlGroup &G = ig[gi];
+      if (k > G.maxdeg) continue;
+      double *X0, *B0, *B1, *Y;
+      il_buffers(G, &X0, &B0, &B1, &Y);
+      const double *gk = ilv[gi][0], *gkm1 = ilv[gi][1];
+      double *gkp1 = k == 1 ? B0 : k == 2 ? B1 : const_cast<double *>(gkm1);
+      const double *dmu = (const double *)ctx().ws[WS_ILMU] + G.mu_off;
+      st = cheb_step_il(G.A, G.S, gk, gkm1, gkp1, Y, G.cc, (k == 1 ? 1.0 : 2.0) / G.dd, dmu,
+                        dmu + (size_t)k * G.S, k == 1);
+      bytes += 12.0 * (double)G.A->nnz + 4.0 * (G.A->nrows + 1.0) +
+               (k == 1 ? 24.0 : 40.0) * (double)G.A->nrows * G.S;
+      ilv[gi][1] = gk;
+      ilv[gi][0] = gkp1;
+    }
     for (int i = 0; i < nlive; i++) {
       const FilterJob &J = jobs[live[i]];
       const pevsl_Polparams *pol = J.pol;
+      if (taken[(size_t)live[i]]) continue;
       if (k > pol->deg) continue;
       /* two work vectors: from degree 3 on, v_{k+1} replaces v_{k-1} */
       void *vkp1 = k == 1 ? b0[i] : k == 2 ? b1[i] : const_cast<void *>(vkm1[i]);
@@ -431,7 +478,9 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
         bytes += entry_bytes(en[i].A, fp32, nb > 1) * (double)en[i].A->nnz +
                  4.0 * (en[i].A->nrows + 1.0);
     }
-    if (nb == 1 && !fp32 && en[0].A->lanes == 0) {
+    if (nb == 0) {
+      /* every live entry of this degree is in an interleaved group */
+    } else if (nb == 1 && !fp32 && en[0].A->lanes == 0) {
       /* one live slice: the one-vector kernel (packed entries when the
        * matrix has them); the same arithmetic as the batch */
       const ChebEntry &c = en[0];
@@ -442,6 +491,14 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     }
     g_filter_launches++;
     g_filter_bytes += bytes;
+  }
+  for (size_t gi = 0; gi < ig.size() && !st; gi++) {
+    const IlGroup &G = ig[gi];
+    double *ys[kMaxBatch];
+    for (int c = 0; c < G.cnt; c++) ys[c] = jobs[G.idx[c]].y;
+    double *X0, *B0, *B1, *Y;
+    il_buffers(G, &X0, &B0, &B1, &Y);
+    st = il_unpack(G.A->nrows, G.S, G.cnt, Y, ys);
   }
   return st;
 }
@@ -480,8 +537,8 @@ static int filter_graphed(FilterGraph &fg, const std::vector<char> &sel, std::ve
   if (!fg.exec || fg.key != sel) {
     if (fg.exec) cudaGraphExecDestroy(fg.exec);
     fg.exec = nullptr;
-    if (filter_form() == 0 && il_applies(ne, staged.data(), fg.mixed)) {
-      st = il_prepare(ne, staged.data());
+    if (filter_form() == 0) {
+      st = il_prepare(ne, staged.data(), fg.mixed);
       if (st) return st;
     }
     const uint64_t l0 = g_filter_launches, k0 = c.launches;
