@@ -502,6 +502,53 @@ def test_multi_problem_equals_separate(gpu):
         ev.close()
 
 
+def test_interleaved_filter_bit_identical(gpu):
+    """Slices of one matrix of at least 2^16 rows run the interleaved filter
+    (row-interleaved vectors, one gather for all slices); every slice gets
+    the bits of solving it alone (one-vector kernel) and the exact count."""
+    grid = (41, 41, 41)  # 68 921 rows
+    M, intvs, fl = _lap_slices(grid, 0.3, 0.36, 3)
+    assert M.n >= 65536
+    v = np.cos(np.arange(M.n) * 0.37)
+    with pv.Instance(M) as ev:
+        r, batch = pv.cheblannr_batch(ev, intvs, [200] * 3, 1e-8, v, fl)
+    assert r == 0
+    for iv, f, b in zip(intvs, fl, batch):
+        with pv.Instance(M) as ev:
+            r, (one,) = pv.cheblannr_batch(ev, [iv], [200], 1e-8, v, [f])
+        assert r == 0
+        assert one["nev"] == b["nev"] and one["its"] == b["its"]
+        assert np.array_equal(one["lam"], b["lam"]) and np.array_equal(one["res"], b["res"])
+        ex = exact_eig_lap(*grid, iv[0], iv[1])
+        assert b["nev"] == len(ex)
+        assert np.max(np.abs(b["lam"] - ex)) <= 1e-10 * np.max(np.abs(ex))
+
+
+def test_multi_problem_with_interleaved_group(gpu):
+    """A lockstep group that mixes a problem above 2^16 rows (interleaved)
+    with small problems (grid-interleaved batch kernel) gives every slice
+    the bits of solving its problem alone."""
+    specs = [((41, 41, 41), 0.3, 0.34, 2), ((11, 10, 9), 0.6, 1.4, 3)]
+    probs, sep, insts = [], [], []
+    for grid, a, b, ns in specs:
+        M, intvs, fl = _lap_slices(grid, a, b, ns)
+        v = np.sin(np.arange(M.n) * 0.11 + ns)
+        ev = pv.Instance(M)
+        insts.append((ev, M))
+        r, o = pv.cheblannr_batch(ev, intvs, [200] * ns, 1e-8, v, fl)
+        assert r == 0
+        sep.append(o)
+        probs.append((ev, intvs, [200] * ns, 1e-8, v, fl))
+    r, multi = pv.cheblannr_multi(probs)
+    assert r == 0
+    for o1, o2 in zip(sep, multi):
+        for a, b in zip(o1, o2):
+            assert a["nev"] == b["nev"] and a["its"] == b["its"]
+            assert np.array_equal(a["lam"], b["lam"])
+    for ev, M in insts:
+        ev.close()
+
+
 def test_kpm_groups_sum_to_one_group(gpu):
     """pEVSL_Kpmdos with the vectors split over two groups (SRC/kpmdos.c:
     97-102): in the counter-based Gaussian stream each group draws exactly
