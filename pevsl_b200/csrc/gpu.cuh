@@ -231,6 +231,10 @@ int cheb_step_batch(int nb, const ChebEntry *e, bool fp32);
  * alias Xkm1 */
 int cheb_step_il(const pevsl_devcsr *A, int S, const double *Xk, const double *Xkm1, double *Xkp1,
                  double *Y, double cc, double t, const double *mu0, const double *muk, int first);
+/* the same with the SpMV reading Xg instead of Xk (generalized filter) */
+int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
+                   const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
+                   const double *mu0, const double *muk, int first);
 /* X[i*S + s] = xs[s][i] (S <= kMaxBatch), and ys[s][i] = X[i*S + s] for
  * the first cols columns */
 int il_pack(long n, int S, const double *const *xs, double *X);

@@ -770,131 +770,155 @@ int pevsl_gen_lantrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pe
   return st;
 }
 
-/* pEVSL_ChebLanNr for the generalized problem (SRC/cheblanNr.c:54-448):
+/* ---------------------------------------------------------------- ChebLanNr
+ * pEVSL_ChebLanNr for the generalized problem (SRC/cheblanNr.c:54-448):
  * the filtered initial vector, the filter applied to z = B v (giving
  * B p(B^{-1}A) v), CGS_DGKS2 against (V, Z), v_{k+1} = B^{-1} z_{k+1},
  * the restricted-trace test every 20 steps from step 30, then Ritz pairs
- * normalised in the B-norm with residuals ||A u - lam B u||. */
-int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
-                        pevsl_Polparams *pol, int *nevOut, double **lamo, pevsl_Parvecs **Wo,
-                        double **reso, int *its, FILE *fstats) {
-  *nevOut = 0;
-  *lamo = nullptr;
-  *Wo = nullptr;
-  *reso = nullptr;
-  if (its) *its = 0;
-  const int Ntest = 30, cycle = 20;
-  const int N = pevsl->N;
-  const long n = pevsl->n, ld = gen_ld(n);
-  maxit = PEVSL_MIN(N, maxit);
-  const double bar = pol->bar, gamB = pol->gam;
-  if (pevsl_check_intv(intv, fstats) < 0) return 0;
-  const double aa = intv[0], bb = intv[1];
+ * normalised in the B-norm with residuals ||A u - lam B u||.  The state of
+ * one slice lives in a GenSlice, so that slices can also advance in
+ * lockstep with one interleaved filter application for all of them. */
+namespace {
+
+struct GenSlice {
+  double intv[4];
+  pevsl_Polparams *pol;
+  int maxit;
+  double *V, *Z; /* bases, ld x (maxit + 1) */
+  std::vector<double> dT, eT, EvalT;
+  double tr0 = 0.0, wn = 0.0, beta = 0.0;
+  int nwn = 0, k = 0, kdim = 0, count = 0, nconv = 0;
+  bool active = false, ran = false;
+  int status = 0;
+  int nev = 0;
+  double *Lam = nullptr, *res = nullptr;
+  pevsl_Parvecs *Rvec = nullptr;
+};
+
+const int kNtest = 30, kCycle = 20;
+
+/* checks and header lines; active when the slice is to be solved */
+void gs_begin(pevsl_Data *pevsl, GenSlice &S, FILE *fstats) {
+  S.maxit = PEVSL_MIN(pevsl->N, S.maxit);
+  S.active = false;
+  S.status = 0;
+  if (pevsl_check_intv(S.intv, fstats) < 0) return; /* no pairs, status 0 */
   if (fstats) {
-    fprintf(fstats, " intv:[%e, %e, %e, %e]\n", intv[0], intv[1], intv[2], intv[3]);
-    fprintf(fstats, " ** Cheb Poly of deg = %d, gam = %.15e, bar: %.15e\n", pol->deg, gamB, bar);
+    fprintf(fstats, " intv:[%e, %e, %e, %e]\n", S.intv[0], S.intv[1], S.intv[2], S.intv[3]);
+    fprintf(fstats, " ** Cheb Poly of deg = %d, gam = %.15e, bar: %.15e\n", S.pol->deg,
+            S.pol->gam, S.pol->bar);
   }
-  if (gamB > 1.0 || gamB < -1.0) {
-    fprintf(stdout, "gamB error %.15e\n", gamB);
-    return -1;
+  if (S.pol->gam > 1.0 || S.pol->gam < -1.0) {
+    fprintf(stdout, "gamB error %.15e\n", S.pol->gam);
+    S.status = -1;
+    return;
   }
   if (fstats) fprintf(fstats, " ** Cheb-LanNr \n");
-  double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
-  double *Z = (double *)ws(WS_ZBASIS, sizeof(double) * (size_t)ld * (size_t)(maxit + 1));
-  double *wf = (double *)ws(WS_GEN, sizeof(double) * 7 * (size_t)ld);
-  std::vector<double> dT(maxit + 1), eT(maxit + 1), EvalT(maxit + 1);
-  if (!V || !Z || !wf) return PEVSL_ERR_NOMEM;
-  double *vrand = wf + 4 * ld, *xs = wf + 5 * ld, *ys = wf + 6 * ld;
-  const bool use_graph = graphable(pevsl);
-  if (use_graph) pretune(pevsl);
-  GenGraph fg;
-  auto filter = [&](const double *in, double *out) -> int {
-    g_gen_ev.begin();
-    const int r = use_graph ? gen_filter_graphed(fg, pevsl, pol, in, out, wf, xs, ys, n)
-                            : gen_filter(pevsl, pol, in, out, wf, n);
-    g_gen_ev.end();
-    return r;
-  };
-  int st = 0, k = 0, kdim = 0, count = 0, nconv = 0;
-  double t = 0.0, tr0 = 0.0, wn = 0.0, beta = 0.0;
-  int nwn = 0;
-  /* filtered initial vector, unit B-norm */
-  st = filter(vinit->data, V);
-  if (!st) st = apply_B(pevsl, V, Z);
-  if (!st) st = dot_host(n, V, Z, &t);
+  S.dT.assign((size_t)S.maxit + 1, 0.0);
+  S.eT.assign((size_t)S.maxit + 1, 0.0);
+  S.EvalT.assign((size_t)S.maxit + 1, 0.0);
+  S.active = S.ran = true;
+}
+
+/* V(:,0) holds the filtered start vector: give it unit B-norm, Z(:,0) = B V(:,0) */
+int gs_normalize0(pevsl_Data *pevsl, GenSlice &S, long n) {
+  double t = 0.0;
+  int st = apply_B(pevsl, S.V, S.Z);
+  if (!st) st = dot_host(n, S.V, S.Z, &t);
   if (!st) {
     t = 1.0 / sqrt(t);
-    st = vscal(Z, n, t);
+    st = vscal(S.Z, n, t);
   }
-  if (!st) st = vscal(V, n, t);
-  for (k = 0; k < maxit && !st; k++) {
-    double *v = V + (size_t)k * ld, *z = Z + (size_t)k * ld;
-    double *vnew = v + ld, *znew = z + ld;
-    double alpha = 0.0;
-    st = filter(z, znew);
-    if (!st && k > 0) st = vaxpy(n, -beta, z - ld, znew);
-    if (!st) st = dot_host(n, v, znew, &alpha);
-    if (st) break;
-    dT[k] = alpha;
-    wn += fabs(alpha);
-    st = vaxpy(n, -alpha, z, znew);
-    if (!st) st = cgs2(n, ld, k + 1, Z, V, znew);
-    if (!st) st = solve_B(pevsl, znew, vnew);
-    if (!st) st = dot_host(n, vnew, znew, &beta);
-    if (st) break;
-    beta = sqrt(beta);
-    wn += 2.0 * beta;
-    nwn += 3;
-    if (beta * nwn < orthTol * wn) {
-      if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, beta);
-      st = pevsl_rand_vector_dev(vrand, (int)n);
-      if (!st) st = filter(vrand, vnew);
-      if (!st) st = cgs2(n, ld, k + 1, V, Z, vnew);
-      if (!st) st = apply_B(pevsl, vnew, znew);
-      if (!st) st = dot_host(n, vnew, znew, &beta);
-      if (st) break;
-      beta = sqrt(beta);
-      t = 1.0 / beta;
-      st = vscal(vnew, n, t);
-      if (!st) st = vscal(znew, n, t);
-      beta = 0.0;
-    } else {
-      t = 1.0 / beta;
-      st = vscal(vnew, n, t);
-      if (!st) st = vscal(znew, n, t);
-    }
-    eT[k] = beta;
-    if ((k < Ntest || (k - Ntest) % cycle != 0) && k != maxit - 1) continue;
-    kdim = k + 1;
-    if (pevsl_tridiag_eig(kdim, dT.data(), eT.data(), EvalT.data(), nullptr)) {
-      st = PEVSL_ERR_EIG;
-      break;
-    }
-    count = kdim;
-    double tr1 = 0.0;
-    nconv = 0;
-    for (int i = 0; i < count; i++)
-      if (EvalT[i] + 5 * DBL_EPSILON >= bar) {
-        tr1 += EvalT[i];
-        nconv++;
-      }
-    if (fstats) fprintf(fstats, "  k %4d:   nconv %4d  tr1 %21.15e\n", k, nconv, tr1);
-    if (fabs(tr1 - tr0) < 2e-12 || fabs(tr1) + fabs(tr0) < 1e-10) break;
-    tr0 = tr1;
+  if (!st) st = vscal(S.V, n, t);
+  return st;
+}
+
+/* the rest of step k once Z(:,k+1) holds the filtered z; filter1(in, out)
+ * is the one-vector filter (for a breakdown restart) */
+template <class F1>
+int gs_step(pevsl_Data *pevsl, GenSlice &S, long n, long ld, double *vrand, F1 filter1,
+            FILE *fstats) {
+  const int k = S.k;
+  double *v = S.V + (size_t)k * ld, *z = S.Z + (size_t)k * ld;
+  double *vnew = v + ld, *znew = z + ld;
+  double alpha = 0.0, t = 0.0;
+  int st = 0;
+  if (k > 0) st = vaxpy(n, -S.beta, z - ld, znew);
+  if (!st) st = dot_host(n, v, znew, &alpha);
+  if (st) return st;
+  S.dT[k] = alpha;
+  S.wn += fabs(alpha);
+  st = vaxpy(n, -alpha, z, znew);
+  if (!st) st = cgs2(n, ld, k + 1, S.Z, S.V, znew);
+  if (!st) st = solve_B(pevsl, znew, vnew);
+  if (!st) st = dot_host(n, vnew, znew, &S.beta);
+  if (st) return st;
+  S.beta = sqrt(S.beta);
+  S.wn += 2.0 * S.beta;
+  S.nwn += 3;
+  if (S.beta * S.nwn < orthTol * S.wn) {
+    if (fstats) fprintf(fstats, "it %4d: Lucky breakdown, beta = %.15e\n", k, S.beta);
+    st = pevsl_rand_vector_dev(vrand, (int)n);
+    if (!st) st = filter1(vrand, vnew);
+    if (!st) st = cgs2(n, ld, k + 1, S.V, S.Z, vnew);
+    if (!st) st = apply_B(pevsl, vnew, znew);
+    if (!st) st = dot_host(n, vnew, znew, &S.beta);
+    if (st) return st;
+    S.beta = sqrt(S.beta);
+    t = 1.0 / S.beta;
+    st = vscal(vnew, n, t);
+    if (!st) st = vscal(znew, n, t);
+    S.beta = 0.0;
+  } else {
+    t = 1.0 / S.beta;
+    st = vscal(vnew, n, t);
+    if (!st) st = vscal(znew, n, t);
   }
   if (st) return st;
-  if (k >= maxit && fstats)
+  S.eT[k] = S.beta;
+  S.k = k + 1;
+  if ((k < kNtest || (k - kNtest) % kCycle != 0) && k != S.maxit - 1) {
+    if (S.k >= S.maxit) S.active = false;
+    return 0;
+  }
+  S.kdim = k + 1;
+  if (pevsl_tridiag_eig(S.kdim, S.dT.data(), S.eT.data(), S.EvalT.data(), nullptr))
+    return PEVSL_ERR_EIG;
+  S.count = S.kdim;
+  double tr1 = 0.0;
+  S.nconv = 0;
+  const double bar = S.pol->bar;
+  for (int i = 0; i < S.count; i++)
+    if (S.EvalT[i] + 5 * DBL_EPSILON >= bar) {
+      tr1 += S.EvalT[i];
+      S.nconv++;
+    }
+  if (fstats) fprintf(fstats, "  k %4d:   nconv %4d  tr1 %21.15e\n", k, S.nconv, tr1);
+  if (fabs(tr1 - S.tr0) < 2e-12 || fabs(tr1) + fabs(S.tr0) < 1e-10) {
+    S.active = false;
+    S.k = k; /* the loop left at step k, as the reference's break */
+    return 0;
+  }
+  S.tr0 = tr1;
+  if (S.k >= S.maxit) S.active = false;
+  return 0;
+}
+
+/* Ritz pairs of a finished slice: eigenvectors of T for the values >= bar */
+int gs_finish(pevsl_Data *pevsl, GenSlice &S, pevsl_Parvec *vinit, long n, long ld, double tol,
+              FILE *fstats) {
+  if (S.k >= S.maxit && fstats)
     fprintf(fstats, "The max number of iterations [%d] has been reached. The eigenvalues "
-                    "computed may not have converged\n", maxit);
-  if (its) *its = kdim;
-  /* Ritz pairs: eigenvectors of T for the values >= bar only */
-  if (kdim > 0 && pevsl_tridiag_eig(kdim, dT.data(), eT.data(), EvalT.data(), nullptr))
+                    "computed may not have converged\n", S.maxit);
+  const int kdim = S.kdim, count = S.count;
+  const double bar = S.pol->bar, aa = S.intv[0], bb = S.intv[1];
+  if (kdim > 0 && pevsl_tridiag_eig(kdim, S.dT.data(), S.eT.data(), S.EvalT.data(), nullptr))
     return PEVSL_ERR_EIG;
   std::vector<int> sel;
   for (int i = 0; i < count; i++)
-    if (EvalT[i] >= bar) sel.push_back(i);
+    if (S.EvalT[i] >= bar) sel.push_back(i);
   const int nsel = (int)sel.size();
-  const int nout = PEVSL_MAX(nconv, nsel);
+  const int nout = PEVSL_MAX(S.nconv, nsel);
   double *Lam = (double *)malloc(sizeof(double) * (size_t)(nout > 0 ? nout : 1));
   double *res = (double *)malloc(sizeof(double) * (size_t)(nout > 0 ? nout : 1));
   pevsl_Parvecs *Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
@@ -905,7 +929,7 @@ int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, 
     return PEVSL_ERR_NOMEM;
   }
   pEVSL_ParvecsDuplParvec(vinit, nout, (int)n, Rvec);
-  int nev = 0;
+  int nev = 0, st = 0;
   if (nsel > 0) {
     std::vector<double> Y((size_t)kdim * nsel), hv(3 * (size_t)nsel);
     double *U = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * (size_t)nsel);
@@ -914,11 +938,11 @@ int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, 
     double *dY = (double *)ws(WS_PART, sizeof(double) * (size_t)kdim * (size_t)nsel);
     double *dv = (double *)ws(WS_MOM, sizeof(double) * 3 * (size_t)nsel);
     if (!U || !W || !BU || !dY || !dv || (nout > 0 && !Rvec->data)) st = PEVSL_ERR_NOMEM;
-    if (!st && pevsl_tridiag_eig_sel(kdim, dT.data(), eT.data(), EvalT.data(), nsel, sel.data(),
-                                     Y.data()))
+    if (!st && pevsl_tridiag_eig_sel(kdim, S.dT.data(), S.eT.data(), S.EvalT.data(), nsel,
+                                     sel.data(), Y.data()))
       st = PEVSL_ERR_EIG;
     if (!st) st = memcpy_async(dY, Y.data(), sizeof(double) * Y.size());
-    if (!st) st = gemm_nn(n, kdim, nsel, V, ld, dY, kdim, U, ld);
+    if (!st) st = gemm_nn(n, kdim, nsel, S.V, ld, dY, kdim, U, ld);
     for (int j = 0; j < nsel && !st; j++) st = apply_B(pevsl, U + (size_t)j * ld, BU + (size_t)j * ld);
     if (!st) st = vdot_cols(n, nsel, U, ld, BU, ld, dv);
     if (!st) st = memcpy_async(hv.data(), dv, sizeof(double) * (size_t)nsel);
@@ -957,11 +981,259 @@ int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, 
     free(Rvec);
     return st;
   }
-  *nevOut = nev;
-  *lamo = Lam;
-  *Wo = Rvec;
-  *reso = res;
+  S.nev = nev;
+  S.Lam = Lam;
+  S.res = res;
+  S.Rvec = Rvec;
   return 0;
+}
+
+/* ------------------------------------------------------------ lockstep filter
+ * The generalized filter for up to 16 slices of one problem at once, their
+ * vectors row-interleaved: per degree, the least-squares B-solve as its
+ * Chebyshev degrees on B (cheb_step_il, the same coefficients for every
+ * column) and the A step (cheb_step_il_x: the SpMV reads B^{-1} X_k, the
+ * recurrence X_k, each column with its slice's coefficients, zero past its
+ * degree).  Per column the arithmetic is that of gen_filter, bit for bit.
+ * The degree loop works on fixed blocks, so it is captured once in a CUDA
+ * graph; packing the inputs and unpacking the outputs stay outside. */
+struct GenIl {
+  int S = 0, maxdeg = 0, degB = 0;
+  long n = 0;
+  const pevsl_devcsr *A = nullptr, *B = nullptr;
+  double cc = 0, dd = 0, ccB = 0, ddB = 0;
+  double *blk = nullptr; /* X0, B0, B1, Y, W, L0, L1: n x S each */
+  double *smu = nullptr, *lmu = nullptr; /* coefficient tables on the device */
+  GenGraph graph;
+  bool use_graph = false;
+  double *X(int i) const { return blk + (size_t)i * (size_t)n * (size_t)S; }
+};
+
+int genil_degrees(pevsl_Data *pevsl, GenIl &G) {
+  const double *vk = G.X(0), *vkm1 = nullptr;
+  int st = 0;
+  for (int k = 1; k <= G.maxdeg && !st; k++) {
+    /* W = the least-squares B^{-1} of X_k */
+    const double *lk = vk, *lkm1 = nullptr;
+    for (int j = 1; j <= G.degB && !st; j++) {
+      double *lkp1 = j == 1 ? G.X(5) : j == 2 ? G.X(6) : const_cast<double *>(lkm1);
+      st = cheb_step_il(G.B, G.S, lk, lkm1, lkp1, G.X(4), G.ccB, (j == 1 ? 1.0 : 2.0) / G.ddB,
+                        G.lmu, G.lmu + (size_t)j * G.S, j == 1);
+      lkm1 = lk;
+      lk = lkp1;
+    }
+    double *vkp1 = k == 1 ? G.X(1) : k == 2 ? G.X(2) : const_cast<double *>(vkm1);
+    if (!st)
+      st = cheb_step_il_x(G.A, G.S, G.X(4), vk, vkm1, vkp1, G.X(3), G.cc,
+                          (k == 1 ? 1.0 : 2.0) / G.dd, G.smu, G.smu + (size_t)k * G.S, k == 1);
+    vkm1 = vk;
+    vk = vkp1;
+  }
+  pevsl->stats->n_mvA += (size_t)G.maxdeg * G.S;
+  pevsl->stats->n_svB += (size_t)G.maxdeg * G.S;
+  g_gen_filters++;
+  g_gen_degrees += (uint64_t)G.maxdeg;
+  const double n = (double)G.n;
+  g_gen_bytes += (double)G.maxdeg *
+                 (G.degB * (12.0 * G.B->nnz + 4.0 * (n + 1) + 40.0 * n * G.S) + 12.0 * G.A->nnz +
+                  4.0 * (n + 1) + 48.0 * n * G.S);
+  return st;
+}
+
+/* one lockstep filter application: column c filters xs[c] into ys[c] */
+int genil_apply(pevsl_Data *pevsl, GenIl &G, const double *const *xs, double *const *ys) {
+  g_gen_ev.begin();
+  int st = il_pack(G.n, G.S, xs, G.X(0));
+  if (!st) {
+    if (G.use_graph)
+      st = graph_run(G.graph, pevsl, [&]() { return genil_degrees(pevsl, G); });
+    else
+      st = genil_degrees(pevsl, G);
+  }
+  if (!st) st = il_unpack(G.n, G.S, G.S, G.X(3), ys);
+  g_gen_ev.end();
+  return st;
+}
+
+}  // namespace
+
+int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
+                        pevsl_Polparams *pol, int *nevOut, double **lamo, pevsl_Parvecs **Wo,
+                        double **reso, int *its, FILE *fstats) {
+  *nevOut = 0;
+  *lamo = nullptr;
+  *Wo = nullptr;
+  *reso = nullptr;
+  if (its) *its = 0;
+  const long n = pevsl->n, ld = gen_ld(n);
+  GenSlice S;
+  memcpy(S.intv, intv, sizeof S.intv);
+  S.pol = pol;
+  S.maxit = maxit;
+  gs_begin(pevsl, S, fstats);
+  if (!S.active) return S.status;
+  double *V = (double *)ws(WS_BASIS, sizeof(double) * (size_t)ld * (size_t)(S.maxit + 1));
+  double *Z = (double *)ws(WS_ZBASIS, sizeof(double) * (size_t)ld * (size_t)(S.maxit + 1));
+  double *wf = (double *)ws(WS_GEN, sizeof(double) * 7 * (size_t)ld);
+  if (!V || !Z || !wf) return PEVSL_ERR_NOMEM;
+  S.V = V;
+  S.Z = Z;
+  double *vrand = wf + 4 * ld, *xs = wf + 5 * ld, *ys = wf + 6 * ld;
+  const bool use_graph = graphable(pevsl);
+  if (use_graph) pretune(pevsl);
+  GenGraph fg;
+  auto filter = [&](const double *in, double *out) -> int {
+    g_gen_ev.begin();
+    const int r = use_graph ? gen_filter_graphed(fg, pevsl, pol, in, out, wf, xs, ys, n)
+                            : gen_filter(pevsl, pol, in, out, wf, n);
+    g_gen_ev.end();
+    return r;
+  };
+  /* filtered initial vector, unit B-norm */
+  int st = filter(vinit->data, S.V);
+  if (!st) st = gs_normalize0(pevsl, S, n);
+  while (!st && S.active) {
+    st = filter(S.Z + (size_t)S.k * ld, S.Z + (size_t)(S.k + 1) * ld);
+    if (!st) st = gs_step(pevsl, S, n, ld, vrand, filter, fstats);
+  }
+  if (st) return st;
+  if (its) *its = S.kdim;
+  st = gs_finish(pevsl, S, vinit, n, ld, tol, fstats);
+  if (st) return st;
+  *nevOut = S.nev;
+  *lamo = S.Lam;
+  *Wo = S.Rvec;
+  *reso = S.res;
+  return 0;
+}
+
+/* Slices [0, ns) of one generalized problem in lockstep (the batched
+ * entry points): one interleaved filter application per step for all
+ * slices still iterating, the rest of each step per slice.  Applies when A
+ * is the built-in matrix, the B-solve is the library's least-squares
+ * polynomial, both matrices have short rows, 2 <= ns <= 16 and the filters
+ * share the spectrum bounds; returns 1 (nothing done) otherwise.  Each
+ * slice's result equals solving it alone (unless a breakdown restart draws
+ * random vectors, whose order then differs). */
+int pevsl_gen_cheblannr_lockstep(pevsl_Data *pevsl, int ns, const double *intvs, const int *maxits,
+                                 double tol, pevsl_Parvec *vinit, pevsl_Polparams *pols,
+                                 int *nevOut, double **lamo, pevsl_Parvecs **Wo, double **reso,
+                                 int *its, int *status, FILE *fstats) {
+  pevsl_devcsr *A = pevsl_builtin_A(pevsl);
+  if (ns < 2 || ns > kMaxBatch || !A || A->lanes != 0 || !pevsl->Bsol ||
+      pevsl->Bsol->func != pEVSL_LSPolSol || getenv("PEVSL_B200_GEN_LOCKSTEP_OFF"))
+    return 1;
+  const pevsl_lspol *L = (const pevsl_lspol *)pevsl->Bsol->data;
+  if (!L || !L->B || L->B->lanes != 0 || L->deg < 1 || L->B->nrows != A->nrows) return 1;
+  for (int s = 0; s < ns; s++)
+    if (pols[s].cc != pols[0].cc || pols[s].dd != pols[0].dd || pols[s].deg < 1) return 1;
+  const long n = pevsl->n, ld = gen_ld(n);
+  std::vector<GenSlice> SL((size_t)ns);
+  size_t basis = 0;
+  for (int s = 0; s < ns; s++) {
+    nevOut[s] = 0;
+    lamo[s] = nullptr;
+    Wo[s] = nullptr;
+    reso[s] = nullptr;
+    its[s] = 0;
+    memcpy(SL[s].intv, intvs + 4 * (size_t)s, sizeof SL[s].intv);
+    SL[s].pol = &pols[s];
+    SL[s].maxit = maxits[s];
+    gs_begin(pevsl, SL[s], fstats);
+    status[s] = SL[s].status;
+    if (SL[s].active) basis += (size_t)ld * (size_t)(SL[s].maxit + 1);
+  }
+  GenIl G;
+  G.S = ns <= 2 ? 2 : ns <= 4 ? 4 : ns <= 8 ? 8 : 16;
+  G.n = n;
+  G.A = A;
+  G.B = L->B;
+  G.cc = pols[0].cc;
+  G.dd = pols[0].dd;
+  G.ccB = L->cc;
+  G.ddB = L->dd;
+  G.degB = L->deg;
+  for (int s = 0; s < ns; s++) G.maxdeg = PEVSL_MAX(G.maxdeg, pols[s].deg);
+  double *V = (double *)ws(WS_BASIS, sizeof(double) * (basis ? basis : 1));
+  double *Z = (double *)ws(WS_ZBASIS, sizeof(double) * (basis ? basis : 1));
+  /* four filter work vectors, a random vector, one scratch output per
+   * padding or finished column */
+  double *wf = (double *)ws(WS_GEN, sizeof(double) * (5 + kMaxBatch) * (size_t)ld);
+  G.blk = (double *)ws(WS_IL, sizeof(double) * 7 * (size_t)n * (size_t)G.S);
+  double *mu = (double *)ws(WS_ILMU, sizeof(double) * (size_t)(G.maxdeg + 1 + G.degB + 1) * G.S);
+  if (!V || !Z || !wf || !G.blk || !mu) return PEVSL_ERR_NOMEM;
+  G.smu = mu;
+  G.lmu = mu + (size_t)(G.maxdeg + 1) * G.S;
+  {
+    std::vector<double> tab((size_t)(G.maxdeg + 1 + G.degB + 1) * G.S, 0.0);
+    for (int s = 0; s < ns; s++)
+      for (int k = 0; k <= pols[s].deg; k++) tab[(size_t)k * G.S + s] = pols[s].mu[k];
+    for (int j = 0; j <= G.degB; j++)
+      for (int c = 0; c < G.S; c++) tab[(size_t)(G.maxdeg + 1 + j) * G.S + c] = L->mu[j];
+    int st0 = memcpy_async(mu, tab.data(), sizeof(double) * tab.size());
+    if (!st0) st0 = sync();
+    if (st0) return st0;
+  }
+  size_t off = 0;
+  for (int s = 0; s < ns; s++)
+    if (SL[s].active) {
+      SL[s].V = V + off;
+      SL[s].Z = Z + off;
+      off += (size_t)ld * (size_t)(SL[s].maxit + 1);
+    }
+  double *vrand = wf + 4 * ld;
+  auto dummy = [&](int c) { return wf + (5 + (size_t)c) * ld; };
+  G.use_graph = graphable(pevsl);
+  if (G.use_graph) pretune(pevsl);
+  auto filter1 = [&](const pevsl_Polparams *pol, const double *in, double *out) -> int {
+    return gen_filter(pevsl, pol, in, out, wf, n);
+  };
+  /* filtered initial vectors of every slice in one application */
+  const double *xs[kMaxBatch];
+  double *ys[kMaxBatch];
+  for (int c = 0; c < G.S; c++) {
+    xs[c] = vinit->data;
+    ys[c] = c < ns && SL[c].active ? SL[c].V : dummy(c);
+  }
+  int st = genil_apply(pevsl, G, xs, ys);
+  for (int s = 0; s < ns && !st; s++)
+    if (SL[s].active) st = gs_normalize0(pevsl, SL[s], n);
+  for (;;) {
+    if (st) break;
+    bool any = false;
+    for (int c = 0; c < G.S; c++) {
+      const bool on = c < ns && SL[c].active;
+      any = any || on;
+      xs[c] = on ? SL[c].Z + (size_t)SL[c].k * ld : vinit->data;
+      ys[c] = on ? SL[c].Z + (size_t)(SL[c].k + 1) * ld : dummy(c);
+    }
+    if (!any) break;
+    st = genil_apply(pevsl, G, xs, ys);
+    for (int s = 0; s < ns && !st; s++) {
+      if (!SL[s].active) continue;
+      const pevsl_Polparams *pol = SL[s].pol;
+      st = gs_step(pevsl, SL[s], n, ld, vrand,
+                   [&](const double *in, double *out) { return filter1(pol, in, out); }, fstats);
+    }
+  }
+  int first_err = st;
+  for (int s = 0; s < ns && !st; s++) {
+    if (!SL[s].ran || SL[s].status) continue;
+    its[s] = SL[s].kdim;
+    const int r = gs_finish(pevsl, SL[s], vinit, n, ld, tol, fstats);
+    status[s] = r;
+    if (r) {
+      if (!first_err) first_err = r;
+      continue;
+    }
+    nevOut[s] = SL[s].nev;
+    lamo[s] = SL[s].Lam;
+    Wo[s] = SL[s].Rvec;
+    reso[s] = SL[s].res;
+  }
+  for (int s = 0; s < ns && !first_err; s++)
+    if (status[s] && !first_err) first_err = status[s];
+  return first_err;
 }
 
 /* ====================================================== C API */

@@ -1973,7 +1973,16 @@ int pEVSL_B200_ChebLanNrBatch(pevsl_Data *pevsl, int nslices, const double *intv
   if (nslices < 0) return PEVSL_ERR_ARG;
   int first_err = 0;
   if (pevsl->ifGenEv) {
-    /* generalized problem: the slices one after the other */
+    /* generalized problem: in lockstep where the lockstep form applies,
+     * else the slices one after the other */
+    if (nslices >= 2 && nslices <= kMaxBatch) {
+      const int r = pevsl_gen_cheblannr_lockstep(pevsl, nslices, intvs, maxits, tol, vinit, pols,
+                                                 nevOut, lamo, Wo, reso, its, status, fstats);
+      if (r != 1) {
+        pevsl->stats->t_iter = pevsl_now() - tall;
+        return r;
+      }
+    }
     for (int s = 0; s < nslices; s++) {
       double iv[4];
       memcpy(iv, intvs + 4 * (size_t)s, sizeof iv);

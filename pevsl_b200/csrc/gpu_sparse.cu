@@ -1000,13 +1000,14 @@ int chebiter2_step(const pevsl_devcsr *B, const double *d, double *x, double *r,
  * per vector.  Lane s adds its row's products in entry order and applies
  * the recurrence of its own column (cheb_update_v with its own mu), which is
  * the arithmetic of the one-vector kernel, bit for bit.  X_{k+1} may alias
- * X_{k-1} (each lane reads its own element first). */
+ * X_{k-1} (each lane reads its own element first).  The SpMV reads Xg,
+ * which is Xk except in the generalized filter (Xg = B^{-1} X_k). */
 template <int S>
 __global__ void __launch_bounds__(kThreads)
     k_cheb_il(int n, const int *__restrict__ ia, const int *__restrict__ ja,
-              const double *__restrict__ a, const double *__restrict__ Xk, const double *Xkm1,
-              double *Xkp1, double *Y, double cc, double t, const double *__restrict__ mu0,
-              const double *__restrict__ muk, int first) {
+              const double *__restrict__ a, const double *__restrict__ Xg,
+              const double *__restrict__ Xk, const double *Xkm1, double *Xkp1, double *Y, double cc,
+              double t, const double *__restrict__ mu0, const double *__restrict__ muk, int first) {
   constexpr int RPW = 32 / S; /* rows per warp */
   const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, s = lane % S;
@@ -1022,14 +1023,14 @@ __global__ void __launch_bounds__(kThreads)
   for (; j + 3 < e; j += 4) {
     const int c0 = __ldg(ja + j), c1 = __ldg(ja + j + 1), c2 = __ldg(ja + j + 2), c3 = __ldg(ja + j + 3);
     const double a0 = __ldg(a + j), a1 = __ldg(a + j + 1), a2 = __ldg(a + j + 2), a3 = __ldg(a + j + 3);
-    const double x0 = __ldg(Xk + (size_t)c0 * S + s), x1 = __ldg(Xk + (size_t)c1 * S + s);
-    const double x2 = __ldg(Xk + (size_t)c2 * S + s), x3 = __ldg(Xk + (size_t)c3 * S + s);
+    const double x0 = __ldg(Xg + (size_t)c0 * S + s), x1 = __ldg(Xg + (size_t)c1 * S + s);
+    const double x2 = __ldg(Xg + (size_t)c2 * S + s), x3 = __ldg(Xg + (size_t)c3 * S + s);
     r = __dadd_rn(r, __dmul_rn(a0, x0));
     r = __dadd_rn(r, __dmul_rn(a1, x1));
     r = __dadd_rn(r, __dmul_rn(a2, x2));
     r = __dadd_rn(r, __dmul_rn(a3, x3));
   }
-  for (; j < e; j++) r = __dadd_rn(r, __dmul_rn(__ldg(a + j), __ldg(Xk + (size_t)__ldg(ja + j) * S + s)));
+  for (; j < e; j++) r = __dadd_rn(r, __dmul_rn(__ldg(a + j), __ldg(Xg + (size_t)__ldg(ja + j) * S + s)));
   double w, yv;
   cheb_update_v(r, x, xm1, Xkm1 != nullptr, cc, t, mu0[s], muk[s], first, yold, &w, &yv);
   Xkp1[me] = w;
@@ -1068,23 +1069,29 @@ int il_unpack(long n, int S, int cols, const double *X, double *const *ys) {
 /* S is padded up to 2, 4, 8 or 16 by the caller (unused columns are zero) */
 int cheb_step_il(const pevsl_devcsr *A, int S, const double *Xk, const double *Xkm1, double *Xkp1,
                  double *Y, double cc, double t, const double *mu0, const double *muk, int first) {
+  return cheb_step_il_x(A, S, Xk, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, first);
+}
+
+int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
+                   const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
+                   const double *mu0, const double *muk, int first) {
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
   switch (S) {
     case 2:
-      k_cheb_il<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1, Xkp1,
+      k_cheb_il<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
                                                      Y, cc, t, mu0, muk, first);
       break;
     case 4:
-      k_cheb_il<4><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1, Xkp1,
+      k_cheb_il<4><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
                                                      Y, cc, t, mu0, muk, first);
       break;
     case 8:
-      k_cheb_il<8><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1, Xkp1,
+      k_cheb_il<8><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
                                                      Y, cc, t, mu0, muk, first);
       break;
     case 16:
-      k_cheb_il<16><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xk, Xkm1,
+      k_cheb_il<16><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1,
                                                       Xkp1, Y, cc, t, mu0, muk, first);
       break;
     default:

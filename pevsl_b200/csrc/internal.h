@@ -115,6 +115,11 @@ int pevsl_gen_lantrbounds(pevsl_Data *pevsl, int lanm, int maxit, double tol, pe
 int pevsl_gen_cheblannr(pevsl_Data *pevsl, double *intv, int maxit, double tol, pevsl_Parvec *vinit,
                         pevsl_Polparams *pol, int *nevOut, double **lamo, pevsl_Parvecs **Wo,
                         double **reso, int *its, FILE *fstats);
+/* slices of one generalized problem in lockstep; 1 when not applicable */
+int pevsl_gen_cheblannr_lockstep(pevsl_Data *pevsl, int ns, const double *intvs, const int *maxits,
+                                 double tol, pevsl_Parvec *vinit, pevsl_Polparams *pols,
+                                 int *nevOut, double **lamo, pevsl_Parvecs **Wo, double **reso,
+                                 int *its, int *status, FILE *fstats);
 
 /* RNG state (host side; rng.cu owns the device generator) */
 int pevsl_rng_mode(void);

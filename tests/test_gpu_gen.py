@@ -207,3 +207,42 @@ def test_generalized_filter_against_dense(gpu):
         yref = yref + f.mu[k] * tn
         tkm1, tk = tk, tn
     assert rel(y, yref) <= 1e-10
+
+
+def test_generalized_lockstep_equals_one_by_one(gpu, monkeypatch):
+    """Slices of one generalized problem with the least-squares B-solve run
+    in lockstep (one interleaved filter application per step for all of
+    them); each slice gets the bits of solving it alone, and every
+    eigenvalue of the dense pencil in the interval (A 2D Laplacian 24 x 24,
+    B 1D Laplacian of the same size)."""
+    import scipy.linalg as sl
+    A, LA = csr_of(24, 24, 1)
+    B, LB = csr_of(576, 1, 1)
+    Ad, Bd = np.zeros((576, 576)), np.zeros((576, 576))
+    for M, L in ((Ad, LA), (Bd, LB)):
+        for i in range(576):
+            M[i, L.ja[L.ia[i]:L.ia[i + 1]]] = L.a[L.ia[i]:L.ia[i + 1]]
+    w = sl.eigh(Ad, Bd, eigvals_only=True)
+    lmin, lmax = w[0] - 1e-6, w[-1] + 1e-6
+    edges = np.linspace(0.4, 0.7, 4)
+    intvs = [[edges[i], edges[i + 1], lmin, lmax] for i in range(3)]
+    fl = [pv.findpol(iv, 3000, 2, 0.6, 0.15)[1] for iv in intvs]
+    v = np.cos(np.arange(576) * 0.3)
+    bs = pv.BSolver(B, "lsrec", 2.0, 6.0, 80, 1e-10)
+    outs = {}
+    for mode in ("lockstep", "one_by_one"):
+        if mode == "one_by_one":
+            monkeypatch.setenv("PEVSL_B200_GEN_LOCKSTEP_OFF", "1")
+        with pv.Instance(A) as ev:
+            ev.set_generalized(B, bs)
+            r, o = pv.cheblannr_batch(ev, intvs, [400] * 3, 1e-8, v, fl)
+        assert r == 0
+        outs[mode] = o
+    bs.free()
+    for iv, a, b in zip(intvs, outs["lockstep"], outs["one_by_one"]):
+        assert a["nev"] == b["nev"] and a["its"] == b["its"]
+        assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
+        ex = w[(w >= iv[0]) & (w <= iv[1])]
+        assert a["nev"] == len(ex)
+        assert np.max(np.abs(a["lam"] - ex) / np.abs(ex)) <= 1e-10
+        assert np.max(a["res"]) <= 1e-8
