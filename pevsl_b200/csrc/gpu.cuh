@@ -243,6 +243,8 @@ int il_unpack(long n, int S, int cols, const double *X, double *const *ys);
  * packed form (int16 column offset + uint8 value index), else 12 (int32
  * column + FP64 value) or 8 (FP32 value) */
 double entry_bytes(const pevsl_devcsr *A, bool fp32, bool batch = false);
+/* bytes per entry the interleaved kernel reads for A (3 packed, 12 plain) */
+double il_entry_bytes(const pevsl_devcsr *A);
 /* L2 persistence window over the part of A the kernels read (if enabled) */
 void matrix_window(const pevsl_devcsr *A);
 /* choose the CSR-stream rows per lane of a matrix by timing (once) */

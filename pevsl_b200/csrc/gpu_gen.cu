@@ -1035,8 +1035,8 @@ int genil_degrees(pevsl_Data *pevsl, GenIl &G) {
   g_gen_degrees += (uint64_t)G.maxdeg;
   const double n = (double)G.n;
   g_gen_bytes += (double)G.maxdeg *
-                 (G.degB * (12.0 * G.B->nnz + 4.0 * (n + 1) + 40.0 * n * G.S) + 12.0 * G.A->nnz +
-                  4.0 * (n + 1) + 48.0 * n * G.S);
+                 (G.degB * (il_entry_bytes(G.B) * G.B->nnz + 4.0 * (n + 1) + 40.0 * n * G.S) +
+                  il_entry_bytes(G.A) * G.A->nnz + 4.0 * (n + 1) + 48.0 * n * G.S);
   return st;
 }
 

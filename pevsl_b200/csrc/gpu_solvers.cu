@@ -450,7 +450,7 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
       const double *dmu = (const double *)ctx().ws[WS_ILMU] + G.mu_off;
       st = cheb_step_il(G.A, G.S, gk, gkm1, gkp1, Y, G.cc, (k == 1 ? 1.0 : 2.0) / G.dd, dmu,
                         dmu + (size_t)k * G.S, k == 1);
-      bytes += 12.0 * (double)G.A->nnz + 4.0 * (G.A->nrows + 1.0) +
+      bytes += il_entry_bytes(G.A) * (double)G.A->nnz + 4.0 * (G.A->nrows + 1.0) +
                (k == 1 ? 24.0 : 40.0) * (double)G.A->nrows * G.S;
       ilv[gi][1] = gk;
       ilv[gi][0] = gkp1;

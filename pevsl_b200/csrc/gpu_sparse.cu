@@ -1037,6 +1037,52 @@ __global__ void __launch_bounds__(kThreads)
   Y[me] = yv;
 }
 
+/* k_cheb_il on the packed entries (int16 column offset from the row's
+ * 32-row group, uint8 index into the value table staged in shared memory):
+ * the same products in the same order */
+template <int S>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb_il_p(int n, const int *__restrict__ ia, const short *__restrict__ dj,
+                const unsigned char *__restrict__ vi, const double *__restrict__ vtab, int nv,
+                const double *__restrict__ Xg, const double *__restrict__ Xk, const double *Xkm1,
+                double *Xkp1, double *Y, double cc, double t, const double *__restrict__ mu0,
+                const double *__restrict__ muk, int first) {
+  __shared__ double vt[256];
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
+  __syncthreads();
+  constexpr int RPW = 32 / S;
+  const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, s = lane % S;
+  const long row = gw * RPW + lane / S;
+  if (row >= n) return;
+  const int g0 = (int)(row & ~31L);
+  const size_t me = (size_t)row * S + s;
+  const double x = Xk[me];
+  const double xm1 = Xkm1 ? Xkm1[me] : 0.0;
+  const double yold = first ? 0.0 : Y[me];
+  const int e = __ldg(ia + row + 1);
+  double r = 0.0;
+  int j = __ldg(ia + row);
+  for (; j + 3 < e; j += 4) {
+    const int c0 = g0 + __ldg(dj + j), c1 = g0 + __ldg(dj + j + 1);
+    const int c2 = g0 + __ldg(dj + j + 2), c3 = g0 + __ldg(dj + j + 3);
+    const double a0 = vt[__ldg(vi + j)], a1 = vt[__ldg(vi + j + 1)];
+    const double a2 = vt[__ldg(vi + j + 2)], a3 = vt[__ldg(vi + j + 3)];
+    const double x0 = __ldg(Xg + (size_t)c0 * S + s), x1 = __ldg(Xg + (size_t)c1 * S + s);
+    const double x2 = __ldg(Xg + (size_t)c2 * S + s), x3 = __ldg(Xg + (size_t)c3 * S + s);
+    r = __dadd_rn(r, __dmul_rn(a0, x0));
+    r = __dadd_rn(r, __dmul_rn(a1, x1));
+    r = __dadd_rn(r, __dmul_rn(a2, x2));
+    r = __dadd_rn(r, __dmul_rn(a3, x3));
+  }
+  for (; j < e; j++)
+    r = __dadd_rn(r, __dmul_rn(vt[__ldg(vi + j)], __ldg(Xg + (size_t)(g0 + __ldg(dj + j)) * S + s)));
+  double w, yv;
+  cheb_update_v(r, x, xm1, Xkm1 != nullptr, cc, t, mu0[s], muk[s], first, yold, &w, &yv);
+  Xkp1[me] = w;
+  Y[me] = yv;
+}
+
 /* X[i*S + s] = x_s[i] and back */
 __global__ void k_il_pack(long n, int S, CPtrs xs, double *X) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n * S;
@@ -1072,11 +1118,41 @@ int cheb_step_il(const pevsl_devcsr *A, int S, const double *Xk, const double *X
   return cheb_step_il_x(A, S, Xk, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, first);
 }
 
+/* packed entries in the interleaved kernel (PEVSL_B200_IL_PACKED: 1 on, the
+ * default; 0 off).  Measured per degree at 100^3: 2 slices 20.6 vs 33.7 us,
+ * 4 slices 47.5 vs 51.1 us, 16 slices 172.8 vs 174.0 us; 160^3, 4 slices
+ * 183.5 vs 200.8 us. */
+static bool il_packed(const pevsl_devcsr *A) {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("PEVSL_B200_IL_PACKED");
+    v = e ? atoi(e) != 0 : 1;
+  }
+  return v && A->pdj != nullptr && packed_mode() >= 1;
+}
+
+double il_entry_bytes(const pevsl_devcsr *A) { return il_packed(A) ? 3.0 : 12.0; }
+
 int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
                    const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
                    const double *mu0, const double *muk, int first) {
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
+  if (il_packed(A)) {
+    cudaStream_t st = ctx().stream;
+#define PV_IL_P(SS)                                                                          \
+  k_cheb_il_p<SS><<<g, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, \
+                                          Xg, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, first)
+    switch (S) {
+      case 2: PV_IL_P(2); break;
+      case 4: PV_IL_P(4); break;
+      case 8: PV_IL_P(8); break;
+      case 16: PV_IL_P(16); break;
+      default: return PEVSL_ERR_ARG;
+    }
+#undef PV_IL_P
+    return launched("cheb_step_il_packed");
+  }
   switch (S) {
     case 2:
       k_cheb_il<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
