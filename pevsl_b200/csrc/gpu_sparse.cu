@@ -1128,7 +1128,10 @@ static bool il_packed(const pevsl_devcsr *A) {
     const char *e = getenv("PEVSL_B200_IL_PACKED");
     v = e ? atoi(e) != 0 : 1;
   }
-  return v && A->pdj != nullptr && packed_mode() >= 1;
+  /* small matrices (the generalized path's lockstep, L2-resident) keep the
+   * plain kernel: the table staging costs more than it saves there
+   * (genlap24: 53.3 vs 49.5 us per degree) */
+  return v && A->pdj != nullptr && packed_mode() >= 1 && A->nrows >= 65536;
 }
 
 double il_entry_bytes(const pevsl_devcsr *A) { return il_packed(A) ? 3.0 : 12.0; }
