@@ -103,7 +103,7 @@ def test_learned_dos_denoises_few_vector_moments(gpu):
     err_learned = np.linalg.norm(P[:, 1:] - Th[:, 1:], axis=1)
     assert np.mean(err_learned) < np.mean(err_plain), (err_learned, err_plain)
     assert np.mean(err_learned < err_plain) >= 0.75, (err_learned, err_plain)
-    # the slicing path with its plain-KPM judge runs end to end
+    # the slicing path with its plain-KPM check runs end to end
     kind, s, size = held[0]
     n, ia, ja, a = ld.family_matrix(kind, s, size)
     M = pv.Matrix.from_csr(n, ia, ja, a)
