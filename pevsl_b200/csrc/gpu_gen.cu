@@ -367,7 +367,7 @@ bool graphable(pevsl_Data *pevsl) {
   if (!pevsl_builtin_A(pevsl) || !pevsl->Bsol) return false;
   const SVFunc f = pevsl->Bsol->func;
   if (f != pEVSL_LSPolSol && f != pEVSL_ChebIterSolv1 && f != pEVSL_ChebIterSolv2) return false;
-  return !capturing() && getenv("PEVSL_B200_GEN_GRAPH") == nullptr;
+  return !capturing() && getenv("PEVSL_B200_GEN_GRAPH_OFF") == nullptr;
 }
 
 /* choose the row kernels of A and of the B-solver's matrix before a
