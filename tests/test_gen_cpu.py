@@ -41,3 +41,83 @@ def test_lspol_approximates_the_function(lib):
         deg, mu, cc, dd = pv.lspol_coefs(kind, 80, 1e-10, 2.0, 6.0)
         p = np.polynomial.chebyshev.chebval((x - cc) / dd, mu)
         assert np.max(np.abs(p - f) / f) < 1e-11, (kind, deg)
+
+
+# ---------------------------------------------------------------- B-solvers
+# numpy restatements of the reference's B-solvers, checked against the
+# reference build's outputs (the fixture's x): the least-squares series
+# (SRC/lspolapprox.c:245-288) and both Chebyshev iterations
+# (EXTERNAL/ITERSOL/chebiter.c:121-198, 204-270).
+
+def _B512():
+    import scipy.sparse as sp
+    from checkers import laplacian
+    L = laplacian(512, 1, 1)
+    return sp.csr_matrix((L.a, L.ja, L.ia), shape=(512, 512))
+
+
+def _b():
+    return np.cos(0.1 * np.arange(512, dtype=np.float64)) + 0.5
+
+
+def lspol_apply(B, mu, cc, dd, b):
+    """y = sum_k mu_k T_k((B - cc)/dd) b by the three-term recurrence"""
+    vkm1, vk = None, b.copy()
+    y = mu[0] * vk
+    for k in range(1, len(mu)):
+        t = (1.0 if k == 1 else 2.0) / dd
+        w = (B @ vk - cc * vk) * t
+        if vkm1 is not None:
+            w = w - vkm1
+        y = y + mu[k] * w
+        vkm1, vk = vk, w
+    return y
+
+
+def chebiter1(B, lb, ub, deg, b):
+    d, c = (ub + lb) * 0.5, (ub - lb) * 0.5
+    if deg < 1:
+        return np.zeros_like(b)
+    alp = 2.0 / d
+    p = b.copy()
+    x = alp * p
+    r = b - B @ x
+    for _ in range(1, deg):
+        t = c * alp * 0.5
+        bet = t * t
+        alp = 1.0 / (d - bet)
+        p = bet * p + r
+        x = x + alp * p
+        r = b - B @ x
+    return x
+
+
+def chebiter2(B, lb, ub, deg, b):
+    theta, delta = (ub + lb) * 0.5, (ub - lb) * 0.5
+    sigma = theta / delta
+    rho = 1.0 / sigma
+    x = np.zeros_like(b)
+    r = b.copy()
+    d = r / theta
+    for _ in range(deg):
+        x = x + d
+        r = r - B @ d
+        rho1 = 1.0 / (2.0 * sigma - rho)
+        d = rho1 * rho * d + 2.0 * rho1 / delta * r
+        rho = rho1
+    return x
+
+
+@pytest.mark.parametrize("case", range(4))
+def test_lspol_restatement_matches_reference_solve(case):
+    g = golden("gen_bsolve.json")["lspol"][case]
+    x = lspol_apply(_B512(), np.array(g["mu"]), g["cc"], g["dd"], _b())
+    assert np.max(np.abs(x - g["x"])) <= 1e-13 * np.max(np.abs(g["x"]))
+
+
+@pytest.mark.parametrize("case", range(5))
+def test_chebiter_restatement_matches_reference_solve(case):
+    g = golden("gen_bsolve.json")["chebiter"][case]
+    f = chebiter1 if g["kind"] == 1 else chebiter2
+    x = f(_B512(), g["lmin"], g["lmax"], g["deg"], _b())
+    assert np.max(np.abs(x - np.array(g["x"]))) <= 1e-13 * max(np.max(np.abs(g["x"])), 1e-300)
