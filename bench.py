@@ -670,9 +670,9 @@ def kernel_case(args):
     the 3D Laplacian of side --grid:
       cheb_step  two degree-16 filter applications (32 fused filter-degree
                  launches, one vector);
-      cheb_batch --batch slices of [0.8, 4.0] with degree-16 filters in
-                 lockstep, 3 Lanczos steps (64 batched filter-degree
-                 launches);
+      cheb_batch --batch slices of [0.8, 4.0] with filters of degree
+                 --degree (16) in lockstep, 3 Lanczos steps; prints the
+                 filter's live timing per degree;
       kpm_step   8 KPM degrees for 16 vectors;
       gen_filter two degree-16 generalized filter applications on the
                  genlap24 problem scaled to --grid (B-solve: least-squares
@@ -745,6 +745,7 @@ def kernel_case(args):
         gs.free()
         print(json.dumps({"kernel_case": "gen_filter", "n": n, "status": st}))
         return
+    extra = {}
     with pv.Instance(M) as ev:
         if args.kernel_case == "cheb_step":
             r, f = pv.findpol([0.8, 4.0, 0.0, 12.0], deg_in=16)
@@ -755,12 +756,18 @@ def kernel_case(args):
             S = args.batch
             edges = np.linspace(0.8, 4.0, S + 1)
             intvs = [[edges[i], edges[i + 1], 0.0, 12.0] for i in range(S)]
-            fl = [pv.findpol(iv, deg_in=16)[1] for iv in intvs]
+            fl = [pv.findpol(iv, deg_in=args.degree)[1] for iv in intvs]
             v = np.cos(np.arange(n) * 0.1)
+            pv.load().pEVSL_B200_ResetFilterCounters()
             pv.cheblannr_batch(ev, intvs, [3] * S, 1e-8, v, fl)
+            l, b, ms = pv.filter_counters()
+            peak, kind = measured_peak()
+            extra = {"batch": S, "launches": l, "us_per_launch": 1e3 * ms / l,
+                     "bytes_per_launch": b / l, "GBps": b / ms / 1e6,
+                     "frac": b / ms / 1e6 / peak, "peak": peak, "peak_source": kind}
         else:
             ev.kpmdos(8, 1, 16, [0.80, 0.82, 0.0, 12.0])
-    print(json.dumps({"kernel_case": args.kernel_case, "n": n, "nnz": int(ia[-1])}))
+    print(json.dumps({"kernel_case": args.kernel_case, "n": n, "nnz": int(ia[-1]), **extra}))
 
 
 def main():
@@ -773,6 +780,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--path", default="batched", choices=["batched", "plain"],
                     help="batched: slices in lockstep; plain: one pEVSL_ChebLanNr per slice")
+    ap.add_argument("--degree", type=int, default=16,
+                    help="filter degree of the cheb_batch kernel case")
     ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "gen_filter",
                                               "c4_filter", "pipeline"],
                     help="run a few launches of one kernel (for ncu) and exit")

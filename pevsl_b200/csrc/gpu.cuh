@@ -235,6 +235,16 @@ int cheb_step_il(const pevsl_devcsr *A, int S, const double *Xk, const double *X
 int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
                    const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
                    const double *mu0, const double *muk, int first);
+/* degree k with a deferred accumulator: Y takes the terms of degrees
+ * k-ny+1 .. k (ny in 0..3; 0 leaves Y untouched, neither read nor
+ * written), whose vectors are X_k (Xkp1), X_{k-1} (Xk) and X_{k-2} (Xkm1);
+ * their mu rows lie at muk, muk - S, muk - 2S.  fresh: Y holds nothing yet
+ * and the sum starts from mu_0 X_0 (X_0 = Xk when ny = 1, Xkm1 when
+ * ny = 2).  The multiply-adds run in degree order, so Y ends bit-identical
+ * to the one-degree-at-a-time sum. */
+int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
+                   const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
+                   const double *mu0, const double *muk, int ny, int fresh);
 /* X[i*S + s] = xs[s][i] (S <= kMaxBatch), and ys[s][i] = X[i*S + s] for
  * the first cols columns */
 int il_pack(long n, int S, const double *const *xs, double *X);

@@ -998,16 +998,32 @@ int chebiter2_step(const pevsl_devcsr *B, const double *d, double *x, double *r,
  * the S lanes read x[col*S .. col*S+S-1] -- one contiguous segment -- so a
  * scattered column costs one L1/L2 access for all S vectors instead of one
  * per vector.  Lane s adds its row's products in entry order and applies
- * the recurrence of its own column (cheb_update_v with its own mu), which is
- * the arithmetic of the one-vector kernel, bit for bit.  X_{k+1} may alias
+ * the recurrence of its own column (cheb_update_v's arithmetic with its own
+ * mu), which is the arithmetic of the one-vector kernel, bit for bit.  X_{k+1} may alias
  * X_{k-1} (each lane reads its own element first).  The SpMV reads Xg,
- * which is Xk except in the generalized filter (Xg = B^{-1} X_k). */
+ * which is Xk except in the generalized filter (Xg = B^{-1} X_k).
+ *
+ * The accumulator may be deferred (ny, fresh: cheb_step_il_y).  A launch
+ * holds v_k (the new value), v_{k-1} and v_{k-2} in registers anyway, so
+ * the terms of up to three degrees can be added in one launch: the launches
+ * in between neither read nor write Y, 16 of 40 bytes per row and slice. */
+template <int S>
+__device__ __forceinline__ double il_accumulate(int ny, int fresh, double yold, double w,
+                                                double x, double xm1, const double *mu0,
+                                                const double *muk, int s) {
+  double y = fresh ? __dmul_rn(mu0[s], ny == 1 ? x : xm1) : yold;
+  if (ny >= 3) y = __fma_rn(muk[s - 2 * S], xm1, y);
+  if (ny >= 2) y = __fma_rn(muk[s - S], x, y);
+  return __fma_rn(muk[s], w, y);
+}
+
 template <int S>
 __global__ void __launch_bounds__(kThreads)
     k_cheb_il(int n, const int *__restrict__ ia, const int *__restrict__ ja,
               const double *__restrict__ a, const double *__restrict__ Xg,
               const double *__restrict__ Xk, const double *Xkm1, double *Xkp1, double *Y, double cc,
-              double t, const double *__restrict__ mu0, const double *__restrict__ muk, int first) {
+              double t, const double *__restrict__ mu0, const double *__restrict__ muk, int ny,
+              int fresh) {
   constexpr int RPW = 32 / S; /* rows per warp */
   const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, s = lane % S;
@@ -1016,7 +1032,6 @@ __global__ void __launch_bounds__(kThreads)
   const size_t me = (size_t)row * S + s;
   const double x = Xk[me];
   const double xm1 = Xkm1 ? Xkm1[me] : 0.0;
-  const double yold = first ? 0.0 : Y[me];
   const int e = __ldg(ia + row + 1);
   double r = 0.0;
   int j = __ldg(ia + row);
@@ -1031,10 +1046,13 @@ __global__ void __launch_bounds__(kThreads)
     r = __dadd_rn(r, __dmul_rn(a3, x3));
   }
   for (; j < e; j++) r = __dadd_rn(r, __dmul_rn(__ldg(a + j), __ldg(Xg + (size_t)__ldg(ja + j) * S + s)));
-  double w, yv;
-  cheb_update_v(r, x, xm1, Xkm1 != nullptr, cc, t, mu0[s], muk[s], first, yold, &w, &yv);
+  double w = __dmul_rn(__fma_rn(-cc, x, r), t);
+  if (Xkm1) w = __dsub_rn(w, xm1);
   Xkp1[me] = w;
-  Y[me] = yv;
+  /* y is loaded here, not before the gathers: held across the loop it
+   * takes this kernel from 32 to 40 registers (6 instead of 8 blocks per
+   * SM), and only the launches that update y load it */
+  if (ny > 0) Y[me] = il_accumulate<S>(ny, fresh, fresh ? 0.0 : Y[me], w, x, xm1, mu0, muk, s);
 }
 
 /* k_cheb_il on the packed entries (int16 column offset from the row's
@@ -1046,7 +1064,7 @@ __global__ void __launch_bounds__(kThreads)
                 const unsigned char *__restrict__ vi, const double *__restrict__ vtab, int nv,
                 const double *__restrict__ Xg, const double *__restrict__ Xk, const double *Xkm1,
                 double *Xkp1, double *Y, double cc, double t, const double *__restrict__ mu0,
-                const double *__restrict__ muk, int first) {
+                const double *__restrict__ muk, int ny, int fresh) {
   __shared__ double vt[256];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
   __syncthreads();
@@ -1059,7 +1077,7 @@ __global__ void __launch_bounds__(kThreads)
   const size_t me = (size_t)row * S + s;
   const double x = Xk[me];
   const double xm1 = Xkm1 ? Xkm1[me] : 0.0;
-  const double yold = first ? 0.0 : Y[me];
+  const double yold = (ny > 0 && !fresh) ? Y[me] : 0.0;
   const int e = __ldg(ia + row + 1);
   double r = 0.0;
   int j = __ldg(ia + row);
@@ -1077,10 +1095,10 @@ __global__ void __launch_bounds__(kThreads)
   }
   for (; j < e; j++)
     r = __dadd_rn(r, __dmul_rn(vt[__ldg(vi + j)], __ldg(Xg + (size_t)(g0 + __ldg(dj + j)) * S + s)));
-  double w, yv;
-  cheb_update_v(r, x, xm1, Xkm1 != nullptr, cc, t, mu0[s], muk[s], first, yold, &w, &yv);
+  double w = __dmul_rn(__fma_rn(-cc, x, r), t);
+  if (Xkm1) w = __dsub_rn(w, xm1);
   Xkp1[me] = w;
-  Y[me] = yv;
+  if (ny > 0) Y[me] = il_accumulate<S>(ny, fresh, yold, w, x, xm1, mu0, muk, s);
 }
 
 /* X[i*S + s] = x_s[i] and back */
@@ -1139,13 +1157,25 @@ double il_entry_bytes(const pevsl_devcsr *A) { return il_packed(A) ? 3.0 : 12.0;
 int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
                    const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
                    const double *mu0, const double *muk, int first) {
+  return cheb_step_il_y(A, S, Xg, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, 1, first);
+}
+
+int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
+                   const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
+                   const double *mu0, const double *muk, int ny, int fresh) {
+  /* the terms must exist: ny - 1 earlier mu rows (from row 0 on) and the
+   * vectors they multiply; a fresh sum starts at degree 1 or 2 */
+  if (ny < 0 || ny > 3 || muk - (size_t)(ny > 0 ? ny - 1 : 0) * S < mu0) return PEVSL_ERR_ARG;
+  if (ny == 3 && !Xkm1) return PEVSL_ERR_ARG;
+  if (fresh && (ny < 1 || ny > 2 || (ny == 2 && !Xkm1) || muk != mu0 + (size_t)ny * S))
+    return PEVSL_ERR_ARG;
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
+  cudaStream_t st = ctx().stream;
   if (il_packed(A)) {
-    cudaStream_t st = ctx().stream;
 #define PV_IL_P(SS)                                                                          \
   k_cheb_il_p<SS><<<g, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, \
-                                          Xg, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, first)
+                                          Xg, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, ny, fresh)
     switch (S) {
       case 2: PV_IL_P(2); break;
       case 4: PV_IL_P(4); break;
@@ -1156,26 +1186,17 @@ int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double 
 #undef PV_IL_P
     return launched("cheb_step_il_packed");
   }
+#define PV_IL(SS)                                                                            \
+  k_cheb_il<SS><<<g, kThreads, 0, st>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1, Y, cc, \
+                                        t, mu0, muk, ny, fresh)
   switch (S) {
-    case 2:
-      k_cheb_il<2><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
-                                                     Y, cc, t, mu0, muk, first);
-      break;
-    case 4:
-      k_cheb_il<4><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
-                                                     Y, cc, t, mu0, muk, first);
-      break;
-    case 8:
-      k_cheb_il<8><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1, Xkp1,
-                                                     Y, cc, t, mu0, muk, first);
-      break;
-    case 16:
-      k_cheb_il<16><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja, A->a, Xg, Xk, Xkm1,
-                                                      Xkp1, Y, cc, t, mu0, muk, first);
-      break;
-    default:
-      return PEVSL_ERR_ARG;
+    case 2: PV_IL(2); break;
+    case 4: PV_IL(4); break;
+    case 8: PV_IL(8); break;
+    case 16: PV_IL(16); break;
+    default: return PEVSL_ERR_ARG;
   }
+#undef PV_IL
   return launched("cheb_step_il");
 }
 
