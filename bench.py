@@ -385,7 +385,8 @@ def run_b200(args, dist):
                        "fused with the recurrence), CUDA-graph replays; one launch = one degree"
                        if gen else
                        "cheb_step_il (fused SpMV + Chebyshev recurrence, all slices per launch with "
-                       "row-interleaved vectors; one live slice: the packed one-vector kernel)"
+                       "row-interleaved vectors, filter sum updated every third degree; one live "
+                       "slice: the packed one-vector kernel)"
                        if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream, "
                        "packed entries)"),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
