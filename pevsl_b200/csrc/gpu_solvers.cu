@@ -324,8 +324,6 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
   if (ne <= 0) return 0;
   if (ne > kMaxEntries) return PEVSL_ERR_ARG;
   int st = 0, maxdeg = 0, nlive = 0;
-  bool one_matrix = true;
-  long rows = 0;
   int live[kMaxEntries];
   for (int e = 0; e < ne && !st; e++) {
     const FilterJob &J = jobs[e];
@@ -339,15 +337,11 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
       if (!st) st = vscal(J.y, n, pol->mu[0]);
       continue;
     }
-    if (J.A != jobs[0].A) one_matrix = false;
     maxdeg = PEVSL_MAX(maxdeg, pol->deg);
-    rows += n;
     if (fp32) st = cvt_f64_f32(n, J.x, (float *)J.work);
     live[nlive++] = e;
   }
   if (st || !nlive) return st;
-  (void)one_matrix;
-  (void)rows;
   /* matrix bytes: each distinct matrix once per degree, up to the largest
    * degree of its entries */
   double mat_bytes = 0.0;
