@@ -380,6 +380,21 @@ def findpol(intv, max_deg=3000, damping=2, thresh_int=0.8, thresh_ext=0.2, deg_i
     return 0, f
 
 
+def findpol_many(intvs, max_deg=3000, damping=2, thresh_int=0.8, thresh_ext=0.2):
+    """findpol for every slice, the slices on concurrent host threads
+    (pEVSL_FindPol keeps no shared state and ctypes releases the GIL, so
+    each result is the one a lone call gives).  Returns [(code, Filter or
+    None)] in slice order."""
+    from concurrent.futures import ThreadPoolExecutor
+    intvs = list(intvs)
+    if len(intvs) <= 1:
+        return [findpol(iv, max_deg, damping, thresh_int, thresh_ext) for iv in intvs]
+    workers = min(len(intvs), os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        return list(ex.map(lambda iv: findpol(iv, max_deg, damping, thresh_int, thresh_ext),
+                           intvs))
+
+
 def _polparams(f: Filter):
     pol = Polparams()
     load().pEVSL_SetPolDef(C.byref(pol))
@@ -903,17 +918,21 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
         res = SliceResult(lmin, lmax, ecount, npts, status, mu, sli)
         ev_int = int(1 + ecount / float(s.nslices))
         t = time.perf_counter()
+        # every slice's filter at once, on host threads (the same filters as
+        # designing them one slice at a time)
+        slice_ivs = [[sli[sl], sli[sl + 1], lmin, lmax] for sl in range(s.nslices)]
+        designed = findpol_many(slice_ivs, s.pol_max_deg, s.pol_damping, s.thresh_int,
+                                s.thresh_ext)
         if batched:
             nev = ev_int + 2
             mlan = min(max(5 * nev, s.mlan_min), A.n)
             filters, intvs = [], []
             for sl in range(s.nslices):
-                iv = [sli[sl], sli[sl + 1], lmin, lmax]
-                r, f = findpol(iv, s.pol_max_deg, s.pol_damping, s.thresh_int, s.thresh_ext)
+                r, f = designed[sl]
                 if r:
                     raise PevslError(f"pEVSL_FindPol returned {r} for slice {sl}")
                 filters.append(f)
-                intvs.append(iv)
+                intvs.append(slice_ivs[sl])
             r, outs = cheblannr_batch(ev, intvs, [mlan] * s.nslices, s.tol, vinit, filters)
             res.fallbacks = int(lib.pEVSL_B200_LastFallbacks())
             for f, out in zip(filters, outs):
@@ -930,8 +949,8 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
         for sl in range(0 if not batched else s.nslices, s.nslices):
             nev = ev_int + 2
             mlan = min(max(5 * nev, s.mlan_min), A.n)
-            iv = [sli[sl], sli[sl + 1], lmin, lmax]
-            r, f = findpol(iv, s.pol_max_deg, s.pol_damping, s.thresh_int, s.thresh_ext)
+            iv = slice_ivs[sl]
+            r, f = designed[sl]
             if r:
                 res.status = res.status or 300 + abs(r)
                 continue

@@ -68,6 +68,25 @@ def test_findpol_matches_reference_golden(lib):
             assert f.cc == c["cc"] and f.dd == c["dd"]
 
 
+def test_findpol_many_equals_one_at_a_time(lib):
+    """The solve driver designs every slice's filter on host threads: each
+    result is bit-for-bit the one a lone call gives, in slice order, with
+    the error codes of the slices that fail."""
+    e = np.linspace(0.8, 0.82, 5)
+    ivs = [[e[i], e[i + 1], 0.0, 12.0] for i in range(4)]
+    ivs.append([0.5, 0.50001, 0.0, 12.0])  # needs a degree above 3000
+    ivs.append([0.3, 0.2, 0.0, 12.0])  # invalid interval
+    many = pv.findpol_many(ivs)
+    for iv, (r, f) in zip(ivs, many):
+        r1, f1 = pv.findpol(iv)
+        assert r == r1
+        if r == 0:
+            assert (f.type, f.deg, f.gam, f.bar, f.cc, f.dd) == \
+                (f1.type, f1.deg, f1.gam, f1.bar, f1.cc, f1.dd)
+            assert np.array_equal(f.mu, f1.mu)
+    assert [r for r, _ in many] == [0, 0, 0, 0, -1003, -1]  # PEVSL_ERR_ARG, check_intv
+
+
 @pytest.mark.parametrize("mode", ["glibc", "gauss"])
 def test_slicer_and_filters_on_reference_moments(lib, mode):
     g = golden("lap20_kpm.json")
