@@ -589,12 +589,25 @@ def run_reference(args, dist):
                 "workloads (lap100_4slices, lap20_5slices)"}
     import multiprocessing as mp
 
-    import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian
     w = WORKLOADS[args.workload]
     n, ia, ja, a = laplacian(*w["grid"])
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so"))
     P = lambda x: x.ctypes.data_as(C.c_void_p)  # noqa: E731
+
+    def ref_findpol(intv, max_deg=3000, damping=2, thresh_int=0.8, thresh_ext=0.2):
+        """the reference's own pEVSL_SetPolDef + pEVSL_FindPol (this arm
+        runs none of the library's code)"""
+        iv = np.ascontiguousarray(intv, dtype=np.float64)
+        mu = np.zeros(max_deg + 1)
+        t, d = C.c_int(), C.c_int()
+        gam, bar, cc, dd = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        r = lib.oref_findpol(P(iv), max_deg, damping, C.c_double(thresh_int),
+                             C.c_double(thresh_ext), 0, C.byref(t), C.byref(d), C.byref(gam),
+                             C.byref(bar), C.byref(cc), C.byref(dd), P(mu))
+        if r:
+            raise RuntimeError(f"reference pEVSL_FindPol returned {r} for {list(intv)}")
+        return d.value, cc.value, dd.value, np.ascontiguousarray(mu[: d.value + 1])
     counts = REF_COUNTS.get(args.workload)
     gen = bool(w.get("gen"))
     lo, hi = C.c_double(), C.c_double()
@@ -617,10 +630,9 @@ def run_reference(args, dist):
         procs = []
         edges = np.linspace(w["a"], w["b"], nsl + 1)
         for s in range(nsl):
-            r, fil = pv.findpol([edges[s], edges[s + 1], lo.value, hi.value], 3000, 2, 0.8, 0.2)
+            deg, cc, dd, mu = ref_findpol([edges[s], edges[s + 1], lo.value, hi.value])
             p = ctx.Process(target=_ref_slice_worker,
-                            args=(q, n, ia, ja, a, fil.deg, fil.cc, fil.dd, fil.mu, 20.0,
-                                  w if gen else None))
+                            args=(q, n, ia, ja, a, deg, cc, dd, mu, 20.0, w if gen else None))
             p.start()
             procs.append(p)
         per = [q.get() for _ in procs]

@@ -1,0 +1,44 @@
+"""CPU test of bench.py's reference arm (`--impl reference`): on the small
+20^3 workload it prints one JSON line with the fields of the bench contract,
+and the process runs the reference's own code only -- this library's shared
+object is never loaded."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from conftest import ROOT
+
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so")
+
+WRAPPER = """
+import runpy, sys
+sys.argv = ["bench.py", "--impl", "reference", "--workload", "lap20_5slices",
+            "--steps", "1", "--warmup", "3"]
+runpy.run_path("bench.py", run_name="__main__")
+maps = open("/proc/self/maps").read()
+print("LOADED", "libpevsl_b200" in maps, "libpevsl_ref" in maps)
+"""
+
+
+@pytest.mark.slow
+def test_reference_arm_contract_and_isolation():
+    if not os.path.exists(REF_SO):
+        pytest.skip("reference build not available")
+    p = subprocess.run([sys.executable, "-c", WRAPPER], cwd=ROOT, capture_output=True, text=True,
+                       timeout=600)
+    assert p.returncode == 0, p.stderr[-2000:]
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    out = json.loads(lines[0])
+    assert out["impl"] == "reference" and out["unit"] == "eigenpairs/s"
+    assert out["higher_is_better"] is True and out["steps"] == 1 and out["warmup"] >= 3
+    assert out["value"] > 0 and out["cpu_baseline"]["kind"] == "reference"
+    assert out["cpu_baseline"]["value"] == out["value"] and out["cpu_baseline"]["cores"] >= 1
+    assert out["e2e"] == {"value": out["value"], "unit": "eigenpairs/s",
+                          "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    assert out["config"]["workload"] == "lap20_5slices"
+    loaded = [ln for ln in p.stdout.splitlines() if ln.startswith("LOADED")]
+    assert loaded == ["LOADED False True"]
