@@ -108,12 +108,18 @@ class Dist:
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.dev = "cpu"
         if self.world > 1:
             import datetime
 
+            import torch
             import torch.distributed as dist
             os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+            # the group carries host-side barriers and the ranks' timings only
             backend = os.environ.get("PEVSL_BENCH_BACKEND", "gloo")
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+                self.dev = torch.device("cuda", self.local)
             dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.pg = dist
 
@@ -125,7 +131,7 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64)
+        t = torch.tensor([x], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -133,7 +139,7 @@ class Dist:
         if not self.pg:
             return x
         import torch
-        t = torch.tensor([x], dtype=torch.float64)
+        t = torch.tensor([x], dtype=torch.float64, device=self.dev)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
