@@ -386,6 +386,7 @@ def findpol_many(intvs, max_deg=3000, damping=2, thresh_int=0.8, thresh_ext=0.2)
     each result is the one a lone call gives).  Returns [(code, Filter or
     None)] in slice order."""
     from concurrent.futures import ThreadPoolExecutor
+    load()  # once, before the threads
     intvs = list(intvs)
     if len(intvs) <= 1:
         return [findpol(iv, max_deg, damping, thresh_int, thresh_ext) for iv in intvs]
