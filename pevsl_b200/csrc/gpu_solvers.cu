@@ -22,7 +22,10 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <array>
+#include <atomic>
+#include <thread>
 #include <vector>
 
 #include "gpu.cuh"
@@ -1202,49 +1205,134 @@ struct SliceState {
   pevsl_Parvecs *Rvec;
 };
 
-/* Ritz pairs of one finished slice (SRC/cheblanNr.c:339-413): eigenvectors
- * of T only for Ritz values >= bar, U = V Y, normalise, W = A U, Rayleigh
- * quotients, interval check, residuals, acceptance below tol. */
-static int ritz_extract(pevsl_Data *pevsl, SliceState *S, pevsl_Parvec *vinit, long n, long ld,
-                        double tol) {
-  Ctx &c = ctx();
+/* Host threads for the per-slice host work of a lockstep group (the
+ * tridiagonal eigenproblems of the convergence tests and the Ritz
+ * extraction): PEVSL_B200_HOST_THREADS caps them (1: the calling thread
+ * only; default: every hardware thread). */
+static unsigned host_threads() {
+  static unsigned v = 0;
+  if (!v) {
+    const char *e = getenv("PEVSL_B200_HOST_THREADS");
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int r = e ? atoi(e) : 0;
+    v = r >= 1 ? std::min((unsigned)r, hw) : hw;
+  }
+  return v;
+}
+
+/* f(0), ..., f(m-1) on up to host_threads() threads, this one included,
+ * when worth is set; else in order on this thread.  f must be host-only
+ * code (no CUDA call) that writes nothing another index reads. */
+extern "C++" {
+template <class F>
+static void host_parallel(size_t m, bool worth, F f) {
+  const size_t nt = std::min<size_t>(m, host_threads());
+  if (!worth || nt <= 1) {
+    for (size_t i = 0; i < m; i++) f(i);
+    return;
+  }
+  std::atomic<size_t> next{0};
+  auto work = [&]() {
+    for (size_t i = next.fetch_add(1); i < m; i = next.fetch_add(1)) f(i);
+  };
+  std::vector<std::thread> th;
+  th.reserve(nt - 1);
+  for (size_t t = 1; t < nt; t++) {
+    try {
+      th.emplace_back(work);
+    } catch (...) {
+      break; /* no more threads: this one does the rest */
+    }
+  }
+  work();
+  for (auto &x : th) x.join();
+}
+}  // extern "C++"
+
+/* The host part of a slice's Ritz extraction: the eigenvalues of T again
+ * and the eigenvectors of those >= bar.  Host arithmetic only, so the
+ * slices of a group run it on host threads (host_parallel). */
+struct RitzHost {
+  int early = 0;  /* error that ends the extraction before any output */
+  int sel_st = 0; /* the eigenvector step failed */
+  int nsel = 0;
+  int *sel = nullptr;
+  double *Y = nullptr;
+  double secs = 0.0;
+};
+
+static void ritz_host(SliceState *S, RitzHost *R) {
   const int kdim = S->kdim, count = S->count;
-  const double bar = S->pol->bar, aa = S->intv[0], bb = S->intv[1];
-  S->nev = 0;
-  int st = 0, nsel = 0;
+  const double bar = S->pol->bar;
   const double te = pevsl_now();
   /* eigenvalues again: the last convergence test may predate the last step
    * (a maxit exit), so more Ritz values than nconv may pass the bar test;
    * the outputs hold max(nconv, nsel) pairs */
-  if (kdim > 0 && pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) return PEVSL_ERR_EIG;
-  int *sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
-  if (!sel) return PEVSL_ERR_NOMEM;
+  if (kdim > 0 && pevsl_tridiag_eig(kdim, S->dT, S->eT, S->EvalT, nullptr)) {
+    R->early = PEVSL_ERR_EIG;
+    return;
+  }
+  R->sel = (int *)malloc(sizeof(int) * (size_t)(kdim > 0 ? kdim : 1));
+  if (!R->sel) {
+    R->early = PEVSL_ERR_NOMEM;
+    return;
+  }
   for (int i = 0; i < count && kdim > 0; i++)
-    if (S->EvalT[i] >= bar) sel[nsel++] = i;
+    if (S->EvalT[i] >= bar) R->sel[R->nsel++] = i;
+  if (kdim > 0 && R->nsel > 0) {
+    R->Y = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)R->nsel);
+    if (!R->Y || pevsl_tridiag_eig_sel(kdim, S->dT, S->eT, S->EvalT, R->nsel, R->sel, R->Y))
+      R->sel_st = PEVSL_ERR_EIG;
+  }
+  R->secs = pevsl_now() - te;
+}
+
+/* Ritz pairs of one finished slice (SRC/cheblanNr.c:339-413): eigenvectors
+ * of T only for Ritz values >= bar (ritz_host, run before), U = V Y,
+ * normalise, W = A U, Rayleigh quotients, interval check, residuals,
+ * acceptance below tol.  Takes over R's buffers. */
+static int ritz_extract(pevsl_Data *pevsl, SliceState *S, RitzHost *R, pevsl_Parvec *vinit,
+                        long n, long ld, double tol) {
+  Ctx &c = ctx();
+  const int kdim = S->kdim;
+  const double aa = S->intv[0], bb = S->intv[1];
+  S->nev = 0;
+  if (R->early) {
+    free(R->sel);
+    free(R->Y);
+    R->sel = nullptr;
+    R->Y = nullptr;
+    return R->early;
+  }
+  int st = 0;
+  const int nsel = R->nsel;
+  int *sel = R->sel;
+  double *Y = R->Y;
+  R->sel = nullptr;
+  R->Y = nullptr;
+  const double te = pevsl_now();
   const int nout = PEVSL_MAX(S->nconv, nsel);
   S->Lam = (double *)malloc(sizeof(double) * (size_t)(nout > 0 ? nout : 1));
   S->res = (double *)malloc(sizeof(double) * (size_t)(nout > 0 ? nout : 1));
   S->Rvec = (pevsl_Parvecs *)calloc(1, sizeof(pevsl_Parvecs));
   if (!S->Lam || !S->res || !S->Rvec) {
     free(sel);
+    free(Y);
     return PEVSL_ERR_NOMEM;
   }
   pEVSL_ParvecsDuplParvec(vinit, nout, (int)n, S->Rvec);
   if (nout > 0 && !S->Rvec->data) {
     free(sel);
+    free(Y);
     return PEVSL_ERR_NOMEM;
   }
   if (kdim <= 0) {
     free(sel);
+    free(Y);
     return 0;
   }
-  double *Y = nullptr;
-  if (nsel > 0) {
-    Y = (double *)malloc(sizeof(double) * (size_t)kdim * (size_t)nsel);
-    st = Y ? pevsl_tridiag_eig_sel(kdim, S->dT, S->eT, S->EvalT, nsel, sel, Y) : PEVSL_ERR_NOMEM;
-    if (st) st = PEVSL_ERR_EIG;
-  }
-  pevsl->stats->t_eig += pevsl_now() - te;
+  st = R->sel_st;
+  pevsl->stats->t_eig += R->secs + (pevsl_now() - te);
   if (!st && nsel > 0) {
     double *U = (double *)ws(WS_RITZ, sizeof(double) * (size_t)ld * (size_t)nsel);
     double *W = (double *)ws(WS_RITZ2, sizeof(double) * (size_t)ld * (size_t)nsel);
@@ -1787,18 +1875,30 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
         return b_scal(len, cs, sc, v, mask);
       });
     if (st) break;
-    /* restricted-trace convergence test (SRC/cheblanNr.c:293-332) */
-    for (int s = 0; s < ns; s++) {
-      if (!act[s]) continue;
-      SliceState *S = &SL[s];
-      if ((k < 30 || (k - 30) % 20 != 0) && k != S->maxit - 1) continue;
-      S->kdim = k + 1;
+    /* restricted-trace convergence test (SRC/cheblanNr.c:293-332); the
+     * eigenvalues of the testing slices' T are computed first, on host
+     * threads (each slice's own arithmetic, so the same values), then the
+     * tests run in slice order */
+    std::vector<int> tests;
+    for (int s = 0; s < ns; s++)
+      if (act[s] && !((k < 30 || (k - 30) % 20 != 0) && k != SL[s].maxit - 1)) tests.push_back(s);
+    std::vector<int> eig_st(tests.size(), 0);
+    std::vector<double> eig_secs(tests.size(), 0.0);
+    host_parallel(tests.size(), k + 1 >= 64, [&](size_t i) {
+      SliceState *S = &SL[tests[i]];
       const double te = pevsl_now();
-      if (pevsl_tridiag_eig(S->kdim, S->dT, S->eT, S->EvalT, nullptr)) {
+      eig_st[i] = pevsl_tridiag_eig(k + 1, S->dT, S->eT, S->EvalT, nullptr);
+      eig_secs[i] = pevsl_now() - te;
+    });
+    for (size_t ti = 0; ti < tests.size(); ti++) {
+      const int s = tests[ti];
+      SliceState *S = &SL[s];
+      S->kdim = k + 1;
+      if (eig_st[ti]) {
         st = PEVSL_ERR_EIG;
         break;
       }
-      S->pevsl->stats->t_eig += pevsl_now() - te;
+      S->pevsl->stats->t_eig += eig_secs[ti];
       S->count = S->kdim;
       double tr1 = 0.0;
       S->nconv = 0;
@@ -1829,13 +1929,30 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
   }
   cudaEventRecord(e_all1, c.stream);
   const double tr_start = pevsl_now();
+  /* the host part of every finished slice's Ritz extraction first, on host
+   * threads; then the device part slice by slice */
+  std::vector<RitzHost> rh((size_t)ns);
+  if (!st && !mixed) {
+    std::vector<int> fin;
+    int kmax = 0;
+    for (int s = 0; s < ns; s++)
+      if (!SL[s].done && !SL[s].status) {
+        fin.push_back(s);
+        kmax = PEVSL_MAX(kmax, SL[s].kdim);
+      }
+    host_parallel(fin.size(), kmax >= 64, [&](size_t i) { ritz_host(&SL[fin[i]], &rh[fin[i]]); });
+  }
   for (int s = 0; s < ns && !st; s++) {
     SliceState *S = &SL[s];
     if (S->done || S->status) continue;
     S->its = S->kdim;
     const int rs = mixed ? ritz_refine(S->pevsl, S, S->vinit, S->n, S->ld, tol, guard, passes)
-                         : ritz_extract(S->pevsl, S, S->vinit, S->n, S->ld, tol);
+                         : ritz_extract(S->pevsl, S, &rh[s], S->vinit, S->n, S->ld, tol);
     if (rs) S->status = rs;
+  }
+  for (RitzHost &R : rh) {
+    free(R.sel);
+    free(R.Y);
   }
   for (int s = 0; s < ns; s++) SL[s].pevsl->stats->t_ritz = pevsl_now() - tr_start;
   cudaEventSynchronize(e_all1);

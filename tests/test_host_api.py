@@ -87,6 +87,41 @@ def test_findpol_many_equals_one_at_a_time(lib):
     assert [r for r, _ in many] == [0, 0, 0, 0, -1003, -1]  # PEVSL_ERR_ARG, check_intv
 
 
+def test_host_eigensolvers_same_bits_on_concurrent_threads(lib):
+    """A lockstep group solves its slices' tridiagonal eigenproblems (the
+    convergence tests and the Ritz vectors) on concurrent host threads:
+    pevsl_tridiag_eig and pevsl_tridiag_eig_sel keep no shared state, so
+    each result is bit-for-bit the one a lone call gives."""
+    from concurrent.futures import ThreadPoolExecutor
+    dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+    rng = np.random.default_rng(7)
+    cases = []
+    for n in (64, 151, 200, 257, 300, 331, 400, 531):
+        d = rng.uniform(-1.0, 1.0, n)
+        e = rng.uniform(0.05, 0.5, n)
+        cases.append((n, d, e, np.arange(n - n // 5, n, dtype=np.int32)))
+
+    def solve(c):
+        n, d, e, sel = c
+        w, w2 = np.zeros(n), np.zeros(n)
+        Z = np.zeros(n * len(sel))
+        r1 = lib.pevsl_tridiag_eig(n, d.ctypes.data_as(dp), e.ctypes.data_as(dp),
+                                   w.ctypes.data_as(dp), None)
+        r2 = lib.pevsl_tridiag_eig_sel(n, d.ctypes.data_as(dp), e.ctypes.data_as(dp),
+                                       w2.ctypes.data_as(dp), len(sel), sel.ctypes.data_as(ip),
+                                       Z.ctypes.data_as(dp))
+        return r1, r2, w, w2, Z
+
+    lone = [solve(c) for c in cases]
+    with ThreadPoolExecutor(8) as ex:
+        together = list(ex.map(solve, cases * 3))
+    for i, t in enumerate(together):
+        a = lone[i % len(cases)]
+        assert t[0] == a[0] == 0 and t[1] == a[1] == 0
+        for x, y in zip(t[2:], a[2:]):
+            assert np.array_equal(x, y)
+
+
 @pytest.mark.parametrize("mode", ["glibc", "gauss"])
 def test_slicer_and_filters_on_reference_moments(lib, mode):
     g = golden("lap20_kpm.json")
