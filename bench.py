@@ -701,8 +701,7 @@ def kernel_case(args):
                  a degree-16 filter on one slice, then on 16 interior slices
                  in lockstep; prints the filter's live timing (CUDA events)
                  and HBM fraction per degree;
-    (the filters are forced to a small degree on wide intervals: a forced
-    degree below a slice's starting degree is an error)
+    (a forced degree d gives a filter of degree d - 1, as in the reference)
       pipeline   one whole batched solve of --workload (for launch lists)."""
     import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian

@@ -541,7 +541,9 @@ static int findpol(const double *intv, orc_pol *pol) {
   if (nitv == 1) {
     chext(pol, aa, bb);
   } else {
-    min_deg = 2 + (int)(0.5 / (bb - aa));
+    /* SRC/chebpol.c:434 writes 2 + (int) 0.5/(bb-aa): the cast applies to
+     * 0.5, so the search starts at degree 2 */
+    min_deg = 2;
     thresh = pol->thresh_int;
     if (pol->deg > 0) {
       thresh = -1;

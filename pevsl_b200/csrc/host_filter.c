@@ -186,9 +186,14 @@ static int balance_centre(int m, const double *v, const double *jac, double tha,
 
 /* Filter for the slice [intv0, intv1] of the spectrum [intv2, intv3]
  * (SRC/chebpol.c:359-484).  Returns -1 for an invalid interval, and
- * PEVSL_ERR_ARG when the slice is so narrow that the starting degree of the
- * search, 2 + 0.5 / (normalised width), is not below max_deg (or below the
- * forced degree): the reference then writes past its max_deg + 1 arrays. */
+ * PEVSL_ERR_ARG when max_deg (or the forced degree) is 2 or less, which
+ * leaves no degree to search (the reference then scales by t = 0).
+ *
+ * The degree search starts at 2 for every slice.  The reference writes its
+ * start as 2 + (int) 0.5/(bb-aa) (SRC/chebpol.c:434), where the cast
+ * applies to 0.5 alone, so its value is 2; the search here starts there too,
+ * which gives the reference's degree whenever a degree below
+ * 2 + 0.5/(bb-aa) already meets the threshold. */
 int pEVSL_FindPol(double *intv, pevsl_Polparams *pol) {
   if (pevsl_check_intv(intv, stdout) < 0) return -1;
   int max_deg = pol->max_deg;
@@ -227,21 +232,19 @@ int pEVSL_FindPol(double *intv, pevsl_Polparams *pol) {
     const double ends[2] = {aa, bb};
     double vals[2] = {0.0, 0.0}, t = 0.0, thc = 0.0, gam = 0.0;
     double thresh = pol->thresh_int;
-    const double start = 2.0 + 0.5 / (bb - aa);
+    const int min_deg = 2;
     if (pol->deg > 0) {
       thresh = -1;
       max_deg = pol->deg;
     }
-    if (!(start < (double)max_deg)) {
-      fprintf(stdout, " FindPol: slice (%e, %e) needs a degree above %d\n", intv[0], intv[1],
-              max_deg);
+    if (max_deg <= min_deg) {
+      fprintf(stdout, " FindPol: degree limit %d leaves no degree to search\n", max_deg);
       free(mu);
       free(v);
       free(jac);
       pol->mu = NULL;
       return PEVSL_ERR_ARG;
     }
-    const int min_deg = (int)start;
     for (int j = 0; j < min_deg; j++) v[j] = cos(j * thb) - cos(j * tha);
     int m;
     for (m = min_deg; m < max_deg; m++) {

@@ -6,7 +6,7 @@ reference is mounted, never on a GPU box) and writes small JSON files that
 the CPU tests use to pin the oracle restatement and the GPU tests use as
 known answers.  Floats are written with repr() so they round-trip exactly.
 
-    python tests/golden/make_golden.py [mm | gen]
+    python tests/golden/make_golden.py [mm | gen | findpol]
 """
 from __future__ import annotations
 
@@ -74,23 +74,7 @@ def main():
     dump("lap20_kpm.json", dict(grid=[20, 20, 20], intv=intv, Mdeg=300, damping=1, nvec=60,
                                 seed=0, cases=kpm))
 
-    # 3. Filter design edge cases: end intervals (chext), forced degree,
-    #    every damping type, invalid intervals (check_intv codes)
-    cases = []
-    for intv_c, kw in (([0.0, 0.5, 0.0, 12.0], {}), ([-1.0, 0.5, 0.0, 12.0], {}),
-                       ([11.0, 12.0, 0.0, 12.0], {}), ([11.5, 13.0, 0.0, 12.0], {}),
-                       ([0.8, 0.82, 0.0, 12.0], {}), ([3.0, 3.5, 0.0, 12.0], {"damping": 0}),
-                       ([3.0, 3.5, 0.0, 12.0], {"damping": 1}), ([3.0, 3.5, 0.0, 12.0], {"deg_in": 40}),
-                       ([0.0, 0.5, 0.0, 12.0], {"deg_in": 25}),
-                       ([2.0, 2.5, 0.0, 8.0], {"thresh_int": 0.6, "thresh_ext": 0.15}),
-                       ([1.0, 0.5, 0.0, 12.0], {}), ([13.0, 14.0, 0.0, 12.0], {})):
-        r, p = ref.findpol(intv_c, **kw)
-        c = dict(intv=intv_c, kw=kw, status=r)
-        if p is not None:
-            c.update(type=p["type"], deg=p["deg"], gam=p["gam"], bar=p["bar"], cc=p["cc"],
-                     dd=p["dd"], mu=fl(p["mu"]))
-        cases.append(c)
-    dump("findpol_cases.json", dict(cases=cases))
+    findpol_cases(ref)
 
     # 4. Slicer edge cases: one slice, many slices, invalid interval
     ref.set_rng(1, 7)
@@ -156,6 +140,36 @@ def main():
                                      tol=1e-8, v0="cos(0.37 i)", seed=9, deg=pol["deg"],
                                      status=out["status"], nev=out["nev"], its=out["its"],
                                      lam=fl(out["lam"]), res=fl(out["res"])))
+
+
+def findpol_cases(ref):
+    """Filter design edge cases: end intervals (chext), forced degree, every
+    damping type, invalid intervals (check_intv codes), and slices on which
+    a degree below 2 + 0.5/(normalised width) already meets the threshold
+    (the reference's search starts at degree 2, SRC/chebpol.c:434): three
+    slices of a random-coefficient 41^3 Laplacian's spectrum bound [0, 24]
+    and a slice of width 1.4e-4 (normalised) with max_deg 3000, 20000 and a
+    forced degree 100."""
+    narrow = [0.4845065036442954, 0.4850594098995861, 0.4435124791600489, 8.445429558871442]
+    cases = []
+    for intv_c, kw in (([0.0, 0.5, 0.0, 12.0], {}), ([-1.0, 0.5, 0.0, 12.0], {}),
+                       ([11.0, 12.0, 0.0, 12.0], {}), ([11.5, 13.0, 0.0, 12.0], {}),
+                       ([0.8, 0.82, 0.0, 12.0], {}), ([3.0, 3.5, 0.0, 12.0], {"damping": 0}),
+                       ([3.0, 3.5, 0.0, 12.0], {"damping": 1}), ([3.0, 3.5, 0.0, 12.0], {"deg_in": 40}),
+                       ([0.0, 0.5, 0.0, 12.0], {"deg_in": 25}),
+                       ([2.0, 2.5, 0.0, 8.0], {"thresh_int": 0.6, "thresh_ext": 0.15}),
+                       ([1.0, 0.5, 0.0, 12.0], {}), ([13.0, 14.0, 0.0, 12.0], {}),
+                       ([0.10, 0.123, 0.0, 24.0], {}), ([0.123, 0.143, 0.0, 24.0], {}),
+                       ([0.143, 0.165, 0.0, 24.0], {}),
+                       (narrow, {"max_deg": 3000}), (narrow, {"max_deg": 20000}),
+                       (narrow, {"max_deg": 3000, "deg_in": 100})):
+        r, p = ref.findpol(intv_c, **kw)
+        c = dict(intv=intv_c, kw=kw, status=r)
+        if p is not None:
+            c.update(type=p["type"], deg=p["deg"], gam=p["gam"], bar=p["bar"], cc=p["cc"],
+                     dd=p["dd"], mu=fl(p["mu"]))
+        cases.append(c)
+    dump("findpol_cases.json", dict(cases=cases))
 
 
 def mm_case(refdir="/root/reference"):
@@ -248,6 +262,8 @@ def write_matfile(path, mtx, intervals):
 if __name__ == "__main__":
     if sys.argv[1:] == ["mm"]:
         mm_case()
+    elif sys.argv[1:] == ["findpol"]:
+        findpol_cases(Checker("ref"))
     elif sys.argv[1:] == ["gen"]:
         gen_case()
     else:
