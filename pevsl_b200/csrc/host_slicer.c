@@ -74,6 +74,9 @@ int pEVSL_SpslicerKpm(double *sli, double *mu, int Mdeg, double *intv, int n_int
   while (++ls < n_int) {
     while (ii < npts && yi[ii] < target) ii++;
     if (ii == npts) break;
+    /* ii > 0: when the first grid point already reaches the target (a
+     * moment set whose mass is not positive) the reference compares with
+     * yi[-1], outside its array; here that grid point is kept */
     if (ii > 0 && target - yi[ii - 1] < yi[ii] - target) ii--;
     sli[ls] = ctr + wid * xi[ii];
     target = yi[ii] + (yi[npts - 1] - yi[ii]) / (n_int - ls);

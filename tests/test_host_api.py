@@ -205,3 +205,70 @@ def test_copy_eigenvectors_rejects_bad_arguments(lib):
     assert f(C.byref(W), 2, p, 9) == pv.ERR_ARG
     assert f(C.byref(W), -1, p, 10) == pv.ERR_ARG
     assert f(C.byref(W), 0, p, 10) == 0
+
+
+# ------------------------------------------------------- randomized, against the reference build
+def _random_filter_requests(count, seed):
+    rng = np.random.default_rng(seed)
+    for _ in range(count):
+        lmin = rng.uniform(-2.0, 1.0)
+        lmax = lmin + rng.uniform(1.0, 20.0)
+        w = (lmax - lmin) * 10 ** rng.uniform(-3.5, -0.3)
+        a = rng.uniform(lmin, lmax - 0.5 * w)
+        kw = dict(max_deg=int(rng.choice([200, 1000, 3000])), damping=int(rng.integers(0, 3)),
+                  thresh_int=float(rng.choice([0.6, 0.8, 0.9])), thresh_ext=0.2)
+        yield [a, a + w, lmin, lmax], kw
+
+
+def test_findpol_random_against_reference(lib, reference):
+    """300 random filter requests (middle and end intervals, widths from
+    3e-4 to 0.5 of the spectrum, every damping, three thresholds): status,
+    type and degree equal to the reference build's, values to 1e-15."""
+    for iv, kw in _random_filter_requests(300, 11):
+        r1, p = reference.findpol(iv, **kw)
+        r2, f = pv.findpol(iv, **kw)
+        assert r1 == r2, (iv, kw)
+        if r1 == 0:
+            assert (f.type, f.deg) == (p["type"], p["deg"]), (iv, kw)
+            assert abs(f.gam - p["gam"]) <= 1e-15 and abs(f.bar - p["bar"]) <= 1e-15
+            assert np.max(np.abs(f.mu - p["mu"])) <= 1e-15 * np.max(np.abs(p["mu"]))
+
+
+def test_spslicer_random_against_reference(lib, reference):
+    """200 random KPM slicing requests on moments of a genuine density
+    (Jackson-damped sums over random eigenvalues): status and every slice
+    end bit for bit as the reference build's."""
+    rng = np.random.default_rng(5)
+    for _ in range(200):
+        Mdeg = int(rng.integers(10, 400))
+        lam = np.cos(rng.uniform(0.0, np.pi, int(rng.integers(5, 500))))
+        k = np.arange(Mdeg + 1)
+        th = np.pi / (Mdeg + 2)
+        jac = ((1 - k / (Mdeg + 2)) * np.sin(th) * np.cos(k * th)
+               + np.cos(th) * np.sin(k * th) / (Mdeg + 2)) / np.sin(th)
+        mu = np.cos(np.outer(k, np.arccos(lam))).sum(axis=1) * jac * 2 / np.pi
+        mu[0] /= 2
+        lmin = rng.uniform(-3.0, 0.0)
+        lmax = lmin + rng.uniform(1.0, 20.0)
+        a = rng.uniform(lmin - 0.5, lmax)
+        iv = [a, a + rng.uniform(0.001, lmax - lmin), lmin, lmax]
+        n_int = int(rng.integers(1, 12))
+        npts = int(rng.integers(2 * n_int - 1, 3000))
+        r1, s1 = reference.spslicer_kpm(mu, Mdeg, iv, n_int, npts)
+        r2, s2 = pv.spslicer_kpm(mu, Mdeg, iv, n_int, npts)
+        assert r1 == r2
+        if r1 >= 0:
+            assert np.array_equal(np.asarray(s1), np.asarray(s2))
+
+
+def test_spslicer_lan_random_against_reference(lib, reference):
+    """200 random sampled densities (3 to 600 points, 1 to 14 slices): the
+    Lanczos-DOS slice ends bit for bit as the reference build's."""
+    rng = np.random.default_rng(9)
+    for _ in range(200):
+        npts, n_int = int(rng.integers(3, 600)), int(rng.integers(1, 15))
+        x = np.sort(rng.uniform(-2.0, 5.0, npts))
+        y = np.abs(rng.standard_normal(npts)) * rng.uniform(0.1, 10.0)
+        s1 = reference.spslicer_lan(x, y, n_int)
+        s2 = pv.spslicer_lan(x, y.copy(), n_int)
+        assert np.array_equal(np.asarray(s1), np.asarray(s2))
