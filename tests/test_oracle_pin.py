@@ -181,3 +181,41 @@ def test_breakdown_restart_golden(oracle):
     out = oracle.cheblannr(D, g["intv"], g["maxit"], g["tol"], np.cos(np.arange(n) * 0.37), pol)
     assert (out["status"], out["nev"], out["its"]) == (g["status"], g["nev"], g["its"])
     assert rel(out["lam"], g["lam"]) <= 1e-10
+
+
+@pytest.mark.slow
+def test_random_pipelines_against_reference(oracle, reference):
+    """Twelve random whole runs (2D and 3D Laplacians of 216 to 1728 rows,
+    1 to 4 slices, either bounds mode and DOS type, both random streams)
+    through the oracle and the reference build: status, slice ends (1e-12),
+    filter types and degrees, eigenvalue counts and eigenvalues (1e-10) as
+    the reference's.  Lanczos step counts may differ by whole test cycles
+    of 20 steps: the restricted-trace test compares a change with 2e-12,
+    and where that change sits within rounding the two builds' dot products
+    and tridiagonal eigensolvers (LAPACK DSTEV there) decide differently."""
+    rng = np.random.default_rng(3)
+    cycles = 0
+    for _ in range(12):
+        d3 = rng.random() < 0.5
+        g = (int(rng.integers(6, 13)),) * 3 if d3 else \
+            (int(rng.integers(12, 40)), int(rng.integers(12, 40)), 1)
+        top = 12.0 if d3 else 8.0
+        a = float(rng.uniform(0.2, top * 0.6))
+        b = a + float(rng.uniform(0.1, 1.2))
+        spec = RunSpec(a_lo=a, b_hi=b, nslices=int(rng.integers(1, 5)),
+                       bounds_mode=int(rng.integers(0, 2)), lmin=0.0, lmax=top,
+                       dos_type=int(rng.integers(0, 2)), Mdeg=int(rng.choice([100, 200, 300])),
+                       nvec=int(rng.choice([10, 20, 40])), rng_mode=int(rng.integers(0, 2)),
+                       seed=int(rng.integers(0, 100)), thresh_int=float(rng.choice([0.6, 0.8])))
+        A = laplacian(*g)
+        r1, r2 = reference.pipeline(A, spec), oracle.pipeline(A, spec)
+        assert r1.status == r2.status
+        assert np.max(np.abs(r1.sli - r2.sli)) <= 1e-12 * max(1.0, np.max(np.abs(r1.sli)))
+        assert list(r1.ptype) == list(r2.ptype) and list(r1.deg) == list(r2.deg)
+        assert list(r1.nev) == list(r2.nev)
+        for x, y, i1, i2 in zip(r1.lam, r2.lam, r1.its, r2.its):
+            assert (i1 - i2) % 20 == 0
+            cycles += i1 != i2
+            if len(x):
+                assert np.max(np.abs(np.sort(x) - np.sort(y))) <= 1e-10 * np.max(np.abs(x))
+    assert cycles <= 3
