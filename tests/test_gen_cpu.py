@@ -121,3 +121,22 @@ def test_chebiter_restatement_matches_reference_solve(case):
     f = chebiter1 if g["kind"] == 1 else chebiter2
     x = f(_B512(), g["lmin"], g["lmax"], g["deg"], _b())
     assert np.max(np.abs(x - np.array(g["x"]))) <= 1e-13 * max(np.max(np.abs(g["x"])), 1e-300)
+
+
+def test_lspol_random_against_reference(lib, reference):
+    """120 random least-squares requests (1/x and 1/sqrt(x), max_deg 5 to
+    200, tolerances 1e-12 to 1e-2, intervals with ratios 1.5 to 400):
+    degree, cc, dd and every coefficient bit for bit as the reference
+    build's."""
+    from checkers import laplacian
+    B, b = laplacian(64, 1, 1), np.ones(64)
+    rng = np.random.default_rng(2)
+    for _ in range(120):
+        kind, md = int(rng.integers(0, 2)), int(rng.integers(5, 200))
+        tol = 10 ** rng.uniform(-12, -2)
+        lo = rng.uniform(0.01, 3.0)
+        hi = lo * rng.uniform(1.5, 400.0)
+        d1, mu1, cc1, dd1, _ = reference.lspol(kind, md, tol, lo, hi, B, b)
+        d2, mu2, cc2, dd2 = pv.lspol_coefs(kind, md, tol, lo, hi)
+        assert (d1, cc1, dd1) == (d2, cc2, dd2)
+        assert np.array_equal(mu1, np.asarray(mu2)[: d1 + 1])
