@@ -288,7 +288,9 @@ typedef struct _pevsl_Data {
 
 /* Filter design — SRC/chebpol.c (INC/pevsl.h:12-14). */
 void pEVSL_SetPolDef(pevsl_Polparams *pol);       /* chebpol.c:10   */
-int pEVSL_FindPol(double *intv, pevsl_Polparams *pol); /* chebpol.c:359 */
+/* chebpol.c:359; the degree search runs from 2 to max_deg (or the forced
+ * degree) as in the reference; a limit of 2 or less returns PEVSL_ERR_ARG */
+int pEVSL_FindPol(double *intv, pevsl_Polparams *pol);
 void pEVSL_FreePol(pevsl_Polparams *pol);         /* chebpol.c:491  */
 
 /* KPM density of states — SRC/kpmdos.c:36 (INC/pevsl.h:17-18). */
