@@ -219,3 +219,44 @@ def test_random_pipelines_against_reference(oracle, reference):
             if len(x):
                 assert np.max(np.abs(np.sort(x) - np.sort(y))) <= 1e-10 * np.max(np.abs(x))
     assert cycles <= 3
+
+
+@pytest.mark.slow
+def test_random_matrix_pipelines_against_reference(oracle, reference):
+    """Whole runs on matrices other than the constant-coefficient Laplacian:
+    random sparse symmetric (800 to 3000 rows, offsets up to 300) and
+    random-coefficient 3D Laplacians (8^3 to 12^3), bounds by thick-restart
+    Lanczos, KPM or Lanczos DOS, 1 to 3 slices.  Bounds to 1e-12
+    (relative), slice ends to 1e-12, filter degrees, eigenvalue counts and
+    eigenvalues (1e-10) as the reference build's; step counts up to whole
+    convergence-test cycles."""
+    from pevsl_b200.problems import random_coef_laplacian, random_sparse_symmetric
+
+    from checkers import Csr
+    rng = np.random.default_rng(4)
+    for t in range(6):
+        if t % 2 == 0:
+            n, ia, ja, a = random_sparse_symmetric(int(rng.integers(800, 3000)), 8,
+                                                   int(rng.integers(10, 300)),
+                                                   int(rng.integers(0, 99)))
+        else:
+            g = int(rng.integers(8, 13))
+            n, ia, ja, a = random_coef_laplacian(g, g, g, seed=int(rng.integers(0, 99)))
+        A = Csr(n, ia, ja, a)
+        _, lo, hi = reference.lantrbounds(A, 50, 200, 1e-8, np.cos(np.arange(n) * 0.37))
+        w = hi - lo
+        aa = lo + w * rng.uniform(0.1, 0.6)
+        spec = RunSpec(a_lo=aa, b_hi=aa + w * rng.uniform(0.02, 0.1),
+                       nslices=int(rng.integers(1, 4)), bounds_mode=1,
+                       dos_type=int(rng.integers(0, 2)), Mdeg=200, nvec=20,
+                       rng_mode=int(rng.integers(0, 2)), seed=t)
+        r1, r2 = reference.pipeline(A, spec), oracle.pipeline(A, spec)
+        assert r1.status == r2.status == 0
+        scale = max(abs(r1.lmin), abs(r1.lmax))
+        assert abs(r1.lmin - r2.lmin) <= 1e-12 * scale and abs(r1.lmax - r2.lmax) <= 1e-12 * scale
+        assert np.max(np.abs(r1.sli - r2.sli)) <= 1e-12 * scale
+        assert list(r1.deg) == list(r2.deg) and list(r1.nev) == list(r2.nev)
+        for x, y, i1, i2 in zip(r1.lam, r2.lam, r1.its, r2.its):
+            assert (i1 - i2) % 20 == 0
+            if len(x):
+                assert np.max(np.abs(np.sort(x) - np.sort(y))) <= 1e-10 * np.max(np.abs(x))
