@@ -272,3 +272,40 @@ def test_spslicer_lan_random_against_reference(lib, reference):
         s1 = reference.spslicer_lan(x, y, n_int)
         s2 = pv.spslicer_lan(x, y.copy(), n_int)
         assert np.array_equal(np.asarray(s1), np.asarray(s2))
+
+
+def test_coo_to_csr_and_host_matvec_against_reference(lib, reference):
+    """pEVSL_CooToCsr (0- and 1-based input, duplicates, empty rows) and the
+    host pEVSL_Matvec on its result: arrays and products bit for bit as the
+    reference build's (SRC/spmat.c), on 300 random matrices."""
+    class Coo(C.Structure):
+        _fields_ = [("nrows", C.c_int), ("ncols", C.c_int), ("nnz", C.c_int),
+                    ("ir", C.POINTER(C.c_int)), ("jc", C.POINTER(C.c_int)),
+                    ("vv", C.POINTER(C.c_double))]
+
+    ip, dp = C.POINTER(C.c_int), C.POINTER(C.c_double)
+    rlib = reference.lib
+    rng = np.random.default_rng(1)
+    for _ in range(300):
+        nr, nc, nnz = int(rng.integers(1, 60)), int(rng.integers(1, 60)), int(rng.integers(0, 300))
+        base = int(rng.integers(0, 2))
+        ir = (rng.integers(0, nr, nnz) + base).astype(np.int32)
+        jc = (rng.integers(0, nc, nnz) + base).astype(np.int32)
+        vv = rng.standard_normal(nnz)
+        x = rng.standard_normal(nc)
+        outs = []
+        for L in (rlib, lib):
+            coo = Coo(nr, nc, nnz, ir.ctypes.data_as(ip), jc.ctypes.data_as(ip),
+                      vv.ctypes.data_as(dp))
+            csr = pv.Csr()
+            r = L.pEVSL_CooToCsr(base, C.byref(coo), C.byref(csr))
+            ia = np.ctypeslib.as_array(csr.ia, shape=(nr + 1,)).copy()
+            m = int(ia[-1])
+            ja = np.ctypeslib.as_array(csr.ja, shape=(m,)).copy() if m else np.zeros(0, np.int32)
+            a = np.ctypeslib.as_array(csr.a, shape=(m,)).copy() if m else np.zeros(0)
+            y = np.zeros(nr)
+            L.pEVSL_Matvec(C.byref(csr), x.ctypes.data_as(dp), y.ctypes.data_as(dp))
+            L.pEVSL_FreeCsr(C.byref(csr))
+            outs.append((r, ia, ja, a, y))
+        for u, w in zip(*outs):
+            assert np.array_equal(np.asarray(u), np.asarray(w))
