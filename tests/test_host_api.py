@@ -309,3 +309,27 @@ def test_coo_to_csr_and_host_matvec_against_reference(lib, reference):
             outs.append((r, ia, ja, a, y))
         for u, w in zip(*outs):
             assert np.array_equal(np.asarray(u), np.asarray(w))
+
+
+def test_findpol_end_intervals_random_against_reference(lib, reference):
+    """200 random end-interval filters (SRC/chebpol.c:166-255; the slice at
+    or beyond either end of the spectrum bounds, forced degrees among them):
+    type, degree and values as the reference build's."""
+    rng = np.random.default_rng(21)
+    for t in range(200):
+        lmin = rng.uniform(-2.0, 1.0)
+        lmax = lmin + rng.uniform(1.0, 20.0)
+        w = (lmax - lmin) * 10 ** rng.uniform(-3.0, -0.2)
+        if t % 2 == 0:
+            iv = [lmin - rng.uniform(0.0, 1.0) * (t % 4 == 0), lmin + w, lmin, lmax]
+        else:
+            iv = [lmax - w, lmax + rng.uniform(0.0, 1.0) * (t % 4 == 1), lmin, lmax]
+        kw = dict(max_deg=int(rng.choice([200, 1000, 3000])), damping=int(rng.integers(0, 3)),
+                  thresh_ext=float(rng.choice([0.1, 0.2, 0.3])),
+                  deg_in=int(rng.choice([0, 0, 0, 50])))
+        r1, p = reference.findpol(iv, **kw)
+        r2, f = pv.findpol(iv, **kw)
+        assert r1 == r2 == 0
+        assert (f.type, f.deg) == (p["type"], p["deg"]) and f.type == (1 if t % 2 == 0 else 2)
+        assert abs(f.gam - p["gam"]) <= 1e-15 and abs(f.bar - p["bar"]) <= 1e-15 * max(1, abs(p["bar"]))
+        assert np.max(np.abs(f.mu - p["mu"])) <= 1e-14 * np.max(np.abs(p["mu"]))
