@@ -1236,7 +1236,6 @@ static void host_parallel(size_t m, bool worth, F f) {
     for (size_t i = next.fetch_add(1); i < m; i = next.fetch_add(1)) f(i);
   };
   std::vector<std::thread> th;
-  th.reserve(nt - 1);
   for (size_t t = 1; t < nt; t++) {
     try {
       th.emplace_back(work);
