@@ -274,46 +274,65 @@ def run_b200(args, dist):
     nnz = int(ia[-1])
     seed = 1000 * dist.rank
     spec = slice_run(w, seed)
-    # pinned host copies of the inputs for the end-to-end leg
+    # pinned host copies of the inputs: every step uploads them
     ia_p, p1 = pv.pinned_empty(n + 1, np.int32)
     ja_p, p2 = pv.pinned_empty(nnz, np.int32)
     a_p, p3 = pv.pinned_empty(nnz, np.float64)
     ia_p[:], ja_p[:], a_p[:] = ia, ja, a
-    M = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
     gen = bool(w.get("gen"))
-    gs, bpins = None, []
+    bpins = []
     if gen:
         _, ib, jb, bv = laplacian(n, 1, 1)
         bpins = [pv.pinned_empty(n + 1, np.int32), pv.pinned_empty(len(jb), np.int32),
                  pv.pinned_empty(len(jb), np.float64)]
         bpins[0][0][:], bpins[1][0][:], bpins[2][0][:] = ib, jb, bv
-        gs = GenSetup(w, n, (bpins[0][0], bpins[1][0], bpins[2][0]))
-
     batched = args.path == "batched"
 
-    def step():
-        return pv.solve_interval(M, spec, batched=batched, setup=gs.install if gen else None)
-
-    for _ in range(args.warmup):
-        r = step()
-    dist.barrier()
-    clocks = ClockSampler(dist.local)
-    clocks.start()
-    pv.load().pEVSL_B200_Sync()
-    pv.load().pEVSL_B200_ResetFilterCounters()
-    pv.load().pEVSL_B200_ResetGenCounters()
-    l0 = pv.launch_count()
+    # One loop of W + K steps.  Every step goes through the public API from
+    # pinned host memory: upload the CSR (pEVSL_ParcsrSetup; for the
+    # generalized workload B and its solvers too), solve, read the
+    # eigenvalues and residuals back, free the matrix.  `value` is the device
+    # time of the solve alone (CUDA events on the library stream, the matrix
+    # resident); `e2e` is the wall time of the whole step, copies included.
+    # The L2 is flushed before every step, outside both clocks.
     eig = 0
     results = []
     ms = 0.0
-    for _ in range(args.steps):
-        lib.pEVSL_B200_FlushL2(0)  # L2 flushed between timed steps (outside the events)
+    wall = 0.0
+    d2h = 0
+    clocks = ClockSampler(dist.local)
+    for it in range(args.warmup + args.steps):
+        timed = it >= args.warmup
+        if it == args.warmup:
+            dist.barrier()
+            clocks.start()
+            lib.pEVSL_B200_Sync()
+            lib.pEVSL_B200_ResetFilterCounters()
+            lib.pEVSL_B200_ResetGenCounters()
+            l0 = pv.launch_count()
+        lib.pEVSL_B200_FlushL2(0)
+        lib.pEVSL_B200_Sync()
+        t0 = time.perf_counter()
+        M = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
+        gs = GenSetup(w, n, (bpins[0][0], bpins[1][0], bpins[2][0])) if gen else None
         lib.pEVSL_B200_EventRecord(0)
-        r = step()
+        r = pv.solve_interval(M, spec, batched=batched, setup=gs.install if gen else None)
         lib.pEVSL_B200_EventRecord(1)
-        ms += lib.pEVSL_B200_EventElapsedMs(0, 1)
-        results.append(r)
-        eig += sum(r.nev)
+        step_ms = lib.pEVSL_B200_EventElapsedMs(0, 1)
+        if gs:
+            gs.free()
+        M.free()
+        lib.pEVSL_B200_Sync()
+        step_wall = time.perf_counter() - t0
+        if timed:
+            ms += step_ms
+            wall += step_wall
+            results.append(r)
+            eig += sum(r.nev)
+            d2h += sum(len(x) for x in r.lam) * 16
+        print(f"[bench] {'step' if timed else 'warmup'} {it + 1}/{args.warmup + args.steps}: "
+              f"{sum(r.nev)} eigenpairs, solve {step_ms / 1e3:.2f} s, step {step_wall:.2f} s",
+              file=sys.stderr, flush=True)
     clk = clocks.stop()
     launches = pv.launch_count() - l0
     f_launch, f_bytes, f_ms = pv.filter_counters()
@@ -326,27 +345,8 @@ def run_b200(args, dist):
     t_max = dist.max(ms / 1e3)
     eig_all = dist.sum(float(eig))
     value = eig_all / t_max
-    # end-to-end leg: upload from pinned memory, solve, results to host
-    dist.barrier()
-    lib.pEVSL_B200_EventRecord(2)
-    t0 = time.perf_counter()
-    e2e_eig = 0
-    d2h = 0
-    for _ in range(args.steps):
-        M2 = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
-        gs2 = GenSetup(w, n, (bpins[0][0], bpins[1][0], bpins[2][0])) if gen else None
-        r2 = pv.solve_interval(M2, spec, batched=batched, setup=gs2.install if gen else None)
-        if gs2:
-            gs2.free()
-        M2.free()
-        e2e_eig += sum(r2.nev)
-        d2h += sum(len(x) for x in r2.lam) * 16
-    lib.pEVSL_B200_EventRecord(3)
-    e2e_ms = lib.pEVSL_B200_EventElapsedMs(2, 3)
-    wall_e2e = time.perf_counter() - t0
-    dist.barrier()
-    e2e_t = dist.max(max(e2e_ms / 1e3, wall_e2e))
-    e2e_val = dist.sum(float(e2e_eig)) / e2e_t
+    e2e_t = dist.max(wall)
+    e2e_val = eig_all / e2e_t
     # roofline of the dominant kernel (fused Chebyshev filter degree)
     peak, peak_kind = measured_peak()
     per_launch_bytes = f_bytes / max(f_launch, 1)
@@ -403,7 +403,9 @@ def run_b200(args, dist):
         "e2e": {"value": e2e_val, "unit": "eigenpairs/s",
                 "h2d_bytes_per_step": int(4 * (n + 1) + 12 * nnz +
                                           (4 * (n + 1) + 12 * (3 * n - 2) if gen else 0)),
-                "d2h_bytes_per_step": int(d2h // max(args.steps, 1))},
+                "d2h_bytes_per_step": int(d2h // max(args.steps, 1)),
+                "how": "same steps as value: wall time of upload from pinned memory + solve + "
+                       "results to host + free, summed over the K timed steps"},
     }
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline and gen:
         try:
@@ -440,9 +442,6 @@ def run_b200(args, dist):
                           f"{kpm} KPM + <=200 bounds matvecs"}
         except Exception as e:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "unavailable": str(e)}
-    M.free()
-    if gs:
-        gs.free()
     for p in [p1, p2, p3] + [bp[1] for bp in bpins]:
         pv.free_pinned(p)
     return out
@@ -490,44 +489,47 @@ def run_b200_multi(args, dist):
                         eig += ev.cheblannr(iv, h[4][k], 1e-8, h[5], h[3][k])["nev"]
         return eig
 
-    mats = [pv.Matrix.from_csr(h[0], h[1][0][0], h[1][1][0], h[1][2][0]) for h in host]
-    for _ in range(args.warmup):
-        solve(mats)
-    dist.barrier()
+    # one loop of W + K steps, each from pinned host memory: upload the 32
+    # matrices, solve (device time between CUDA events), results to host,
+    # free; e2e is the wall time of the same steps
     clocks = ClockSampler(dist.local)
-    clocks.start()
-    lib.pEVSL_B200_Sync()
-    lib.pEVSL_B200_ResetFilterCounters()
-    l0 = pv.launch_count()
-    eig, ms = 0, 0.0
-    for _ in range(args.steps):
-        lib.pEVSL_B200_FlushL2(0)  # L2 flushed between timed steps (outside the events)
+    eig, ms, wall, h2d = 0, 0.0, 0.0, 0
+    for it in range(args.warmup + args.steps):
+        timed = it >= args.warmup
+        if it == args.warmup:
+            dist.barrier()
+            clocks.start()
+            lib.pEVSL_B200_Sync()
+            lib.pEVSL_B200_ResetFilterCounters()
+            l0 = pv.launch_count()
+        lib.pEVSL_B200_FlushL2(0)
+        lib.pEVSL_B200_Sync()
+        t0 = time.perf_counter()
+        mats = [pv.Matrix.from_csr(h[0], h[1][0][0], h[1][1][0], h[1][2][0]) for h in host]
         lib.pEVSL_B200_EventRecord(0)
-        eig += solve(mats)
+        e = solve(mats)
         lib.pEVSL_B200_EventRecord(1)
-        ms += lib.pEVSL_B200_EventElapsedMs(0, 1)
+        step_ms = lib.pEVSL_B200_EventElapsedMs(0, 1)
+        for M in mats:
+            M.free()
+        lib.pEVSL_B200_Sync()
+        step_wall = time.perf_counter() - t0
+        if timed:
+            eig += e
+            ms += step_ms
+            wall += step_wall
+            h2d += sum(4 * (h[0] + 1) + 12 * len(h[1][1][0]) for h in host)
+        print(f"[bench] {'step' if timed else 'warmup'} {it + 1}/{args.warmup + args.steps}: "
+              f"{e} eigenpairs, solve {step_ms / 1e3:.2f} s, step {step_wall:.2f} s",
+              file=sys.stderr, flush=True)
     clk = clocks.stop()
     launches = pv.launch_count() - l0
     f_launch, f_bytes, f_ms = pv.filter_counters()
     dist.barrier()
     t_max = dist.max(ms / 1e3)
     value = dist.sum(float(eig)) / t_max
-    for M in mats:
-        M.free()
-    # end to end: every step uploads the 32 matrices from pinned memory
-    dist.barrier()
-    lib.pEVSL_B200_EventRecord(2)
-    t0 = time.perf_counter()
-    e2e_eig = 0
-    h2d = 0
-    for _ in range(args.steps):
-        mats = [pv.Matrix.from_csr(h[0], h[1][0][0], h[1][1][0], h[1][2][0]) for h in host]
-        h2d += sum(4 * (h[0] + 1) + 12 * len(h[1][1][0]) for h in host)
-        e2e_eig += solve(mats)
-        for M in mats:
-            M.free()
-    lib.pEVSL_B200_EventRecord(3)
-    e2e_t = dist.max(max(lib.pEVSL_B200_EventElapsedMs(2, 3) / 1e3, time.perf_counter() - t0))
+    e2e_eig = eig
+    e2e_t = dist.max(wall)
     peak, peak_kind = measured_peak()
     per_launch_bytes = f_bytes / max(f_launch, 1)
     per_launch_ms = f_ms / max(f_launch, 1)

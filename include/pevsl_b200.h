@@ -59,6 +59,19 @@ int pEVSL_B200_SetPrecision(pevsl_Data *pevsl, int precision);
  * PEVSL_B200_FILTER_FORM sets the start value. */
 int pEVSL_B200_SetFilterForm(int form);
 
+/* Wait limit of the persistent filter's grid barrier (form 1), in polls of
+ * about 64 ns; 0 restores the default (2^24 polls, about 2 s).  A wait that
+ * runs out sets a flag and the kernel returns; the call that launched it
+ * then returns PEVSL_ERR_CUDA (the flag is read after every filter
+ * application), and the context stays usable. */
+int pEVSL_B200_SetBarrierSpins(unsigned spins);
+
+/* Fault injection for tests: preset the barrier's arrival counter to
+ * `count`, so that (for count >= the grid size) no arrival completes the
+ * next barrier and every wait runs out after the spin limit.  The timeout
+ * report clears the counter again. */
+int pEVSL_B200_SeedBarrierArrivals(unsigned count);
+
 /* The cross-group sum of a split KPM: pEVSL_Kpmdos with ngroups > 1 computes
  * the moments of its group's share of the random vectors (pEVSL_Part1d)
  * and then, in place of MPI_Allreduce on gl_comm (SRC/kpmdos.c:160-176),

@@ -287,8 +287,10 @@ int oref_cheblannr(int n, const int *ia, const int *ja, const double *a, const d
 }
 
 /* The whole driver run (LapPLanN.c:118-296 with the bounds step of
- * MMPLanN.c:104-118): one pEVSL instance, one group, all slices in order. */
-int oref_pipeline(const orc_spec *s, orc_out *o) {
+ * MMPLanN.c:104-118): one pEVSL instance, one group, slices sl_lo..sl_hi-1
+ * in order (bounds, DOS and slicing always run in full, so the slice ends
+ * and filters are those of the whole run). */
+static int pipeline_range(const orc_spec *s, orc_out *o, int sl_lo, int sl_hi) {
   pevsl_Parcsr A;
   pevsl_Data *pevsl;
   pevsl_Parvec vinit;
@@ -349,7 +351,7 @@ int oref_pipeline(const orc_spec *s, orc_out *o) {
   }
   int ev_int = (int)(1 + o->ecount / ((double)nsl));
   t = pEVSL_Wtime();
-  for (int sl = 0; sl < nsl; sl++) {
+  for (int sl = sl_lo; sl < sl_hi && sl < nsl; sl++) {
     pevsl_Polparams pol;
     int nev = ev_int + 2;
     int mlan = nev * 5 > s->mlan_min ? nev * 5 : s->mlan_min;
@@ -403,6 +405,17 @@ int oref_pipeline(const orc_spec *s, orc_out *o) {
   pEVSL_ParcsrFree(&A);
   o->t_total = pEVSL_Wtime() - t0;
   return o->status;
+}
+
+int oref_pipeline(const orc_spec *s, orc_out *o) { return pipeline_range(s, o, 0, s->nslices); }
+
+/* One or a few slices of a whole run: several processes, each with its own
+ * range, reproduce a long run slice by slice in parallel.  A slice draws
+ * random vectors only on a breakdown restart (SRC/cheblanNr.c:248-281), so
+ * the stream a slice sees equals the one-process run's unless an earlier
+ * slice restarted. */
+int oref_pipeline_slices(const orc_spec *s, orc_out *o, int sl_lo, int sl_hi) {
+  return pipeline_range(s, o, sl_lo, sl_hi);
 }
 
 /* ------------------------------------------------------------ B-solvers */

@@ -54,23 +54,27 @@ def _run(cmd, verbose):
 
 
 def build(force: bool = False, verbose: bool = False, extra_nvflags=None) -> str:
+    """Compile the stale modules (in parallel, one process per module) and
+    link the library when anything changed."""
+    from concurrent.futures import ThreadPoolExecutor
     os.makedirs(OUT_DIR, exist_ok=True)
     hdr = max((os.path.getmtime(h) for h in _headers()), default=0.0)
-    objs = []
-    rebuilt = False
+    objs, jobs = [], []
     for src in sorted(glob.glob(os.path.join(CSRC, "*.c"))):
         obj = os.path.join(OUT_DIR, os.path.basename(src) + ".o")
         if force or _stale(obj, src, hdr):
-            _run([CC] + CFLAGS + ["-c", src, "-o", obj], verbose)
-            rebuilt = True
+            jobs.append([CC] + CFLAGS + ["-c", src, "-o", obj])
         objs.append(obj)
     for src in sorted(glob.glob(os.path.join(CSRC, "*.cu"))):
         obj = os.path.join(OUT_DIR, os.path.basename(src) + ".o")
         if force or _stale(obj, src, hdr):
-            _run([NVCC] + NVFLAGS + (extra_nvflags or []) + ["-c", src, "-o", obj], verbose)
-            rebuilt = True
+            jobs.append([NVCC] + NVFLAGS + (extra_nvflags or []) + ["-c", src, "-o", obj])
         objs.append(obj)
-    if rebuilt or force or not os.path.exists(LIB):
+    if jobs:
+        with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1)) as ex:
+            for f in [ex.submit(_run, cmd, verbose) for cmd in jobs]:
+                f.result()
+    if jobs or force or not os.path.exists(LIB):
         _run([NVCC, "-shared"] + ARCH + ["-o", LIB] + objs + ["-lm"], verbose)
     return LIB
 

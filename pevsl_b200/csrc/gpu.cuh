@@ -285,6 +285,8 @@ constexpr int kTabSlots = 4; /* staging slots: a slot is reused only after its c
 int cheb_filter_persistent(int ne, const FiltDev *entries, int maxdeg);
 /* the barrier's timeout flag of the last persistent filter (read after a sync) */
 int persistent_filter_error();
+void set_barrier_spins(unsigned spins);
+int seed_barrier_arrivals(unsigned count);
 
 /* ---------------------------------------------------------------- FP32 (mixed) */
 int csr_make_fp32(pevsl_devcsr *A); /* FP32 copy of the values, once */

@@ -16,6 +16,8 @@
 #include <cuda_runtime.h>
 #include <stdio.h>
 
+#include <atomic>
+
 #include "internal.h"
 
 namespace {
@@ -30,9 +32,10 @@ constexpr int kNaColsPerBlock = kNaThreads / 32;
  * so nothing has to be cleared; calls that overlap on the GPU race on it. */
 static __device__ __align__(256) double g_noalloc_partials[kNaRowBlocks * kNaMaxCols];
 
-/* device address of the scratch array, looked up once per device */
+/* device address of the scratch array, looked up once per device; host
+ * threads that race on the first lookup store the same address */
 constexpr int kNaMaxDevices = 64;
-double *g_noalloc_ptr[kNaMaxDevices] = {};
+std::atomic<double *> g_noalloc_ptr[kNaMaxDevices] = {};
 
 /* partial[rb * k + j] = sum over the rows of block rb of V[i + j ld] x[i];
  * a warp per column, lanes across rows. */
@@ -92,21 +95,21 @@ int pEVSL_B200_ParvecsGemtvNoAlloc(const double *V, long n, long ld, int k, cons
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) return PEVSL_ERR_CUDA;
-  if (!g_noalloc_ptr[dev]) {
-    double *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress((void **)&p, g_noalloc_partials);
+  double *scratch = g_noalloc_ptr[dev].load(std::memory_order_acquire);
+  if (!scratch) {
+    const cudaError_t e = cudaGetSymbolAddress((void **)&scratch, g_noalloc_partials);
     if (e != cudaSuccess) {
       fprintf(stderr, "pEVSL_B200_ParvecsGemtvNoAlloc: cudaGetSymbolAddress: %s\n",
               cudaGetErrorString(e));
       return PEVSL_ERR_CUDA;
     }
-    g_noalloc_ptr[dev] = p;
+    g_noalloc_ptr[dev].store(scratch, std::memory_order_release);
   }
   cudaStream_t s = (cudaStream_t)stream;
   const long rows = n > 0 ? (n + kNaRowBlocks - 1) / kNaRowBlocks : 1;
   dim3 g(kNaRowBlocks, (unsigned)((k + kNaColsPerBlock - 1) / kNaColsPerBlock));
-  k_noalloc_partial<<<g, kNaThreads, 0, s>>>(n, k, V, ld, x, rows, g_noalloc_ptr[dev]);
-  k_noalloc_reduce<<<(k + 127) / 128, 128, 0, s>>>(k, g_noalloc_ptr[dev], w);
+  k_noalloc_partial<<<g, kNaThreads, 0, s>>>(n, k, V, ld, x, rows, scratch);
+  k_noalloc_reduce<<<(k + 127) / 128, 128, 0, s>>>(k, scratch, w);
   const cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     fprintf(stderr, "pEVSL_B200_ParvecsGemtvNoAlloc: launch failed: %s\n", cudaGetErrorString(e));

@@ -409,6 +409,12 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     g_filter_launches += (uint64_t)maxdeg;
     g_filter_bytes += bytes;
     g_filter_persistent++;
+    /* a barrier wait that ran out leaves the filter half applied: report it
+     * before anything uses the result (one 16-byte read per application) */
+    if (!st && persistent_filter_error()) {
+      fprintf(stderr, "pevsl_b200: persistent filter barrier timed out\n");
+      st = PEVSL_ERR_CUDA;
+    }
     return st;
   }
   /* one launch per degree for all live entries; a matrix is read once per
@@ -1572,6 +1578,13 @@ int pEVSL_B200_SetFilterForm(int form) {
   return 0;
 }
 
+int pEVSL_B200_SetBarrierSpins(unsigned spins) {
+  set_barrier_spins(spins);
+  return 0;
+}
+
+int pEVSL_B200_SeedBarrierArrivals(unsigned count) { return seed_barrier_arrivals(count); }
+
 /* Filtered Lanczos in lockstep (pEVSL_ChebLanNr, SRC/cheblanNr.c:54-448) for
  * ns <= kMaxEntries slices, which may belong to different problems (each
  * entry carries its instance, matrix, length and start vector).  Every
@@ -1921,10 +1934,6 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
         nact--;
       }
     }
-  }
-  if (!st && g_filter_persistent && persistent_filter_error()) {
-    fprintf(stderr, "pevsl_b200: persistent filter barrier timed out\n");
-    st = PEVSL_ERR_CUDA;
   }
   cudaEventRecord(e_all1, c.stream);
   const double tr_start = pevsl_now();

@@ -417,12 +417,13 @@ __global__ void __launch_bounds__(kThreads, 4)
 /* ---------------------------------------------------------------- persistent filter */
 
 constexpr unsigned kBarrierSpins = 1u << 24; /* ~2 s of polling before giving up */
+static unsigned g_barrier_spins = kBarrierSpins;
 
 /* Sense-counting grid barrier for a cooperative launch (all blocks are
  * co-resident).  bar[0] counts arrivals, bar[1] is the generation; the
- * waits are bounded: after kBarrierSpins polls the block sets bar[2] and
+ * waits are bounded: after `spins` polls the block sets bar[2] and
  * continues, and the kernel returns at its next check. */
-__device__ __forceinline__ void grid_barrier(unsigned *bar) {
+__device__ __forceinline__ void grid_barrier(unsigned *bar, unsigned spins) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile unsigned *gen = bar + 1;
@@ -435,7 +436,7 @@ __device__ __forceinline__ void grid_barrier(unsigned *bar) {
     } else {
       unsigned it = 0;
       while (*gen == g) {
-        if (++it > kBarrierSpins) {
+        if (++it > spins) {
           atomicExch(bar + 2, 1u);
           break;
         }
@@ -483,7 +484,7 @@ __device__ __forceinline__ void rotation(const FiltDev &E, int j, const T **vk, 
 template <class T, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_filter_persistent(const FiltDev *__restrict__ tab, int ne, const int *__restrict__ blk_off,
-                        int maxdeg, int shared, unsigned *bar) {
+                        int maxdeg, int shared, unsigned *bar, unsigned spins) {
   __shared__ T prod[kThreads / 32][kStreamChunk];
   extern __shared__ double dyn[];
   FiltDev *s_tab = (FiltDev *)dyn;                /* ne entries */
@@ -535,7 +536,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
       }
     }
     if (j < maxdeg) {
-      grid_barrier(bar); /* also orders the s_mu rewrite after every use */
+      grid_barrier(bar, spins); /* also orders the s_mu rewrite after every use */
       if (*(volatile unsigned *)(bar + 2)) return;
     }
   }
@@ -613,12 +614,27 @@ int cheb_filter_persistent(int ne, const FiltDev *entries, int maxdeg) {
   if ((long)grid > total) grid = (unsigned)total;
   const int *doff = (const int *)(dtab + kMaxEntries);
   unsigned *bar = c.bar;
-  void *args[] = {(void *)&dtab, (void *)&ne,     (void *)&doff,
-                  (void *)&maxdeg, (void *)&shared, (void *)&bar};
+  unsigned spins = g_barrier_spins;
+  void *args[] = {(void *)&dtab,   (void *)&ne,     (void *)&doff, (void *)&maxdeg,
+                  (void *)&shared, (void *)&bar,    (void *)&spins};
   if (fail(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(kThreads), args, dsm, c.stream),
            "cudaLaunchCooperativeKernel"))
     return PEVSL_ERR_CUDA;
   return launched("filter_persistent");
+}
+
+/* polls before a barrier wait of the persistent filter gives up (0: the
+ * default, about 2 s) */
+void set_barrier_spins(unsigned spins) { g_barrier_spins = spins ? spins : kBarrierSpins; }
+
+/* Preset the barrier's arrival counter so that no arrival completes it:
+ * every wait then runs out after the spin limit and the kernel returns with
+ * the timeout flag set (a fault injected from the host, for tests). */
+int seed_barrier_arrivals(unsigned count) {
+  if (ensure()) return PEVSL_ERR_CUDA;
+  return fail(cudaMemcpy(ctx().bar, &count, sizeof count, cudaMemcpyHostToDevice), "cudaMemcpy")
+             ? PEVSL_ERR_CUDA
+             : 0;
 }
 
 int persistent_filter_error() {

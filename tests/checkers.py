@@ -23,7 +23,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 ORACLE_DIR = os.path.join(ROOT, "oracle")
 REF_SO = os.path.join(ORACLE_DIR, "_ref", "libpevsl_ref.so")
 ORC_SO = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
-REFERENCE_TREE = "/root/reference"
+# the reference source tree (read only); one variable for every recipe,
+# script and test that builds or reads the reference
+REFERENCE_TREE = os.environ.get("PEVSL_REFDIR", "/root/reference")
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -39,7 +41,8 @@ def build_oracle() -> None:
     if os.path.isdir(REFERENCE_TREE) and not os.path.exists(REF_SO):
         targets.append("ref")
     if not os.path.exists(ORC_SO) or "ref" in targets:
-        subprocess.run(["make", "-s", "-C", ORACLE_DIR] + targets, check=True)
+        subprocess.run(["make", "-s", "-C", ORACLE_DIR, f"REFDIR={REFERENCE_TREE}"] + targets,
+                       check=True)
 
 
 class OrcSpec(C.Structure):
@@ -253,7 +256,9 @@ class Checker:
             out["W"] = W[:m].copy()
         return out
 
-    def pipeline(self, A: Csr, s: RunSpec, cap: int = 4000) -> RunResult:
+    def pipeline(self, A: Csr, s: RunSpec, cap: int = 4000, slices=None) -> RunResult:
+        """The whole run; with slices=(lo, hi) (reference build only) bounds,
+        DOS and slicing run in full and ChebLanNr only on slices lo..hi-1."""
         spec = OrcSpec()
         spec.n = A.n
         spec.ia, spec.ja, spec.a = _ptr(A.ia), _ptr(A.ja), _ptr(A.a)
@@ -270,7 +275,10 @@ class Checker:
         for name, arr in (("mu", mu), ("sli", sli), ("deg", deg), ("ptype", ptype), ("gam", gam),
                           ("bar", bar), ("nev", nev), ("its", its), ("lam", lam), ("res", res)):
             setattr(out, name, _ptr(arr))
-        self.f("pipeline")(C.byref(spec), C.byref(out))
+        if slices is None:
+            self.f("pipeline")(C.byref(spec), C.byref(out))
+        else:
+            self.f("pipeline_slices")(C.byref(spec), C.byref(out), int(slices[0]), int(slices[1]))
         rr = RunResult(out.lmin, out.lmax, out.ecount, out.npts, out.status, mu, sli, deg, ptype,
                        gam, bar, nev, its)
         for sl in range(ns):

@@ -28,8 +28,8 @@ def oracle():
 
 @pytest.fixture(scope="session")
 def reference():
-    from checkers import REF_SO, Checker
-    if not os.path.exists(REF_SO) and not os.path.isdir("/root/reference"):
+    from checkers import REF_SO, REFERENCE_TREE, Checker
+    if not os.path.exists(REF_SO) and not os.path.isdir(REFERENCE_TREE):
         pytest.skip("reference build not available")
     return Checker("ref")
 

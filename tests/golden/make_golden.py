@@ -6,7 +6,7 @@ reference is mounted, never on a GPU box) and writes small JSON files that
 the CPU tests use to pin the oracle restatement and the GPU tests use as
 known answers.  Floats are written with repr() so they round-trip exactly.
 
-    python tests/golden/make_golden.py [mm | gen | findpol]
+    python tests/golden/make_golden.py [mm | gen | findpol | c2]
 """
 from __future__ import annotations
 
@@ -172,7 +172,7 @@ def findpol_cases(ref):
     dump("findpol_cases.json", dict(cases=cases))
 
 
-def mm_case(refdir="/root/reference"):
+def mm_case(refdir=None):
     """The reference's Matrix Market driver (TESTS/MM/MMPLanN.c, built by
     `make -C oracle drivers` against the reference build) on its own
     MATRICES/A.mtx (stiff1) with the first two intervals of TESTS/MM/matfile.
@@ -180,6 +180,9 @@ def mm_case(refdir="/root/reference"):
     file lists them (one triangle, 1-based), and the driver's output."""
     import subprocess
     import tempfile
+
+    from checkers import REFERENCE_TREE
+    refdir = refdir or REFERENCE_TREE
     root = os.path.dirname(os.path.dirname(HERE))
     exe = os.path.join(root, "oracle", "_ref", "MMPLanN")
     src = os.path.join(refdir, "MATRICES", "A.mtx")
@@ -259,8 +262,69 @@ def write_matfile(path, mtx, intervals):
             f.write(f"{mtx} stiff1 MM1 {a} {b} {ns}\n")
 
 
+# The 100^3 Laplacian run of the benchmark: interval [0.80, 0.82], 4 slices,
+# thick-restart bounds (50, 200, 1e-8), KPM Mdeg 300 with 30 Philox Gaussian
+# vectors (seed 0), filters FindPol(damping 2, max_deg 3000, 0.8 / 0.2),
+# ChebLanNr tol 1e-8.
+C2_GRID = (100, 100, 100)
+C2_SPEC = dict(a_lo=0.80, b_hi=0.82, nslices=4, bounds_mode=1, Mdeg=300, nvec=30, kpm_damping=1,
+               pol_damping=2, pol_max_deg=3000, thresh_int=0.8, thresh_ext=0.2, tol=1e-8,
+               rng_mode=1, seed=0)
+
+
+def _c2_slice(args):
+    """One slice of the run in its own process (the reference build on one
+    core): bounds, KPM and slicing in full, then ChebLanNr on this slice."""
+    grid, spec, sl = args
+    import time
+    t = time.time()
+    ref = Checker("ref")
+    r = ref.pipeline(laplacian(*grid), RunSpec(**spec), cap=1000, slices=(sl, sl + 1))
+    return sl, r, time.time() - t
+
+
+def c2_case(grid=C2_GRID, spec=None, name="lap100_c2.json", procs=None):
+    """The benchmark's run on the reference build, one process per slice
+    (a few hours of CPU on 100^3): slice ends, filters, per-slice Lanczos
+    steps, accepted counts, eigenvalues and residuals -> lap100_c2.json."""
+    import multiprocessing as mp
+    import time
+    spec = dict(C2_SPEC if spec is None else spec)
+    ns = spec["nslices"]
+    os.environ["OPENBLAS_NUM_THREADS"] = "1"
+    t0 = time.time()
+    with mp.get_context("spawn").Pool(procs or ns) as pool:
+        parts = {}
+        for sl, r, dt in pool.imap_unordered(_c2_slice, [(grid, spec, k) for k in range(ns)]):
+            parts[sl] = (r, dt)
+            print(f"slice {sl}: its {int(r.its[sl])} nev {int(r.nev[sl])} deg {int(r.deg[sl])} "
+                  f"({dt:.0f} s)", flush=True)
+    r0 = parts[0][0]
+    for sl in range(1, ns):  # every process computed the same bounds, moments and slices
+        r = parts[sl][0]
+        assert (r.lmin, r.lmax, r.ecount) == (r0.lmin, r0.lmax, r0.ecount)
+        assert np.array_equal(r.sli, r0.sli) and np.array_equal(r.mu, r0.mu)
+    pick = lambda f: [f(parts[sl][0], sl) for sl in range(ns)]  # noqa: E731
+    dump(name, dict(
+        grid=list(grid), spec=spec, status=max(parts[sl][0].status for sl in range(ns)),
+        lmin=r0.lmin, lmax=r0.lmax, ecount=r0.ecount, npts=r0.npts, mu=fl(r0.mu), sli=fl(r0.sli),
+        deg=pick(lambda r, k: int(r.deg[k])), ptype=pick(lambda r, k: int(r.ptype[k])),
+        gam=pick(lambda r, k: float(r.gam[k])), bar=pick(lambda r, k: float(r.bar[k])),
+        nev=pick(lambda r, k: int(r.nev[k])), its=pick(lambda r, k: int(r.its[k])),
+        lam=pick(lambda r, k: fl(r.lam[k])), res=pick(lambda r, k: fl(r.res[k])),
+        seconds_per_slice=[round(parts[sl][1], 1) for sl in range(ns)],
+        wall_seconds=round(time.time() - t0, 1),
+        how="reference build (oracle/_ref), one process per slice, one core each"))
+
+
 if __name__ == "__main__":
-    if sys.argv[1:] == ["mm"]:
+    if sys.argv[1:] == ["c2"]:
+        c2_case()
+    elif sys.argv[1:] == ["c2-check"]:
+        # the same machinery on the README matrix, against pipelines.json
+        c2_case((20, 20, 20), dict(a_lo=0.6, b_hi=1.2, nslices=5, bounds_mode=1, rng_mode=1,
+                                   seed=0), name="_c2_check.json")
+    elif sys.argv[1:] == ["mm"]:
         mm_case()
     elif sys.argv[1:] == ["findpol"]:
         findpol_cases(Checker("ref"))

@@ -23,8 +23,10 @@ BUILD = os.path.join(HERE, "dropin", "_build")
 def binary(name):
     path = os.path.join(BUILD, name)
     if not os.path.exists(path):
-        if os.path.isdir("/root/reference"):
-            subprocess.run(["make", "-s", "-C", os.path.join(HERE, "dropin")], check=True)
+        from checkers import REFERENCE_TREE
+        if os.path.isdir(REFERENCE_TREE):
+            subprocess.run(["make", "-s", "-C", os.path.join(HERE, "dropin"),
+                            f"REFDIR={REFERENCE_TREE}"], check=True)
         else:
             pytest.fail(f"{path} missing: build tests/dropin where the reference tree exists")
     return path

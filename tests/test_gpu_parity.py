@@ -473,6 +473,40 @@ def test_filter_forms_bit_identical(gpu):
             assert np.array_equal(a["lam"], b["lam"]) and np.array_equal(a["res"], b["res"])
 
 
+def test_persistent_barrier_timeout_reports_error(gpu):
+    """The persistent filter's grid barrier gives up after its spin limit:
+    with the arrival counter preset so that no arrival completes it and a
+    short limit (4096 polls, well under a millisecond), the kernel returns,
+    the lockstep call reports PEVSL_ERR_CUDA right after that filter
+    application, and the next call on the same context runs normally and
+    gives the bits of the default form."""
+    lib = pv.load()
+    lib.pEVSL_B200_SetBarrierSpins.argtypes = [C.c_uint]
+    lib.pEVSL_B200_SeedBarrierArrivals.argtypes = [C.c_uint]
+    M, intvs, fl = _lap_slices((14, 13, 12), 0.5, 1.3, 4)
+    v = np.cos(np.arange(M.n) * 0.37)
+    with pv.Instance(M) as ev:
+        r, ref = pv.cheblannr_batch(ev, intvs, [150] * 4, 1e-8, v, fl)
+    assert r == 0
+    try:
+        assert lib.pEVSL_B200_SetFilterForm(1) == 0
+        assert lib.pEVSL_B200_SetBarrierSpins(4096) == 0
+        assert lib.pEVSL_B200_SeedBarrierArrivals(1 << 30) == 0
+        with pv.Instance(M) as ev:
+            r, outs = pv.cheblannr_batch(ev, intvs, [150] * 4, 1e-8, v, fl)
+        assert r == pv.ERR_CUDA
+        assert lib.pEVSL_B200_SetBarrierSpins(0) == 0
+        with pv.Instance(M) as ev:
+            r, again = pv.cheblannr_batch(ev, intvs, [150] * 4, 1e-8, v, fl)
+        assert r == 0
+    finally:
+        lib.pEVSL_B200_SetBarrierSpins(0)
+        lib.pEVSL_B200_SetFilterForm(-1)
+    for a, b in zip(ref, again):
+        assert a["nev"] == b["nev"] and a["its"] == b["its"]
+        assert np.array_equal(a["lam"], b["lam"])
+
+
 def test_multi_problem_equals_separate(gpu):
     """pEVSL_B200_ChebLanNrMulti over problems of different sizes, slice
     counts and filter degrees gives every slice the bits of solving its

@@ -7,8 +7,10 @@ memory budget).  It computes w = V(:,0:k)' x into caller memory with only a
 fixed scratch array of the library as workspace.  This test calls it through
 the C-ABI twice in a row with different inputs and checks each result
 against the allocating entry point pEVSL_ParvecsGemtv (and numpy) to 1e-13
-relative, the tolerance of the other Gram-Schmidt tests; it also checks that
-sizes beyond the limit (k > 256) are refused with an error code.
+relative, the tolerance of the other Gram-Schmidt tests; it checks that a
+third, warmed-up call leaves the device's free memory (cudaMemGetInfo, read
+through torch) unchanged, and that sizes beyond the limit (k > 256) are
+refused with an error code.
 
 The file name makes pytest collect it last.
 """
@@ -53,6 +55,18 @@ def test_gemtv_no_alloc_matches_allocating_entry_point():
             assert rel(got, ref) <= 1e-13, call
             assert rel(got, Vh[:, :n] @ x.get()) <= 1e-13, call
             x.free()
+        # a warmed-up call takes no device memory: the free bytes that the
+        # driver reports are the same before and after it
+        import torch
+        x = pv.Vector(n, rng.standard_normal(n))
+        assert lib.pEVSL_B200_Sync() == 0
+        free0, _ = torch.cuda.mem_get_info()
+        assert f(X.data, n, ld, k, x.pv.data, w.pv.data, None) == 0
+        assert lib.pEVSL_B200_Sync() == 0
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0, (free0, free1)
+        assert rel(w.get(), Vh[:, :n] @ x.get()) <= 1e-13
+        x.free()
         # sizes beyond the stated maximum are refused, nothing is launched
         assert f(X.data, n, ld, 257, w.pv.data, w.pv.data, None) == pv.ERR_ARG
         assert f(X.data, n, ld, 0, w.pv.data, w.pv.data, None) == pv.ERR_ARG
