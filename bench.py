@@ -272,8 +272,20 @@ def run_b200(args, dist):
     lib = pv.load()
     n, ia, ja, a = laplacian(*w["grid"])
     nnz = int(ia[-1])
-    seed = 1000 * dist.rank
+    distributed = args.mode == "distributed" and dist.world > 1 and not w.get("gen")
+    # replicas: every rank its own seed; distributed: one problem, one seed
+    seed = 0 if distributed else 1000 * dist.rank
     spec = slice_run(w, seed)
+    reduce, gather = None, None
+    if distributed:
+        from pevsl_b200.distributed import GroupReduce
+
+        reduce = GroupReduce()
+
+        def gather(obj):
+            out = [None] * dist.world
+            dist.pg.all_gather_object(out, obj)
+            return out
     # pinned host copies of the inputs: every step uploads them
     ia_p, p1 = pv.pinned_empty(n + 1, np.int32)
     ja_p, p2 = pv.pinned_empty(nnz, np.int32)
@@ -316,7 +328,11 @@ def run_b200(args, dist):
         M = pv.Matrix.from_csr(n, ia_p, ja_p, a_p)
         gs = GenSetup(w, n, (bpins[0][0], bpins[1][0], bpins[2][0])) if gen else None
         lib.pEVSL_B200_EventRecord(0)
-        r = pv.solve_interval(M, spec, batched=batched, setup=gs.install if gen else None)
+        if distributed:
+            from pevsl_b200.distributed import solve_interval_distributed
+            r = solve_interval_distributed(M, spec, dist.rank, dist.world, reduce, gather)
+        else:
+            r = pv.solve_interval(M, spec, batched=batched, setup=gs.install if gen else None)
         lib.pEVSL_B200_EventRecord(1)
         step_ms = lib.pEVSL_B200_EventElapsedMs(0, 1)
         if gs:
@@ -324,14 +340,20 @@ def run_b200(args, dist):
         M.free()
         lib.pEVSL_B200_Sync()
         step_wall = time.perf_counter() - t0
+        if distributed:
+            # rank 0 gathered every slice; the others count nothing
+            nev = sum(r.nev) if r is not None else 0
+        else:
+            nev = sum(r.nev)
         if timed:
             ms += step_ms
             wall += step_wall
-            results.append(r)
-            eig += sum(r.nev)
-            d2h += sum(len(x) for x in r.lam) * 16
+            if r is not None:
+                results.append(r)
+                d2h += sum(len(x) for x in r.lam) * 16
+            eig += nev
         print(f"[bench] {'step' if timed else 'warmup'} {it + 1}/{args.warmup + args.steps}: "
-              f"{sum(r.nev)} eigenpairs, solve {step_ms / 1e3:.2f} s, step {step_wall:.2f} s",
+              f"{nev} eigenpairs, solve {step_ms / 1e3:.2f} s, step {step_wall:.2f} s",
               file=sys.stderr, flush=True)
     clk = clocks.stop()
     launches = pv.launch_count() - l0
@@ -352,6 +374,8 @@ def run_b200(args, dist):
     per_launch_bytes = f_bytes / max(f_launch, 1)
     per_launch_ms = f_ms / max(f_launch, 1)
     achieved = per_launch_bytes / (per_launch_ms * 1e-3) / 1e9 if f_launch else None
+    if not results:  # a distributed rank other than 0: rank 0 prints the line
+        return None
     r0 = results[0]
     out = {
         "metric": metric_of(w),
@@ -362,12 +386,13 @@ def run_b200(args, dist):
         "warmup": args.warmup,
         "ms_per_step": t_max * 1e3 / args.steps,
         "higher_is_better": True,
-        "scaling": "weak",
+        "scaling": "strong" if distributed else "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": ("synthetic: 3D Dirichlet Laplacian A" + (" and 1D Laplacian B (diagonal 4)"
                  if gen else "") + " generated on the host, seeded Philox Gaussian random "
-                 "vectors (seed 1000*rank)"),
+                 "vectors (" + ("seed 0, one problem over the ranks" if distributed else
+                                "seed 1000*rank") + ")"),
         "config": {"workload": args.workload, "n": n, "nnz": nnz, "interval": [w["a"], w["b"]],
                    **({"problem": "generalized A x = lam B x (pEVSL_SetGenEig)",
                        "b_solve": "least-squares 1/x on [2, 6], pEVSL_SetupLSPolRec(80, 1e-10)",
@@ -383,7 +408,10 @@ def run_b200(args, dist):
                    "lanczos_steps_per_slice": r0.its, "filter_degree_per_slice": r0.deg,
                    "l2": "256 MiB written between timed steps (L2 flush); within a step the "
                          "working set streams thousands of times",
-                   "parallelism": f"replicas x{dist.world}"},
+                   "parallelism": (f"one problem over {dist.world} ranks: KPM vectors split "
+                                   "and summed by one all-reduce, slices shared out "
+                                   "(pevsl_b200.distributed)" if distributed else
+                                   f"replicas x{dist.world}")},
         "gpu_launches": int(launches),
         "clocks": clk,
         "roofline": {
@@ -571,34 +599,58 @@ def run_b200_multi(args, dist):
 
 
 # ---------------------------------------------------------------- reference arm
-def _ref_slice_worker(q, n, ia, ja, a, deg, cc, dd, mu, budget, gen_w=None):
+def _ref_slice_worker(q, n, ia, ja, a, deg, cc, dd, mu, budget):
     os.environ["OPENBLAS_NUM_THREADS"] = "1"
 
     class F:
         pass
     f = F()
     f.deg, f.cc, f.dd, f.mu = deg, cc, dd, mu
-    if gen_w:
-        q.put(cpu_reference_gen_sample(gen_w, n, ia, ja, a, f, budget))
-    else:
-        q.put(cpu_reference_sample(n, ia, ja, a, f, budget))
+    q.put(cpu_reference_sample(n, ia, ja, a, f, budget))
+
+
+def ref_golden(workload):
+    """The reference build's own run of a workload (tests/golden, written by
+    tests/golden/make_golden.py from oracle/_ref on the same inputs: seeded
+    Gaussian vectors, thick-restart bounds, KPM, slicing, ChebLanNr): its
+    bounds, slice ends and per-slice filter degrees, Lanczos steps and
+    accepted counts, or None when the fixture is absent."""
+    name, key = {"lap100_4slices": ("lap100_c2.json", None),
+                 "lap20_5slices": ("pipelines.json", "lap20_lantr_gauss")}.get(workload, (None, None))
+    if name is None:
+        return None
+    try:
+        with open(os.path.join(ROOT, "tests", "golden", name)) as f:
+            g = json.load(f)
+    except OSError:
+        return None
+    g = g[key] if key else g
+    return {k: g[k] for k in ("lmin", "lmax", "sli", "deg", "its", "nev")} | {
+        "eigenpairs": int(sum(g["nev"])), "seconds_per_slice": g.get("seconds_per_slice"),
+        "fixture": name + (f":{key}" if key else "")}
 
 
 def run_reference(args, dist):
-    """The reference's own CPU code (oracle/_ref) on this workload: its
-    pEVSL_LanTrbounds/Kpmdos-free filter cost measured per slice, one process
-    per slice as the reference's MPI groups, each step a bounded sample."""
+    """The reference's own CPU code (oracle/_ref, compiled from its sources)
+    on this workload, one process per slice as the reference's MPI groups.
+    A step times a bounded sample: each process runs the reference's
+    pEVSL_ChebAv with its slice's filter (pEVSL_FindPol on the reference's
+    own slice ends) for about 20 s; the time of the whole run is
+    extrapolated from it to the per-slice filter degrees and Lanczos steps
+    of the reference's own run of the workload (ref_golden)."""
     if dist.rank != 0:
         return None
-    if WORKLOADS[args.workload].get("gen") and args.workload not in REF_COUNTS:
-        return {"impl": "reference", "unavailable": "per-slice counts of this workload not recorded"}
-    if WORKLOADS[args.workload].get("multi"):
+    w = WORKLOADS[args.workload]
+    if w.get("gen") or w.get("multi"):
         return {"impl": "reference", "unavailable": "the reference arm times the single-problem "
-                "workloads (lap100_4slices, lap20_5slices)"}
+                "Laplacian workloads (lap100_4slices, lap20_5slices)"}
+    g = ref_golden(args.workload)
+    if g is None:
+        return {"impl": "reference", "unavailable": "the reference build's run of this workload "
+                "(tests/golden) is missing"}
     import multiprocessing as mp
 
     from pevsl_b200.problems import laplacian
-    w = WORKLOADS[args.workload]
     n, ia, ja, a = laplacian(*w["grid"])
     lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so"))
     P = lambda x: x.ctypes.data_as(C.c_void_p)  # noqa: E731
@@ -616,31 +668,20 @@ def run_reference(args, dist):
         if r:
             raise RuntimeError(f"reference pEVSL_FindPol returned {r} for {list(intv)}")
         return d.value, cc.value, dd.value, np.ascontiguousarray(mu[: d.value + 1])
-    counts = REF_COUNTS.get(args.workload)
-    gen = bool(w.get("gen"))
-    lo, hi = C.c_double(), C.c_double()
-    if gen:
-        # spectrum bounds of B^{-1} A recorded with the counts below
-        lo.value, hi.value = counts["bounds"]
-    else:
-        # bounds with the reference's thick-restart Lanczos (real run)
-        lib.oref_set_unit_rng(1, C.c_uint64(0))
-        v0 = np.cos(np.arange(n) * 0.37)
-        lib.oref_lantrbounds(n, P(ia), P(ja), P(a), 50, 200, C.c_double(1e-8), P(v0), 1,
-                             C.byref(lo), C.byref(hi))
     nsl = w["nslices"]
+    sli = g["sli"]
+    filters = [ref_findpol([sli[s], sli[s + 1], g["lmin"], g["lmax"]]) for s in range(nsl)]
+    assert [f[0] for f in filters] == g["deg"], "filter degrees differ from the reference run"
     cores = min(os.cpu_count() or 1, nsl)
     ctx = mp.get_context("spawn")
-    times = []
+    times, per = [], []
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         q = ctx.Queue()
         procs = []
-        edges = np.linspace(w["a"], w["b"], nsl + 1)
         for s in range(nsl):
-            deg, cc, dd, mu = ref_findpol([edges[s], edges[s + 1], lo.value, hi.value])
-            p = ctx.Process(target=_ref_slice_worker,
-                            args=(q, n, ia, ja, a, deg, cc, dd, mu, 20.0, w if gen else None))
+            deg, cc, dd, mu = filters[s]
+            p = ctx.Process(target=_ref_slice_worker, args=(q, n, ia, ja, a, deg, cc, dd, mu, 20.0))
             p.start()
             procs.append(p)
         per = [q.get() for _ in procs]
@@ -650,40 +691,33 @@ def run_reference(args, dist):
             times.append(time.perf_counter() - t0)
     per_deg = float(np.mean([x[0] for x in per]))
     kpm = w["Mdeg"] * w["nvec"]
-    if counts:
-        # slices run concurrently (one process each): the slowest slice
-        # sets the time; KPM vectors split across the same processes
-        slice_t = max(per_deg * (its + 1) * deg for its, deg in zip(counts["its"], counts["deg"]))
-        total_t = slice_t + per_deg * (kpm / cores + 200)
-        value = counts["eigenpairs"] / total_t
-        how = (f"per-slice filter cost measured with the reference's pEVSL_ChebAv "
-               f"({per_deg*1e3:.2f} ms per degree, {nsl} processes in parallel), extrapolated to "
-               f"the per-slice Lanczos steps {counts['its']} and degrees {counts['deg']} of this "
-               f"workload (identical in the reference and the GPU path) + KPM split over "
-               f"{cores} processes")
-    else:
-        value, how = None, "per-slice step counts for this workload not recorded"
+    # slices run concurrently (one process each): the slowest slice sets
+    # the time; the KPM vectors are split across the same processes
+    slice_t = max(per_deg * (its + 1) * deg for its, deg in zip(g["its"], g["deg"]))
+    total_t = slice_t + per_deg * (kpm / cores + 200)
+    value = g["eigenpairs"] / total_t
+    sample_s = float(np.mean(times)) if times else 0.0
+    measured = g.get("seconds_per_slice")
+    how = (f"reference pEVSL_ChebAv (oracle/_ref, one core per process, {nsl} processes in "
+           f"parallel) for ~20 s per slice with each slice's own filter: {per_deg*1e3:.2f} ms per "
+           f"degree; extrapolated x{total_t / max(sample_s, 1e-9):.0f} to the reference run's "
+           f"per-slice Lanczos steps {g['its']} and filter degrees {g['deg']} "
+           f"({g['fixture']}) + the KPM matvecs split over {cores} processes + <=200 bounds "
+           f"matvecs" + (f"; the full reference run that wrote the fixture took "
+                         f"{[round(x) for x in measured]} s per slice on one core each"
+                         if measured else ""))
     return {"metric": metric_of(w), "value": value, "unit": "eigenpairs/s", "n_gpus": dist.world,
-            "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * float(np.mean(times)) if times else None,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sample_s,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic: 3D Dirichlet Laplacian" + (" A, 1D Laplacian B" if gen else ""),
-            "impl": "reference",
-            "config": {"workload": args.workload, "n": n, "nnz": int(ia[-1])},
+            "data": "synthetic: 3D Dirichlet Laplacian", "impl": "reference",
+            "config": {"workload": args.workload, "n": n, "nnz": int(ia[-1]),
+                       "slice_ends": sli, "filter_degree_per_slice": g["deg"],
+                       "lanczos_steps_per_slice": g["its"], "nev_per_slice": g["nev"],
+                       "estimated_seconds_per_run": total_t},
             "cpu_baseline": {"value": value, "unit": "eigenpairs/s", "cores": cores,
                              "kind": "reference", "sample": how},
             "e2e": {"value": value, "unit": "eigenpairs/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
-
-
-# per-slice Lanczos steps / filter degrees / accepted pairs of the workload,
-# recorded from a parity-checked run (used only to extrapolate the CPU sample)
-REF_COUNTS = {
-    "lap100_4slices": {"its": [431, 531, 531, 431], "deg": [1888, 1902, 1917, 1930],
-                       "eigenpairs": 454},
-    "lap20_5slices": {"its": [151, 151, 151, 151, 151], "deg": [54, 72, 91, 89, 110],
-                      "eigenpairs": 118},
-}
 
 
 def kernel_case(args):
@@ -800,6 +834,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--path", default="batched", choices=["batched", "plain"],
                     help="batched: slices in lockstep; plain: one pEVSL_ChebLanNr per slice")
+    ap.add_argument("--mode", default="replicas", choices=["replicas", "distributed"],
+                    help="N > 1: replicas (every rank solves its own copy, weak scaling) or "
+                         "distributed (one problem over the ranks: KPM vectors split and summed "
+                         "by an all-reduce, slices shared out; strong scaling)")
     ap.add_argument("--degree", type=int, default=16,
                     help="filter degree of the cheb_batch kernel case")
     ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "gen_filter",

@@ -183,6 +183,18 @@ int pEVSL_B200_ChebLanNrMulti(int nprob, pevsl_Data **pevsls, const int *nslices
 int pEVSL_B200_ParvecsGemtvNoAlloc(const double *V, long n, long ld, int k, const double *x,
                                    double *w, void *stream);
 
+/* The two dense products of the solvers, on the FP64 tensor cores (DMMA,
+ * mma.sync m8n8k4), for device pointers, column-major, on the library
+ * stream: U = V(:, 0:k) Y (n x m; V n x k, leading dimension ldv; Y k x m,
+ * ldy) -- the Ritz vectors (SRC/cheblanNr.c:363-365) -- and C = V' W (k x m;
+ * W n x m, ldw) -- the Gram matrices of the refinement sweep, the block form
+ * of GemtvWithWspace (SRC/parvecs.c:117-136).  Deterministic: a fixed
+ * partition of the rows and a fixed order of the partial sums. */
+int pEVSL_B200_GemmNN(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy,
+                      double *U, long ldu);
+int pEVSL_B200_GemmTN(long n, int k, int m, const double *V, long ldv, const double *W, long ldw,
+                      double *C, long ldc);
+
 /* Release cached device workspaces (they are reused across calls). */
 void pEVSL_B200_ReleaseWorkspace(void);
 

@@ -75,6 +75,7 @@ enum Ws {
   WS_GEN,       /* generalized problem: filter / KPM vectors  */
   WS_IL,        /* interleaved filter: three n x S blocks     */
   WS_ILMU,      /* interleaved filter: per-degree coefficients */
+  WS_WAVE,      /* wavefront filter: chunk progress + claim counters */
   WS_COUNT
 };
 
@@ -245,6 +246,29 @@ int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double 
 int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
                    const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
                    const double *mu0, const double *muk, int ny, int fresh);
+/* the staged (cp.async.bulk) form of cheb_step_il_y for Xg == Xk on a
+ * packed matrix with a chunk table (gpu_filter_tma.cu); il_tma_usable says
+ * whether it applies; il_tma_error returns 1 (and clears the flag) when one
+ * of its bounded waits ran out since the last check */
+bool il_tma_usable(const pevsl_devcsr *A, int S);
+int cheb_step_il_tma(const pevsl_devcsr *A, int S, const double *Xk, const double *Xkm1,
+                     double *Xkp1, double *Y, double cc, double t, const double *mu0,
+                     const double *muk, int ny, int fresh);
+int il_tma_error();
+/* all degrees of one interleaved filter application as wavefront launches
+ * of several degrees each (gpu_filter_tma.cu): X0 = T_0, B0/B1 the two
+ * recurrence blocks, Y the accumulator, mu the (maxdeg + 1) x S table,
+ * defer the accumulator deferral of cheb_step_il_y; flags: il_wave_ints
+ * ints of device memory (zeroed here).  Same bits as the degree-by-degree
+ * launches. */
+bool il_wave_usable(const pevsl_devcsr *A, int S);
+size_t il_wave_ints(const pevsl_devcsr *A, int maxdeg);
+int cheb_filter_il_wave(const pevsl_devcsr *A, int S, const double *X0, double *B0, double *B1,
+                        double *Y, double cc, double dd, const double *mu, int maxdeg, int defer,
+                        int *flags);
+/* the staged kernel for one vector: cheb_step's recurrence (y every degree) */
+int cheb_step_tma(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1,
+                  double *y, double cc, double t, double mu0, double muk, int first);
 /* X[i*S + s] = xs[s][i] (S <= kMaxBatch), and ys[s][i] = X[i*S + s] for
  * the first cols columns */
 int il_pack(long n, int S, const double *const *xs, double *X);

@@ -1,9 +1,11 @@
 /*
- * Dense kernel over the Lanczos basis V (n x k, column major, leading
- * dimension ldv); the Gram-Schmidt passes live in gpu_batch.cu.
+ * Dense kernels over the Lanczos basis V (n x k, column major, leading
+ * dimension ldv), on the FP64 tensor cores (mma.sync m8n8k4 .f64); the
+ * Gram-Schmidt passes live in gpu_batch.cu.
  *
  *  - gemm_nn: Ritz vectors U = V(:,0:k) Y (SRC/cheblanNr.c:363-365 does one
- *    GEMV per Ritz vector; here one pass over V serves 8 of them).
+ *    GEMV per Ritz vector; here one pass over V serves 64 of them).
+ *  - gemm_tn: Gram matrices C = V' W of the refinement sweep.
  */
 #include <cuda_runtime.h>
 
@@ -11,56 +13,84 @@
 
 namespace pv {
 
-/* U[:, c0:c0+8] = V(:, 0:k) Y[:, c0:c0+8]; thread per row, Y tile in smem */
-constexpr int kGemmTile = 8;
+/* FP64 tensor-core product (DMMA): D = A B + C for an 8 x 4 tile of A and a
+ * 4 x 8 tile of B.  Fragments per lane l: a = A[l / 4][l % 4],
+ * b = B[l % 4][l / 4], c/d = C[l / 4][2 (l % 4) + {0, 1}]. */
+__device__ __forceinline__ void dmma_8x8x4(double a, double b, double &c0, double &c1) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+               : "+d"(c0), "+d"(c1)
+               : "d"(a), "d"(b));
+}
+
+/* U = V(:, 0:k) Y on the FP64 tensor cores: a block owns a 64 x 64 tile of
+ * U (64 rows, 64 Ritz vectors) and walks k in panels of 16 columns of V,
+ * staged in shared memory with the matching 16 rows of Y; each of the 8
+ * warps accumulates 8 of the tile's 8 x 8 sub-tiles (warp w: sub-tile rows
+ * w, sub-tile columns 0..7).  V is read m / 64 times instead of once per
+ * eight Ritz vectors.  (SRC/cheblanNr.c:363-365 forms the Ritz vectors one
+ * GEMV each.) */
+constexpr int kNnTile = 64, kNnPanel = 16;
 __global__ void __launch_bounds__(kThreads)
-    k_gemm_nn(long n, int k, int m, const double *__restrict__ V, long ldv,
-              const double *__restrict__ Y, long ldy, double *__restrict__ U, long ldu) {
-  extern __shared__ double ysh[]; /* k x kGemmTile */
-  const int c0 = blockIdx.y * kGemmTile;
-  const int mc = m - c0 < kGemmTile ? m - c0 : kGemmTile;
-  for (int t = threadIdx.x; t < k * kGemmTile; t += blockDim.x) {
-    const int j = t / kGemmTile, c = t % kGemmTile;
-    ysh[t] = c < mc ? Y[(size_t)(c0 + c) * ldy + j] : 0.0;
-  }
-  __syncthreads();
-  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-    double acc[kGemmTile];
+    k_gemm_nn_dmma(long n, int k, int m, const double *__restrict__ V, long ldv,
+                   const double *__restrict__ Y, long ldy, double *__restrict__ U, long ldu) {
+  __shared__ double vs[kNnPanel][kNnTile + 1]; /* vs[jj][i] = V[i0 + i, j + jj] */
+  __shared__ double ys[kNnPanel][kNnTile + 1]; /* ys[jj][c] = Y[j + jj, c0 + c] */
+  const long i0 = (long)blockIdx.x * kNnTile;
+  const int c0 = blockIdx.y * kNnTile;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lr = lane >> 2, lc = lane & 3;
+  double acc[8][2];
 #pragma unroll
-    for (int c = 0; c < kGemmTile; c++) acc[c] = 0.0;
-    for (int j = 0; j < k; j++) {
-      const double x = V[(size_t)j * ldv + i];
+  for (int t = 0; t < 8; t++) acc[t][0] = acc[t][1] = 0.0;
+  for (int j = 0; j < k; j += kNnPanel) {
+    /* 64 rows x 16 columns of V (a column's 64 rows are contiguous) and 16
+     * rows x 64 columns of Y, zero outside */
 #pragma unroll
-      for (int c = 0; c < kGemmTile; c++) acc[c] = fma(x, ysh[j * kGemmTile + c], acc[c]);
+    for (int q = 0; q < 4; q++) {
+      const int t = threadIdx.x + kThreads * q;
+      const int i = t & 63, jj = t >> 6;
+      const long row = i0 + i;
+      vs[jj][i] = (row < n && j + jj < k) ? V[(size_t)(j + jj) * ldv + row] : 0.0;
+      const int c = t >> 4, yj = t & 15;
+      ys[yj][c] = (c0 + c < m && j + yj < k) ? Y[(size_t)(c0 + c) * ldy + j + yj] : 0.0;
     }
+    __syncthreads();
 #pragma unroll
-    for (int c = 0; c < kGemmTile; c++)
-      if (c < mc) U[(size_t)(c0 + c) * ldu + i] = acc[c];
+    for (int kk = 0; kk < kNnPanel; kk += 4) {
+      const double a = vs[kk + lc][warp * 8 + lr];
+#pragma unroll
+      for (int t = 0; t < 8; t++) dmma_8x8x4(a, ys[kk + lc][t * 8 + lr], acc[t][0], acc[t][1]);
+    }
+    __syncthreads();
+  }
+  const long row = i0 + warp * 8 + lr;
+  if (row < n) {
+#pragma unroll
+    for (int t = 0; t < 8; t++)
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int c = c0 + t * 8 + 2 * lc + h;
+        if (c < m) U[(size_t)c * ldu + row] = acc[t][h];
+      }
   }
 }
 
 int gemm_nn(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy, double *U,
             long ldu) {
   if (m <= 0 || n <= 0) return 0;
-  const size_t sh = sizeof(double) * (size_t)k * kGemmTile;
-  if (sh > 200 * 1024) return PEVSL_ERR_ARG;
-  if (sh > 48 * 1024) {
-    static bool attr_done = false;
-    if (!attr_done) {
-      cudaFuncSetAttribute(k_gemm_nn, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-      attr_done = true;
-    }
-  }
-  dim3 g(grid_for(n, 1), (unsigned)((m + kGemmTile - 1) / kGemmTile));
-  k_gemm_nn<<<g, kThreads, sh, ctx().stream>>>(n, k, m, V, ldv, Y, ldy, U, ldu);
-  return launched("gemm_nn");
+  dim3 g((unsigned)((n + kNnTile - 1) / kNnTile), (unsigned)((m + kNnTile - 1) / kNnTile));
+  k_gemm_nn_dmma<<<g, kThreads, 0, ctx().stream>>>(n, k, m, V, ldv, Y, ldy, U, ldu);
+  return launched("gemm_nn_dmma");
 }
 
-/* C = V' W for tall V (n x k) and W (n x m): a block owns a 64 x 64 tile
- * of C and one chunk of rows; it stages 16 rows of the two 64-column
- * panels in shared memory and each thread accumulates a 4 x 4 subtile
- * (rows ty + 16 i, columns tx + 16 j, conflict-free).  Per-chunk tiles go
- * to partial[chunk], then k_gemm_tn_reduce adds them in chunk order. */
+/* C = V' W for tall V (n x k) and W (n x m) on the FP64 tensor cores: a
+ * block owns a 64 x 64 tile of C and one chunk of rows; it stages 16 rows of
+ * the two 64-column panels in shared memory, and each of the 8 warps
+ * accumulates 8 of the tile's 8 x 8 sub-tiles (sub-tile row = warp) with
+ * m8n8k4 DMMA over the panel's rows.  Per-chunk tiles go to partial[chunk],
+ * then k_gemm_tn_reduce adds them in chunk order (deterministic).  These are
+ * the block Gram products of the refinement sweep, the dense counterpart of
+ * the reference's GemtvWithWspace (SRC/parvecs.c:117-136). */
 constexpr int kTnTile = 64, kTnRows = 16;
 __global__ void __launch_bounds__(kThreads)
     k_gemm_tn_partial(long n, int k, int m, const double *__restrict__ V, long ldv,
@@ -70,12 +100,11 @@ __global__ void __launch_bounds__(kThreads)
   const int ti = blockIdx.x, tj = blockIdx.y;
   const long r_beg = (long)blockIdx.z * rows_per_chunk;
   const long r_end = r_beg + rows_per_chunk < n ? r_beg + rows_per_chunk : n;
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int lr = lane >> 2, lc = lane & 3;
+  double acc[8][2];
 #pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  for (int t = 0; t < 8; t++) acc[t][0] = acc[t][1] = 0.0;
   for (long r0 = r_beg; r0 < r_end; r0 += kTnRows) {
     /* 16 rows x 64 columns of each panel: thread t loads row t % 16 of
      * columns t / 16 + 16 q (16 consecutive rows of a column per half-warp) */
@@ -88,30 +117,27 @@ __global__ void __launch_bounds__(kThreads)
       wsh[r][c] = (row < r_end && cw < m) ? W[(size_t)cw * ldw + row] : 0.0;
     }
     __syncthreads();
-#pragma unroll 4
-    for (int r = 0; r < kTnRows; r++) {
-      double a[4], b[4];
+    /* A = V' (rows: columns of V, k: rows of the panel), B = W panel */
 #pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = vs[r][ty + 16 * i];
+    for (int kk = 0; kk < kTnRows; kk += 4) {
+      const double a = vs[kk + lc][warp * 8 + lr];
 #pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = wsh[r][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+      for (int t = 0; t < 8; t++) dmma_8x8x4(a, wsh[kk + lc][t * 8 + lr], acc[t][0], acc[t][1]);
     }
     __syncthreads();
   }
   double *out = partial + (size_t)blockIdx.z * (size_t)k * (size_t)m;
+  const int ci = ti * kTnTile + warp * 8 + lr;
+  if (ci < k) {
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+    for (int t = 0; t < 8; t++)
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int ci = ti * kTnTile + ty + 16 * i, cj = tj * kTnTile + tx + 16 * j;
-      if (ci < k && cj < m) out[(size_t)cj * k + ci] = acc[i][j];
-    }
+      for (int h = 0; h < 2; h++) {
+        const int cj = tj * kTnTile + t * 8 + 2 * lc + h;
+        if (cj < m) out[(size_t)cj * k + ci] = acc[t][h];
+      }
+  }
 }
-
 __global__ void k_gemm_tn_reduce(int k, int m, int nchunk, const double *__restrict__ partial,
                                  double *__restrict__ C, long ldc) {
   const long tot = (long)k * m;
@@ -145,3 +171,21 @@ int gemm_tn(long n, int k, int m, const double *V, long ldv, const double *W, lo
 }
 
 }  // namespace pv
+
+extern "C" {
+
+int pEVSL_B200_GemmNN(long n, int k, int m, const double *V, long ldv, const double *Y, long ldy,
+                      double *U, long ldu) {
+  if (pv::ensure()) return PEVSL_ERR_CUDA;
+  if (n < 0 || k < 0 || m < 0 || ldv < n || ldu < n || ldy < k) return PEVSL_ERR_ARG;
+  return pv::gemm_nn(n, k, m, V, ldv, Y, ldy, U, ldu);
+}
+
+int pEVSL_B200_GemmTN(long n, int k, int m, const double *V, long ldv, const double *W, long ldw,
+                      double *C, long ldc) {
+  if (pv::ensure()) return PEVSL_ERR_CUDA;
+  if (n < 0 || k < 0 || m < 0 || ldv < n || ldw < n || ldc < k) return PEVSL_ERR_ARG;
+  return pv::gemm_tn(n, k, m, V, ldv, W, ldw, C, ldc);
+}
+
+}  // extern "C"

@@ -19,6 +19,7 @@
  */
 #include <ctype.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <vector>
 #include <stdio.h>
 #include <stdlib.h>
@@ -961,6 +962,10 @@ int spmv(const pevsl_devcsr *A, const double *x, double *y) {
 int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1, double *y,
               double cc, double t, double mu0, double muk, int first) {
   if (A->nrows <= 0) return 0;
+  /* packed matrices of at least 2^16 rows: the staged kernel (same bits);
+   * smaller ones sit in L2, where the CSR-stream kernel's finer grid wins */
+  if (A->lanes == 0 && use_packed(A) && A->nrows >= 65536 && il_tma_usable(A, 1))
+    return cheb_step_tma(A, vk, vkm1, vkp1, y, cc, t, mu0, muk, first);
   if (A->lanes == 0) {
     launch_stream(A, (const double *)A->a, vk, EpiCheb{vk, vkm1, vkp1, y, cc, t, mu0, muk, first});
     return launched("cheb_step_stream");
@@ -1188,6 +1193,8 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
   cudaStream_t st = ctx().stream;
+  if (Xg == Xk && il_packed(A) && il_tma_usable(A, S))
+    return cheb_step_il_tma(A, S, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, ny, fresh);
   if (il_packed(A)) {
 #define PV_IL_P(SS)                                                                          \
   k_cheb_il_p<SS><<<g, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, \
@@ -1394,11 +1401,70 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
       vi[(size_t)k] = (unsigned char)hval[h];
     }
   }
+  /* row chunks of the staged kernels: at most RMAX rows and EMAX entries,
+   * starting at multiples of 4 rows (16-byte aligned row-pointer and
+   * vector copies) */
+  std::vector<int> ch;
+  for (int r = 0; r < nr;) {
+    ch.push_back(r);
+    ch.push_back(Ai->ia[r]);
+    int e = PEVSL_MIN(nr, r + 4);
+    while (e < nr && e - r < PEVSL_WAVE_RMAX) {
+      const int e2 = PEVSL_MIN(nr, e + 4);
+      if (Ai->ia[e2] - Ai->ia[r] > PEVSL_WAVE_EMAX) break;
+      e = e2;
+    }
+    r = e;
+  }
+  const int wnc = (int)(ch.size() / 2);
+  ch.push_back(nr);
+  ch.push_back((int)nnz);
+  /* dependency ranges of the chunks: [lo, hi] of the chunks of the columns
+   * of its rows, widened to every chunk that has a column in it (prefix max
+   * of hi / suffix min of lo; a superset for unsymmetric patterns) */
+  std::vector<int> starts((size_t)wnc + 1);
+  for (int c = 0; c <= wnc; c++) starts[(size_t)c] = ch[(size_t)2 * c];
+  auto chunk_of = [&](int col) {
+    return (int)(std::upper_bound(starts.begin(), starts.end() - 1, col) - starts.begin()) - 1;
+  };
+  std::vector<int> clo((size_t)wnc), chi((size_t)wnc);
+  for (int c = 0; c < wnc; c++) {
+    int mn = INT32_MAX, mx = -1;
+    for (int k = Ai->ia[starts[(size_t)c]]; k < Ai->ia[starts[(size_t)c + 1]]; k++) {
+      mn = PEVSL_MIN(mn, Ai->ja[k]);
+      mx = PEVSL_MAX(mx, Ai->ja[k]);
+    }
+    clo[(size_t)c] = mx < 0 ? c : PEVSL_MIN(c, chunk_of(mn));
+    chi[(size_t)c] = mx < 0 ? c : PEVSL_MAX(c, chunk_of(mx));
+  }
+  std::vector<int> pmax((size_t)wnc), smin((size_t)wnc);
+  for (int c = 0; c < wnc; c++) pmax[(size_t)c] = PEVSL_MAX(chi[(size_t)c], c ? pmax[(size_t)c - 1] : -1);
+  for (int c = wnc - 1; c >= 0; c--)
+    smin[(size_t)c] = PEVSL_MIN(clo[(size_t)c], c + 1 < wnc ? smin[(size_t)c + 1] : INT32_MAX);
+  std::vector<int> dep((size_t)2 * wnc);
+  int reach = 0;
+  for (int c = 0; c < wnc; c++) {
+    /* first c' with pmax >= c, last c' with smin <= c (both monotone) */
+    const int rlo = (int)(std::lower_bound(pmax.begin(), pmax.end(), c) - pmax.begin());
+    const int rhi = (int)(std::upper_bound(smin.begin(), smin.end(), c) - smin.begin()) - 1;
+    const int lo = PEVSL_MIN(clo[(size_t)c], rlo), hi = PEVSL_MAX(chi[(size_t)c], rhi);
+    dep[(size_t)2 * c] = lo;
+    dep[(size_t)2 * c + 1] = hi;
+    reach = PEVSL_MAX(reach, PEVSL_MAX(c - lo, hi - c));
+  }
+  /* the parts are 256-byte multiples: a staged copy rounded up to 16 bytes
+   * never leaves its part */
   const size_t b_dj = ((sizeof(short) * (size_t)nnz + 255) / 256) * 256;
   const size_t b_vi = ((size_t)nnz + 255) / 256 * 256;
   const size_t b_tab = 256 * sizeof(double) + 256 * sizeof(float);
-  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab);
+  const size_t b_ch = (sizeof(int) * ch.size() + 255) / 256 * 256;
+  const size_t b_dep = (sizeof(int) * dep.size() + 255) / 256 * 256;
+  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab + b_ch + b_dep);
   if (!base) return PEVSL_ERR_NOMEM;
+  d->wchunk = (int *)(base + b_dj + b_vi + b_tab);
+  d->wnc = wnc;
+  d->wdep = (int *)(base + b_dj + b_vi + b_tab + b_ch);
+  d->wreach = reach;
   std::vector<float> tab32(tab.size());
   for (size_t t = 0; t < tab.size(); t++) tab32[t] = (float)tab[t];
   d->pdj = (short *)base;
@@ -1408,6 +1474,8 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
   d->pnv = (int)tab.size();
   d->pbytes = b_dj + b_vi + b_tab;
   int st = memcpy_async(d->pdj, dj.data(), sizeof(short) * (size_t)nnz);
+  if (!st) st = memcpy_async(d->wchunk, ch.data(), sizeof(int) * ch.size());
+  if (!st) st = memcpy_async(d->wdep, dep.data(), sizeof(int) * dep.size());
   if (!st) st = memcpy_async(d->pvi, vi.data(), (size_t)nnz);
   if (!st) st = memcpy_async(d->pvtab, tab.data(), sizeof(double) * tab.size());
   if (!st) st = memcpy_async(d->pvtab32, tab32.data(), sizeof(float) * tab.size());
@@ -1443,7 +1511,9 @@ int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
    * aligned parts, so that a single L2 access-policy window can cover it */
   const size_t bytes_a = ((sizeof(double) * (size_t)nnz + 255) / 256) * 256;
   const size_t bytes_ja = ((sizeof(int) * (size_t)nnz + 255) / 256) * 256;
-  const size_t bytes_ia = sizeof(int) * (size_t)(nr + 1);
+  /* 256-byte multiple: a staged copy of row pointers rounded up to 16
+   * bytes stays inside the block */
+  const size_t bytes_ia = ((sizeof(int) * (size_t)(nr + 1) + 255) / 256) * 256;
   char *base = (char *)alloc_dev(bytes_a + bytes_ja + bytes_ia);
   if (!base) {
     free(d);

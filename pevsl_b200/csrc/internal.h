@@ -60,7 +60,22 @@ typedef struct pevsl_devcsr {
   float *pvtab32;
   int pnv;
   size_t pbytes;
+  /* row chunks of the staged filter kernels (packed matrices only): chunk c
+   * holds rows wchunk[2c] .. wchunk[2c+2]-1 and entries wchunk[2c+1] ..
+   * wchunk[2c+3]-1; every chunk starts at a multiple of 4 rows and holds at
+   * most PEVSL_WAVE_RMAX rows and (unless one 4-row group alone exceeds it)
+   * PEVSL_WAVE_EMAX entries; wnc chunks, then the sentinel (nrows, nnz) */
+  int *wchunk;
+  int wnc;
+  /* per chunk c, wdep[2c] .. wdep[2c+1]: the chunks holding a column of one
+   * of c's rows or a row with a column in c (a superset of both), and
+   * wreach = max over c of the distance to either end */
+  int *wdep;
+  int wreach;
 } pevsl_devcsr;
+
+#define PEVSL_WAVE_RMAX 256
+#define PEVSL_WAVE_EMAX 4096
 
 /* The device matrix behind a Parcsr, or NULL if it was never set up here. */
 pevsl_devcsr *pevsl_devcsr_of(const pevsl_Parcsr *A);

@@ -1,7 +1,8 @@
 """CPU test of bench.py's reference arm (`--impl reference`): on the small
 20^3 workload it prints one JSON line with the fields of the bench contract,
-and the process runs the reference's own code only -- this library's shared
-object is never loaded."""
+its per-slice counts and slice ends are the reference build's own run of the
+workload (tests/golden/pipelines.json), and the process runs the reference's
+own code only -- this library's shared object is never loaded."""
 import json
 import os
 import subprocess
@@ -9,7 +10,7 @@ import sys
 
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, golden
 
 REF_SO = os.path.join(ROOT, "oracle", "_ref", "libpevsl_ref.so")
 
@@ -40,5 +41,11 @@ def test_reference_arm_contract_and_isolation():
     assert out["e2e"] == {"value": out["value"], "unit": "eigenpairs/s",
                           "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert out["config"]["workload"] == "lap20_5slices"
+    # the extrapolation uses the reference build's own run of the workload
+    g = golden("pipelines.json")["lap20_lantr_gauss"]
+    assert out["config"]["slice_ends"] == g["sli"]
+    assert out["config"]["filter_degree_per_slice"] == g["deg"]
+    assert out["config"]["lanczos_steps_per_slice"] == g["its"]
+    assert out["config"]["nev_per_slice"] == g["nev"]
     loaded = [ln for ln in p.stdout.splitlines() if ln.startswith("LOADED")]
     assert loaded == ["LOADED False True"]

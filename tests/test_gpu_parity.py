@@ -156,6 +156,39 @@ def test_parvecs_gemv_gemtv(gpu):
     lib.pEVSL_ParvecsFree(C.byref(X))
 
 
+@pytest.mark.parametrize("n,k,m", [(10007, 53, 70), (777, 300, 129), (65, 4, 1), (3, 17, 64)])
+def test_dense_products_on_tensor_cores(gpu, n, k, m):
+    """The DMMA products of the solvers (Ritz vectors U = V Y, Gram
+    matrices C = V' W) against numpy's FP64 products on ragged shapes (tiles
+    of 64 and panels of 16 cut through rows, columns and the inner
+    dimension), within 1e-13 of the largest entry, and identical bits on a
+    second call (fixed reduction order)."""
+    lib = pv.load()
+    for f in (lib.pEVSL_B200_GemmNN, lib.pEVSL_B200_GemmTN):
+        f.argtypes = [C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_long,
+                      C.c_void_p, C.c_long]
+    rng = np.random.default_rng(n + k + m)
+    ldv = n + 3
+    V = rng.standard_normal((k, ldv))   # column-major n x k with leading dimension ldv
+    Y = rng.standard_normal((m, k))     # column-major k x m
+    W = rng.standard_normal((m, ldv))   # column-major n x m
+    dV, dY, dW = pv.Vector(k * ldv, V.ravel()), pv.Vector(m * k, Y.ravel()), pv.Vector(m * ldv, W.ravel())
+    dU, dC = pv.Vector(m * n), pv.Vector(k * m)
+    outs = []
+    for _ in range(2):
+        assert lib.pEVSL_B200_GemmNN(n, k, m, dV.pv.data, ldv, dY.pv.data, k, dU.pv.data, n) == 0
+        assert lib.pEVSL_B200_GemmTN(n, k, m, dV.pv.data, ldv, dW.pv.data, ldv, dC.pv.data, k) == 0
+        assert lib.pEVSL_B200_Sync() == 0
+        outs.append((dU.get().reshape(m, n), dC.get().reshape(m, k)))
+    Vn, Wn = V[:, :n].T, W[:, :n].T
+    U_ref, C_ref = Vn @ Y.T, Vn.T @ Wn
+    assert np.max(np.abs(outs[0][0].T - U_ref)) <= 1e-13 * np.max(np.abs(U_ref))
+    assert np.max(np.abs(outs[0][1].T - C_ref)) <= 1e-13 * np.max(np.abs(C_ref))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
+    for x in (dV, dY, dW, dU, dC):
+        x.free()
+
+
 def test_rng_glibc_stream_matches_reference_formula(gpu, oracle):
     lib = pv.load()
     n = 7777
@@ -584,6 +617,68 @@ def test_interleaved_filter_plain_entries_bit_identical(gpu):
         assert one["nev"] == b["nev"] == cnt and one["its"] == b["its"]
         assert np.array_equal(one["lam"], b["lam"]) and np.array_equal(one["res"], b["res"])
         assert np.all(b["res"] < 1e-8) and np.all(b["res"] / np.abs(b["lam"]) <= 1e-8)
+    M.free()
+
+
+def _banded_heavy_matrix(n, seed):
+    """Symmetric packed-eligible matrix: 6 random off-diagonals per row within
+    +-30000 columns, values from a set of 64, and heavy rows of 1500
+    entries: one alone and four in one 4-row group (the row chunk holding
+    those four exceeds the 4096 entries a staged chunk can hold and takes
+    the unstaged path)."""
+    rng = np.random.default_rng(seed)
+    vals = np.round(rng.standard_normal(64), 3)
+    r, c = [], []
+    for _ in range(3):
+        off = rng.integers(1, 30000, size=n)
+        rows = np.arange(n)
+        keep = rows + off < n
+        r.append(rows[keep])
+        c.append(rows[keep] + off[keep])
+    h0 = n // 2 - (n // 2) % 4
+    for h in (n // 5, h0, h0 + 1, h0 + 2, h0 + 3):
+        cols = np.unique(rng.integers(max(0, h - 30000), min(n, h + 30000), size=1600))
+        cols = cols[cols != h][:1500]
+        r.append(np.full(len(cols), h))
+        c.append(cols)
+    r, c = np.concatenate(r), np.concatenate(c)
+    key = np.unique(np.minimum(r, c) * n + np.maximum(r, c))
+    r, c = key // n, key % n
+    v = vals[rng.integers(0, 64, size=len(r))]
+    rows = np.concatenate([r, c, np.arange(n)])
+    cols = np.concatenate([c, r, np.arange(n)])
+    vv = np.concatenate([v, v, np.full(n, 40.0)])
+    order = np.lexsort((cols, rows))
+    rows, cols, vv = rows[order], cols[order], vv[order]
+    ia = np.zeros(n + 1, np.int32)
+    np.add.at(ia, rows + 1, 1)
+    ia = np.cumsum(ia).astype(np.int32)
+    return Csr(n, ia, cols.astype(np.int32), vv.astype(np.float64))
+
+
+def test_staged_filter_heavy_rows_bit_identical(gpu):
+    """The staged interleaved filter on a scattered matrix with heavy rows
+    (some row chunks exceed the staging buffer and read their entries from
+    global memory): three slices in lockstep give every slice the bits of
+    solving it alone with the one-vector kernel, after 40 Lanczos steps of
+    degree-60 filters."""
+    A = _banded_heavy_matrix(70001, 5)
+    M = dev_matrix(A)
+    rows = np.repeat(np.arange(A.n), np.diff(A.ia))
+    rad = np.bincount(rows, weights=np.abs(A.a), minlength=A.n) - 40.0
+    lmin, lmax = 40.0 - rad.max() - 1.0, 40.0 + rad.max() + 1.0
+    edges = np.linspace(39.0, 41.0, 4)
+    intvs = [[edges[i], edges[i + 1], lmin, lmax] for i in range(3)]
+    fl = [pv.findpol(iv, deg_in=61)[1] for iv in intvs]
+    v = np.cos(np.arange(A.n) * 0.37)
+    with pv.Instance(M) as ev:
+        r, batch = pv.cheblannr_batch(ev, intvs, [40] * 3, 1e-8, v, fl)
+    for iv, f, b in zip(intvs, fl, batch):
+        with pv.Instance(M) as ev:
+            r1, (one,) = pv.cheblannr_batch(ev, [iv], [40], 1e-8, v, [f])
+        assert one["status"] == b["status"] and one["nev"] == b["nev"] and one["its"] == b["its"]
+        if b["status"] == 0:
+            assert np.array_equal(one["lam"], b["lam"]) and np.array_equal(one["res"], b["res"])
     M.free()
 
 
