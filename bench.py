@@ -738,7 +738,10 @@ def kernel_case(args):
                  in lockstep; prints the filter's live timing (CUDA events)
                  and HBM fraction per degree;
     (a forced degree d gives a filter of degree d - 1, as in the reference)
-      pipeline   one whole batched solve of --workload (for launch lists)."""
+      pipeline   one whole batched solve of --workload (for launch lists);
+      gemm       the DMMA products: Ritz vectors U = V Y and Gram matrix
+                 V' U with n = --grid^3, k = --degree, m = 128 (device
+                 time and TFLOP/s of each)."""
     import pevsl_b200 as pv
     from pevsl_b200.problems import laplacian
     if args.kernel_case == "c4_filter":
@@ -771,6 +774,35 @@ def kernel_case(args):
                               "frac": b / ms / 1e6 / peak, "peak": peak, "peak_source": kind}
         M.free()
         print(json.dumps(out))
+        return
+    if args.kernel_case == "gemm":
+        # the two DMMA products at the size of one C2 slice's Ritz step:
+        # U = V Y (n = 1e6, k = --degree Lanczos vectors, m = 128 Ritz vectors)
+        # and the Gram matrix C = V' W (W = U)
+        lib = pv.load()
+        for f in (lib.pEVSL_B200_GemmNN, lib.pEVSL_B200_GemmTN):
+            f.argtypes = [C.c_long, C.c_int, C.c_int, C.c_void_p, C.c_long, C.c_void_p, C.c_long,
+                          C.c_void_p, C.c_long]
+        n, k, m = args.grid ** 3, args.degree, 128
+        V = pv.Vector(n * k, np.cos(np.arange(n * k) * 1e-3))
+        Y = pv.Vector(k * m, np.sin(np.arange(k * m) * 0.1))
+        U, G = pv.Vector(n * m), pv.Vector(k * m)
+        lib.pEVSL_B200_EventRecord(0)
+        for _ in range(2):
+            lib.pEVSL_B200_GemmNN(n, k, m, V.pv.data, n, Y.pv.data, k, U.pv.data, n)
+        lib.pEVSL_B200_EventRecord(1)
+        for _ in range(2):
+            lib.pEVSL_B200_GemmTN(n, k, m, V.pv.data, n, U.pv.data, n, G.pv.data, k)
+        lib.pEVSL_B200_EventRecord(2)
+        t_nn = lib.pEVSL_B200_EventElapsedMs(0, 1) / 2
+        t_tn = lib.pEVSL_B200_EventElapsedMs(1, 2) / 2
+        fl = 2.0 * n * k * m
+        print(json.dumps({"kernel_case": "gemm", "n": n, "k": k, "m": m,
+                          "gemm_nn_ms": t_nn, "gemm_nn_tflops": fl / t_nn / 1e9,
+                          "gemm_tn_ms": t_tn, "gemm_tn_tflops": fl / t_tn / 1e9,
+                          "gemm_nn_GBps": 8.0 * (n * k * ((m + 63) // 64) + n * m) / t_nn / 1e6}))
+        for x in (V, Y, U, G):
+            x.free()
         return
     if args.kernel_case == "pipeline":
         w = WORKLOADS[args.workload]
@@ -841,7 +873,7 @@ def main():
     ap.add_argument("--degree", type=int, default=16,
                     help="filter degree of the cheb_batch kernel case")
     ap.add_argument("--kernel-case", choices=["cheb_step", "cheb_batch", "kpm_step", "gen_filter",
-                                              "c4_filter", "pipeline"],
+                                              "c4_filter", "pipeline", "gemm"],
                     help="run a few launches of one kernel (for ncu) and exit")
     ap.add_argument("--grid", type=int, default=128)
     ap.add_argument("--batch", type=int, default=4)

@@ -216,27 +216,22 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_tma(const __grid_constant__ IlT
       int j = g.ia[lr];
       double r = 0.0;
       if (!big) {
-        for (; j + 3 < e; j += 4) {
-          const int c0 = g0 + g.dj[j - jdj], c1 = g0 + g.dj[j + 1 - jdj];
-          const int c2 = g0 + g.dj[j + 2 - jdj], c3 = g0 + g.dj[j + 3 - jdj];
-          const double a0 = vt[g.vi[j - jvi]], a1 = vt[g.vi[j + 1 - jvi]];
-          const double a2 = vt[g.vi[j + 2 - jvi]], a3 = vt[g.vi[j + 3 - jvi]];
-          const unsigned l0 = (unsigned)(c0 - r0), l1 = (unsigned)(c1 - r0);
-          const unsigned l2 = (unsigned)(c2 - r0), l3 = (unsigned)(c3 - r0);
-          const double x0 = l0 < (unsigned)nr ? g.x[l0 * S + sl] : __ldg(a.Xk + (size_t)c0 * S + sl);
-          const double x1 = l1 < (unsigned)nr ? g.x[l1 * S + sl] : __ldg(a.Xk + (size_t)c1 * S + sl);
-          const double x2 = l2 < (unsigned)nr ? g.x[l2 * S + sl] : __ldg(a.Xk + (size_t)c2 * S + sl);
-          const double x3 = l3 < (unsigned)nr ? g.x[l3 * S + sl] : __ldg(a.Xk + (size_t)c3 * S + sl);
-          r = __dadd_rn(r, __dmul_rn(a0, x0));
-          r = __dadd_rn(r, __dmul_rn(a1, x1));
-          r = __dadd_rn(r, __dmul_rn(a2, x2));
-          r = __dadd_rn(r, __dmul_rn(a3, x3));
-        }
-        for (; j < e; j++) {
-          const int c0 = g0 + g.dj[j - jdj];
-          const unsigned l0 = (unsigned)(c0 - r0);
-          const double x0 = l0 < (unsigned)nr ? g.x[l0 * S + sl] : __ldg(a.Xk + (size_t)c0 * S + sl);
-          r = __dadd_rn(r, __dmul_rn(vt[g.vi[j - jvi]], x0));
+        /* up to 8 entries' gathers in flight, then added in entry order
+         * (an entry past the row end is skipped, never added as zero) */
+        for (; j < e; j += 8) {
+          double xv[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            xv[u] = 0.0;
+            if (j + u < e) {
+              const int cu = g0 + g.dj[j + u - jdj];
+              const unsigned lu = (unsigned)(cu - r0);
+              xv[u] = lu < (unsigned)nr ? g.x[lu * S + sl] : __ldg(a.Xk + (size_t)cu * S + sl);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (j + u < e) r = __dadd_rn(r, __dmul_rn(vt[g.vi[j + u - jvi]], xv[u]));
         }
       } else {
         for (; j < e; j++) {
@@ -434,7 +429,8 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_wave(const __grid_constant__ Il
         const int big = e1 - e0 > kEmax;
         const int jdj = e0 & ~7, jvi = e0 & ~15;
         const unsigned b_ia = round16(4u * (unsigned)(r1 + 1 - r0));
-        const unsigned b_x = 8u * S * (unsigned)(r1 - r0);
+        /* S = 1: an odd row count stages one row less (16-byte copies) */
+        const unsigned b_x = (8u * S * (unsigned)(r1 - r0)) & ~15u;
         const unsigned b_dj = big ? 0u : round16(2u * (unsigned)(e1 - jdj));
         const unsigned b_vi = big ? 0u : round16((unsigned)(e1 - jvi));
         g.r0 = r0;
@@ -465,7 +461,9 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_wave(const __grid_constant__ Il
     const int r0 = g.r0;
     if (r0 < 0) return;
     const int k = hdr_k[2 * s], c = hdr_k[2 * s + 1];
-    const int r1 = g.r1, nr = r1 - r0, jdj = g.jdj, jvi = g.jvi, big = g.big;
+    const int r1 = g.r1, jdj = g.jdj, jvi = g.jvi, big = g.big;
+    const int nrows = r1 - r0;
+    const int nr = S == 1 ? (nrows & ~1) : nrows; /* rows staged in g.x */
     const double *Xg = wave_buf(a, k - 1);                 /* T_{k-1}: gathered  */
     const double *Xm = k >= 2 ? wave_buf(a, k - 2) : nullptr; /* T_{k-2}: own rows */
     double *Xo = const_cast<double *>(wave_buf(a, k));     /* T_k (over T_{k-2}) */
@@ -473,11 +471,11 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_wave(const __grid_constant__ Il
     const double *mu0 = a.mu, *muk = a.mu + (size_t)k * S;
     int fresh;
     const int ny = wave_terms(k, a.maxdeg, a.defer, &fresh);
-    for (int p = tid; p < nr * S; p += kCW * 32) {
+    for (int p = tid; p < nrows * S; p += kCW * 32) {
       const int lr = p / S, sl = p % S;
       const int row = r0 + lr;
       const size_t me = (size_t)row * S + sl;
-      const double x = g.x[p];
+      const double x = lr < nr ? g.x[p] : __ldcg(Xg + me);
       const double xm1 = Xm ? __ldcg(Xm + me) : 0.0;
       const double yold = (ny > 0 && !fresh) ? __ldcg(a.Y + me) : 0.0;
       const int g0 = row & ~31;
@@ -485,27 +483,21 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_wave(const __grid_constant__ Il
       int j = g.ia[lr];
       double r = 0.0;
       if (!big) {
-        for (; j + 3 < e; j += 4) {
-          const int c0 = g0 + g.dj[j - jdj], c1 = g0 + g.dj[j + 1 - jdj];
-          const int c2 = g0 + g.dj[j + 2 - jdj], c3 = g0 + g.dj[j + 3 - jdj];
-          const double a0 = vt[g.vi[j - jvi]], a1 = vt[g.vi[j + 1 - jvi]];
-          const double a2 = vt[g.vi[j + 2 - jvi]], a3 = vt[g.vi[j + 3 - jvi]];
-          const unsigned l0 = (unsigned)(c0 - r0), l1 = (unsigned)(c1 - r0);
-          const unsigned l2 = (unsigned)(c2 - r0), l3 = (unsigned)(c3 - r0);
-          const double x0 = l0 < (unsigned)nr ? g.x[l0 * S + sl] : __ldcg(Xg + (size_t)c0 * S + sl);
-          const double x1 = l1 < (unsigned)nr ? g.x[l1 * S + sl] : __ldcg(Xg + (size_t)c1 * S + sl);
-          const double x2 = l2 < (unsigned)nr ? g.x[l2 * S + sl] : __ldcg(Xg + (size_t)c2 * S + sl);
-          const double x3 = l3 < (unsigned)nr ? g.x[l3 * S + sl] : __ldcg(Xg + (size_t)c3 * S + sl);
-          r = __dadd_rn(r, __dmul_rn(a0, x0));
-          r = __dadd_rn(r, __dmul_rn(a1, x1));
-          r = __dadd_rn(r, __dmul_rn(a2, x2));
-          r = __dadd_rn(r, __dmul_rn(a3, x3));
-        }
-        for (; j < e; j++) {
-          const int c0 = g0 + g.dj[j - jdj];
-          const unsigned l0 = (unsigned)(c0 - r0);
-          const double x0 = l0 < (unsigned)nr ? g.x[l0 * S + sl] : __ldcg(Xg + (size_t)c0 * S + sl);
-          r = __dadd_rn(r, __dmul_rn(vt[g.vi[j - jvi]], x0));
+        /* up to 8 entries' gathers in flight, added in entry order */
+        for (; j < e; j += 8) {
+          double xv[8];
+#pragma unroll
+          for (int u = 0; u < 8; u++) {
+            xv[u] = 0.0;
+            if (j + u < e) {
+              const int cu = g0 + g.dj[j + u - jdj];
+              const unsigned lu = (unsigned)(cu - r0);
+              xv[u] = lu < (unsigned)nr ? g.x[lu * S + sl] : __ldcg(Xg + (size_t)cu * S + sl);
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; u++)
+            if (j + u < e) r = __dadd_rn(r, __dmul_rn(vt[g.vi[j + u - jvi]], xv[u]));
         }
       } else {
         for (; j < e; j++) {
@@ -692,7 +684,7 @@ bool il_wave_usable(const pevsl_devcsr *A, int S) {
     const char *e = getenv("PEVSL_B200_IL_WAVE");
     v = e ? atoi(e) != 0 : 1;
   }
-  return v && il_tma_usable(A, S) && S >= 2 && A->wdep != nullptr;
+  return v && il_tma_usable(A, S) && A->wdep != nullptr;
 }
 
 size_t il_wave_ints(const pevsl_devcsr *A, int maxdeg) {
@@ -712,6 +704,7 @@ int cheb_filter_il_wave(const pevsl_devcsr *A, int S, const double *X0, double *
     return PEVSL_ERR_CUDA;
   int grid = 0;
   switch (S) {
+    case 1: grid = wave_grid<1>(); break;
     case 2: grid = wave_grid<2>(); break;
     case 4: grid = wave_grid<4>(); break;
     case 8: grid = wave_grid<8>(); break;
@@ -748,6 +741,7 @@ int cheb_filter_il_wave(const pevsl_devcsr *A, int S, const double *X0, double *
     const long total = (long)a.nc * a.D;
     int st;
     switch (S) {
+      case 1: st = launch_il_wave<1>(a, total); break;
       case 2: st = launch_il_wave<2>(a, total); break;
       case 4: st = launch_il_wave<4>(a, total); break;
       case 8: st = launch_il_wave<8>(a, total); break;

@@ -258,11 +258,14 @@ static void il_partition(int ne, const FilterJob *jobs, bool fp32, std::vector<I
       }
     for (size_t c0 = 0; c0 < L.size(); c0 += kMaxBatch) {
       const int cnt = (int)PEVSL_MIN((size_t)kMaxBatch, L.size() - c0);
-      if (cnt < 2) continue;
+      /* one slice takes the interleaved path only in the wavefront form
+       * (S = 1; the vectors are then plain vectors) */
+      const bool one = cnt == 1 && il_wave_usable(A, 1);
+      if (cnt < 2 && !one) continue;
       IlGroup G;
       G.A = A;
       G.cnt = cnt;
-      G.S = il_width(cnt);
+      G.S = one ? 1 : il_width(cnt);
       G.maxdeg = 0;
       G.cc = J.pol->cc;
       G.dd = J.pol->dd;
