@@ -376,19 +376,21 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_wave(const __grid_constant__ Il
   const long total = (long)a.nc * a.D;
 
   if (warp == kCW) {
-    /* producer warp: claim, wait for the dependencies, stage */
+    /* producer warp: claim (one item ahead), wait for the dependencies,
+     * stage.  A block holds at most two claimed items, the earlier one
+     * staged first, so every wait still ends (items depend only on items
+     * claimed before them). */
+    unsigned next = 0;
+    if (lane == 0) next = atomicAdd(a.ctr, 1u);
+    next = __shfl_sync(0xffffffffu, next, 0);
     for (int it = 0;; it++) {
       const int s = it % NST;
       Stage<S> &g = st[s];
-      int ok = 1;
-      if (it >= NST && lane == 0) ok = mbar_wait(&empty[s], ((it / NST) - 1) & 1);
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      if (!ok) return;
-      unsigned idx = 0;
-      if (lane == 0) idx = atomicAdd(a.ctr, 1u);
-      idx = __shfl_sync(0xffffffffu, idx, 0);
+      const unsigned idx = next;
       if ((long)idx >= total) {
-        if (lane == 0) {
+        int ok = 1;
+        if (it >= NST && lane == 0) ok = mbar_wait(&empty[s], ((it / NST) - 1) & 1);
+        if (lane == 0 && ok) {
           g.r0 = -1;
           mbar_arrive(&full[s]);
         }
@@ -397,35 +399,58 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_wave(const __grid_constant__ Il
       int j, c;
       wave_item((long)idx, a.nc, a.D, a.Lp, &j, &c);
       const int k = a.k0 + j;
+      /* the chunk's bounds (lanes 0..3), independent of the waits below */
+      const int bnd = lane < 4 ? __ldg(a.wchunk + 2 * c + lane) : 0;
       if (j > 0) {
-        /* degree k - 1 done on every chunk of the dependency range */
+        /* degree k - 1 done on every chunk of the dependency range: each
+         * lane reads its (up to 4) flags at once, then spins on the late */
         const int lo = __ldg(a.wdep + 2 * c), hi = __ldg(a.wdep + 2 * c + 1);
         const int need = kCW * (k - 1);
         int fine = 1;
-        for (int q = lo + lane; q <= hi && fine; q += 32) {
-          unsigned spin = 0;
-          while (ld_acquire(a.done + q) < need) {
-            if (++spin > kDepSpins) {
-              atomicExch(&g_tma_err, 2u);
-              fine = 0;
-              break;
+        for (int q0 = lo; q0 <= hi && fine; q0 += 128) {
+          int v[4];
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int q = q0 + lane + 32 * u;
+            v[u] = q <= hi ? ld_acquire(a.done + q) : need;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; u++) {
+            const int q = q0 + lane + 32 * u;
+            unsigned spin = 0;
+            while (v[u] < need) {
+              if (++spin > kDepSpins) {
+                atomicExch(&g_tma_err, 2u);
+                fine = 0;
+                break;
+              }
+              __nanosleep(32);
+              v[u] = ld_acquire(a.done + q);
             }
-            __nanosleep(32);
           }
         }
         if (!__all_sync(0xffffffffu, fine)) {
           /* give up: end the consumers after what they hold */
-          if (lane == 0) {
+          int ok = 1;
+          if (it >= NST && lane == 0) ok = mbar_wait(&empty[s], ((it / NST) - 1) & 1);
+          if (lane == 0 && ok) {
             g.r0 = -1;
             mbar_arrive(&full[s]);
           }
           return;
         }
       }
+      /* the next claim overlaps the stage wait and the copies */
+      if (lane == 0) next = atomicAdd(a.ctr, 1u);
+      next = __shfl_sync(0xffffffffu, next, 0);
+      const int r0 = __shfl_sync(0xffffffffu, bnd, 0), e0 = __shfl_sync(0xffffffffu, bnd, 1);
+      const int r1 = __shfl_sync(0xffffffffu, bnd, 2), e1 = __shfl_sync(0xffffffffu, bnd, 3);
+      int ok = 1;
+      if (it >= NST && lane == 0) ok = mbar_wait(&empty[s], ((it / NST) - 1) & 1);
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) return;
       if (lane == 0) {
         fence_proxy_async_global();
-        const int r0 = __ldg(a.wchunk + 2 * c), e0 = __ldg(a.wchunk + 2 * c + 1);
-        const int r1 = __ldg(a.wchunk + 2 * c + 2), e1 = __ldg(a.wchunk + 2 * c + 3);
         const int big = e1 - e0 > kEmax;
         const int jdj = e0 & ~7, jvi = e0 & ~15;
         const unsigned b_ia = round16(4u * (unsigned)(r1 + 1 - r0));

@@ -471,6 +471,28 @@ def test_mixed_precision_counts_and_residuals(gpu, name):
         assert np.max(np.abs(lam - ex) / np.abs(ex)) <= 1e-10
 
 
+def test_mixed_precision_per_eigenvalue_against_fp64_run(gpu):
+    """The mixed form against the FP64 run on the same inputs, eigenvalue by
+    eigenvalue (README matrix, thick-restart bounds, Gaussian stream): every
+    slice whose ends the FP32 moments leave in place has the FP64 run's
+    count, and each of its eigenvalues agrees with the FP64 run's within
+    1e-10 relative (the largest error is reported in the message)."""
+    g = golden("pipelines.json")["lap20_lantr_gauss"]
+    A = dev_matrix(laplacian(*g["grid"]))
+    spec = pv.SliceRun(**g["spec"])
+    r64 = pv.solve_interval(A, spec, batched=True, precision=pv.PREC_FP64)
+    r32 = pv.solve_interval(A, spec, batched=True, precision=pv.PREC_MIXED)
+    assert r64.status == 0 and r32.status == 0
+    worst = 0.0
+    for sl in range(len(r64.nev)):
+        if rel(r32.sli[sl:sl + 2], r64.sli[sl:sl + 2]) > 1e-12:
+            continue  # the FP32 moments moved this slice's ends
+        assert r32.nev[sl] == r64.nev[sl]
+        err = np.abs(r32.lam[sl] - r64.lam[sl]) / np.abs(r64.lam[sl])
+        worst = max(worst, float(err.max()))
+    assert worst <= 1e-10, f"largest per-eigenvalue error against FP64: {worst:.3e}"
+
+
 # ---------------------------------------------------------------- batching forms
 def _lap_slices(grid, a, b, ns, seed=3):
     """Bounds from the analytic spectrum, slices evenly spaced, filters."""
