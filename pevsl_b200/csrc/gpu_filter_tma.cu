@@ -295,7 +295,7 @@ __device__ __forceinline__ const double *wave_buf(const IlWaveArgs &a, int k) {
 }
 
 /* items with time < t */
-__device__ __forceinline__ long wave_before(long t, int nc, int D, int Lp) {
+__host__ __device__ __forceinline__ long wave_before(long t, int nc, int D, int Lp) {
   long f = 0;
   for (int j = 0; j < D; j++) {
     const long v = t - (long)j * Lp;
@@ -304,7 +304,7 @@ __device__ __forceinline__ long wave_before(long t, int nc, int D, int Lp) {
   return f;
 }
 
-__device__ __forceinline__ void wave_item(long idx, int nc, int D, int Lp, int *j, int *c) {
+__host__ __device__ __forceinline__ void wave_item(long idx, int nc, int D, int Lp, int *j, int *c) {
   long lo = 0, hi = nc + (long)(D - 1) * Lp; /* before(lo) <= idx < before(hi) */
   while (hi - lo > 1) {
     const long mid = (lo + hi) >> 1;
@@ -320,7 +320,7 @@ __device__ __forceinline__ void wave_item(long idx, int nc, int D, int Lp, int *
 /* terms of the deferred sum that degree k adds (the host's il_terms in
  * closed form): the first update at degree min(defer, 2), then every defer
  * degrees, and the last at maxdeg */
-__device__ __forceinline__ int wave_terms(int k, int maxdeg, int defer, int *fresh) {
+__host__ __device__ __forceinline__ int wave_terms(int k, int maxdeg, int defer, int *fresh) {
   const int first = defer < 2 ? defer : 2;
   *fresh = 0;
   if (k < first) {
@@ -798,3 +798,23 @@ int il_tma_error() {
 }
 
 }  // namespace pv
+
+extern "C" {
+
+/* the wavefront's claim order and deferral schedule, on the host (the same
+ * functions the kernel runs), for tests */
+int pEVSL_B200_WaveItem(int nc, int D, int Lp, long idx, int *j, int *c) {
+  if (nc <= 0 || D <= 0 || Lp <= 0 || idx < 0 || idx >= (long)nc * D || !j || !c)
+    return PEVSL_ERR_ARG;
+  pv::wave_item(idx, nc, D, Lp, j, c);
+  return 0;
+}
+
+int pEVSL_B200_WaveTerms(int k, int maxdeg, int defer, int *fresh) {
+  int f = 0;
+  const int ny = pv::wave_terms(k, maxdeg, defer, &f);
+  if (fresh) *fresh = f;
+  return ny;
+}
+
+}  // extern "C"

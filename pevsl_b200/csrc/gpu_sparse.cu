@@ -1361,6 +1361,69 @@ int pEVSL_ParcsrCreate(int nrow, int ncol, int *row_starts, int *col_starts, pev
   return 0;
 }
 
+/* Row chunks of the staged filter kernels and their dependency ranges, from
+ * a host CSR (also exported for tests; see include/pevsl_b200.h). */
+extern "C" int pEVSL_B200_WaveLayout(int n, const int *ia, const int *ja, int *nchunks,
+                                     int *chunks, int *deps, int *reach) {
+  if (n < 0 || !ia || !ja || !nchunks) return PEVSL_ERR_ARG;
+  /* chunks: at most RMAX rows and EMAX entries, starting at multiples of 4
+   * rows (16-byte aligned row-pointer and vector copies) */
+  std::vector<int> ch;
+  for (int r = 0; r < n;) {
+    ch.push_back(r);
+    ch.push_back(ia[r]);
+    int e = PEVSL_MIN(n, r + 4);
+    while (e < n && e - r < PEVSL_WAVE_RMAX) {
+      const int e2 = PEVSL_MIN(n, e + 4);
+      if (ia[e2] - ia[r] > PEVSL_WAVE_EMAX) break;
+      e = e2;
+    }
+    r = e;
+  }
+  const int wnc = (int)(ch.size() / 2);
+  ch.push_back(n);
+  ch.push_back(ia[n]);
+  /* dependency ranges: [lo, hi] of the chunks of the columns of its rows,
+   * widened to every chunk that has a column in it (prefix max of hi /
+   * suffix min of lo; a superset for unsymmetric patterns) */
+  std::vector<int> starts((size_t)wnc + 1);
+  for (int c = 0; c <= wnc; c++) starts[(size_t)c] = ch[(size_t)2 * c];
+  auto chunk_of = [&](int col) {
+    return (int)(std::upper_bound(starts.begin(), starts.end() - 1, col) - starts.begin()) - 1;
+  };
+  std::vector<int> clo((size_t)wnc), chi((size_t)wnc);
+  for (int c = 0; c < wnc; c++) {
+    int mn = INT32_MAX, mx = -1;
+    for (int k = ia[starts[(size_t)c]]; k < ia[starts[(size_t)c + 1]]; k++) {
+      if (ja[k] < 0 || ja[k] >= n) return PEVSL_ERR_ARG;
+      mn = PEVSL_MIN(mn, ja[k]);
+      mx = PEVSL_MAX(mx, ja[k]);
+    }
+    clo[(size_t)c] = mx < 0 ? c : PEVSL_MIN(c, chunk_of(mn));
+    chi[(size_t)c] = mx < 0 ? c : PEVSL_MAX(c, chunk_of(mx));
+  }
+  std::vector<int> pmax((size_t)wnc), smin((size_t)wnc);
+  for (int c = 0; c < wnc; c++) pmax[(size_t)c] = PEVSL_MAX(chi[(size_t)c], c ? pmax[(size_t)c - 1] : -1);
+  for (int c = wnc - 1; c >= 0; c--)
+    smin[(size_t)c] = PEVSL_MIN(clo[(size_t)c], c + 1 < wnc ? smin[(size_t)c + 1] : INT32_MAX);
+  int rch = 0;
+  for (int c = 0; c < wnc; c++) {
+    /* first c' with pmax >= c, last c' with smin <= c (both monotone) */
+    const int rlo = (int)(std::lower_bound(pmax.begin(), pmax.end(), c) - pmax.begin());
+    const int rhi = (int)(std::upper_bound(smin.begin(), smin.end(), c) - smin.begin()) - 1;
+    const int lo = PEVSL_MIN(clo[(size_t)c], rlo), hi = PEVSL_MAX(chi[(size_t)c], rhi);
+    if (deps) {
+      deps[(size_t)2 * c] = lo;
+      deps[(size_t)2 * c + 1] = hi;
+    }
+    rch = PEVSL_MAX(rch, PEVSL_MAX(c - lo, hi - c));
+  }
+  *nchunks = wnc;
+  if (chunks) memcpy(chunks, ch.data(), sizeof(int) * ch.size());
+  if (reach) *reach = rch;
+  return 0;
+}
+
 /* Upload the caller's host CSR (the local rows, global column indices) as
  * one device CSR (SRC/parcsr.c:70-283 without the split and halo plan). */
 /* The packed copy of a matrix's entries, when every column lies within
@@ -1401,57 +1464,12 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
       vi[(size_t)k] = (unsigned char)hval[h];
     }
   }
-  /* row chunks of the staged kernels: at most RMAX rows and EMAX entries,
-   * starting at multiples of 4 rows (16-byte aligned row-pointer and
-   * vector copies) */
-  std::vector<int> ch;
-  for (int r = 0; r < nr;) {
-    ch.push_back(r);
-    ch.push_back(Ai->ia[r]);
-    int e = PEVSL_MIN(nr, r + 4);
-    while (e < nr && e - r < PEVSL_WAVE_RMAX) {
-      const int e2 = PEVSL_MIN(nr, e + 4);
-      if (Ai->ia[e2] - Ai->ia[r] > PEVSL_WAVE_EMAX) break;
-      e = e2;
-    }
-    r = e;
-  }
-  const int wnc = (int)(ch.size() / 2);
-  ch.push_back(nr);
-  ch.push_back((int)nnz);
-  /* dependency ranges of the chunks: [lo, hi] of the chunks of the columns
-   * of its rows, widened to every chunk that has a column in it (prefix max
-   * of hi / suffix min of lo; a superset for unsymmetric patterns) */
-  std::vector<int> starts((size_t)wnc + 1);
-  for (int c = 0; c <= wnc; c++) starts[(size_t)c] = ch[(size_t)2 * c];
-  auto chunk_of = [&](int col) {
-    return (int)(std::upper_bound(starts.begin(), starts.end() - 1, col) - starts.begin()) - 1;
-  };
-  std::vector<int> clo((size_t)wnc), chi((size_t)wnc);
-  for (int c = 0; c < wnc; c++) {
-    int mn = INT32_MAX, mx = -1;
-    for (int k = Ai->ia[starts[(size_t)c]]; k < Ai->ia[starts[(size_t)c + 1]]; k++) {
-      mn = PEVSL_MIN(mn, Ai->ja[k]);
-      mx = PEVSL_MAX(mx, Ai->ja[k]);
-    }
-    clo[(size_t)c] = mx < 0 ? c : PEVSL_MIN(c, chunk_of(mn));
-    chi[(size_t)c] = mx < 0 ? c : PEVSL_MAX(c, chunk_of(mx));
-  }
-  std::vector<int> pmax((size_t)wnc), smin((size_t)wnc);
-  for (int c = 0; c < wnc; c++) pmax[(size_t)c] = PEVSL_MAX(chi[(size_t)c], c ? pmax[(size_t)c - 1] : -1);
-  for (int c = wnc - 1; c >= 0; c--)
-    smin[(size_t)c] = PEVSL_MIN(clo[(size_t)c], c + 1 < wnc ? smin[(size_t)c + 1] : INT32_MAX);
-  std::vector<int> dep((size_t)2 * wnc);
-  int reach = 0;
-  for (int c = 0; c < wnc; c++) {
-    /* first c' with pmax >= c, last c' with smin <= c (both monotone) */
-    const int rlo = (int)(std::lower_bound(pmax.begin(), pmax.end(), c) - pmax.begin());
-    const int rhi = (int)(std::upper_bound(smin.begin(), smin.end(), c) - smin.begin()) - 1;
-    const int lo = PEVSL_MIN(clo[(size_t)c], rlo), hi = PEVSL_MAX(chi[(size_t)c], rhi);
-    dep[(size_t)2 * c] = lo;
-    dep[(size_t)2 * c + 1] = hi;
-    reach = PEVSL_MAX(reach, PEVSL_MAX(c - lo, hi - c));
-  }
+  /* row chunks of the staged kernels and their dependency ranges */
+  int wnc = 0, reach = 0;
+  if (pEVSL_B200_WaveLayout(nr, Ai->ia, Ai->ja, &wnc, nullptr, nullptr, &reach))
+    return PEVSL_ERR_ARG;
+  std::vector<int> ch((size_t)2 * wnc + 2), dep((size_t)2 * wnc);
+  pEVSL_B200_WaveLayout(nr, Ai->ia, Ai->ja, &wnc, ch.data(), dep.data(), &reach);
   /* the parts are 256-byte multiples: a staged copy rounded up to 16 bytes
    * never leaves its part */
   const size_t b_dj = ((sizeof(short) * (size_t)nnz + 255) / 256) * 256;
