@@ -255,6 +255,9 @@ int cheb_step_il_tma(const pevsl_devcsr *A, int S, const double *Xk, const doubl
                      double *Xkp1, double *Y, double cc, double t, const double *mu0,
                      const double *muk, int ny, int fresh);
 int il_tma_error();
+/* shared-memory attributes and resident grids of the staged kernels, once
+ * per context (outside any capture) */
+int tma_init();
 /* all degrees of one interleaved filter application as wavefront launches
  * of several degrees each (gpu_filter_tma.cu): X0 = T_0, B0/B1 the two
  * recurrence blocks, Y the accumulator, mu the (maxdeg + 1) x S table,

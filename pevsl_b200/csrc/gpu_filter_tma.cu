@@ -258,6 +258,25 @@ __global__ void __launch_bounds__(kWT) k_cheb_il_tma(const __grid_constant__ IlT
   }
 }
 
+/* resident blocks of each kernel and width (index log2 S), set by tma_init */
+int g_grid_tma[5] = {0, 0, 0, 0, 0}, g_grid_wave[5] = {0, 0, 0, 0, 0};
+
+constexpr int slot_of(int S) { return S == 1 ? 0 : S == 2 ? 1 : S == 4 ? 2 : S == 8 ? 3 : 4; }
+
+/* dynamic shared memory above 48 KB and the resident grid of one kernel */
+int setup_kernel(const void *fn, size_t smem, int *grid) {
+  if (fail(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+           "cudaFuncSetAttribute"))
+    return PEVSL_ERR_CUDA;
+  int per_sm = 0;
+  if (fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWT, smem),
+           "cudaOccupancyMaxActiveBlocksPerMultiprocessor"))
+    return PEVSL_ERR_CUDA;
+  if (per_sm < 1) return PEVSL_ERR_ARG;
+  *grid = per_sm * ctx().sms;
+  return 0;
+}
+
 /* ---------------------------------------------------------------- wavefront
  * Several degrees per launch.  Item (j, c) is degree k = k0 + j on chunk c;
  * it needs degree k - 1 done on the chunks of wdep[c] (its gathers, and the
@@ -557,20 +576,8 @@ constexpr size_t wave_smem() {
 
 template <int S>
 int launch_il_wave(const IlWaveArgs &args, long total) {
-  static int grid = 0;
-  if (!grid) {
-    const void *fn = (const void *)k_cheb_il_wave<S>;
-    if (fail(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)wave_smem<S>()),
-             "cudaFuncSetAttribute"))
-      return PEVSL_ERR_CUDA;
-    int per_sm = 0;
-    if (fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWT, wave_smem<S>()),
-             "cudaOccupancyMaxActiveBlocksPerMultiprocessor"))
-      return PEVSL_ERR_CUDA;
-    if (per_sm < 1) return PEVSL_ERR_ARG;
-    grid = per_sm * ctx().sms;
-  }
+  const int grid = g_grid_wave[slot_of(S)];
+  if (grid < 1) return PEVSL_ERR_ARG; /* tma_init did not run */
   const unsigned g = (unsigned)(total < grid ? total : grid);
   k_cheb_il_wave<S><<<g, kWT, wave_smem<S>(), ctx().stream>>>(args);
   g_tma_launches++;
@@ -578,30 +585,16 @@ int launch_il_wave(const IlWaveArgs &args, long total) {
 }
 
 template <int S>
-int wave_grid() {
-  const void *fn = (const void *)k_cheb_il_wave<S>;
-  int per_sm = 0;
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)wave_smem<S>());
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWT, wave_smem<S>());
-  return per_sm * ctx().sms;
+int setup_width() {
+  if (setup_kernel((const void *)k_cheb_il_tma<S>, tma_smem<S>(), &g_grid_tma[slot_of(S)]))
+    return PEVSL_ERR_CUDA;
+  return setup_kernel((const void *)k_cheb_il_wave<S>, wave_smem<S>(), &g_grid_wave[slot_of(S)]);
 }
 
 template <int S>
 int launch_il_tma(const pevsl_devcsr *A, const IlTmaArgs &args) {
-  static int grid = 0;
-  if (!grid) {
-    const void *fn = (const void *)k_cheb_il_tma<S>;
-    if (fail(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)tma_smem<S>()),
-             "cudaFuncSetAttribute"))
-      return PEVSL_ERR_CUDA;
-    int per_sm = 0;
-    if (fail(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, kWT, tma_smem<S>()),
-             "cudaOccupancyMaxActiveBlocksPerMultiprocessor"))
-      return PEVSL_ERR_CUDA;
-    if (per_sm < 1) return PEVSL_ERR_ARG;
-    grid = per_sm * ctx().sms;
-  }
+  const int grid = g_grid_tma[slot_of(S)];
+  if (grid < 1) return PEVSL_ERR_ARG; /* tma_init did not run */
   const unsigned g = (unsigned)(A->wnc < grid ? A->wnc : grid);
   k_cheb_il_tma<S><<<g, kWT, tma_smem<S>(), ctx().stream>>>(args);
   g_tma_launches++;
@@ -727,15 +720,9 @@ int cheb_filter_il_wave(const pevsl_devcsr *A, int S, const double *X0, double *
   if (fail(cudaMemsetAsync(flags, 0, sizeof(int) * ((size_t)A->wnc + nl), ctx().stream),
            "cudaMemsetAsync"))
     return PEVSL_ERR_CUDA;
-  int grid = 0;
-  switch (S) {
-    case 1: grid = wave_grid<1>(); break;
-    case 2: grid = wave_grid<2>(); break;
-    case 4: grid = wave_grid<4>(); break;
-    case 8: grid = wave_grid<8>(); break;
-    case 16: grid = wave_grid<16>(); break;
-    default: return PEVSL_ERR_ARG;
-  }
+  if (S != 1 && S != 2 && S != 4 && S != 8 && S != 16) return PEVSL_ERR_ARG;
+  const int grid = g_grid_wave[slot_of(S)];
+  if (grid < 1) return PEVSL_ERR_ARG;
   IlWaveArgs a;
   a.n = A->nrows;
   a.nc = A->wnc;
@@ -774,6 +761,13 @@ int cheb_filter_il_wave(const pevsl_devcsr *A, int S, const double *X0, double *
     }
     if (st) return st;
   }
+  return 0;
+}
+
+int tma_init() {
+  if (setup_width<1>() || setup_width<2>() || setup_width<4>() || setup_width<8>() ||
+      setup_width<16>())
+    return PEVSL_ERR_CUDA;
   return 0;
 }
 
