@@ -195,23 +195,14 @@ int pEVSL_B200_GemmNN(long n, int k, int m, const double *V, long ldv, const dou
 int pEVSL_B200_GemmTN(long n, int k, int m, const double *V, long ldv, const double *W, long ldw,
                       double *C, long ldc);
 
-/* The staged filter kernels' layout and schedule, on the host (what the
- * kernels use; no GPU needed), for tests and diagnostics.
- * pEVSL_B200_WaveLayout: the row chunks of a CSR (n rows, ia/ja 0-based):
- * *nchunks, chunks[2c], chunks[2c+1] = first row and first entry of chunk c
- * (2 * nchunks + 2 ints, the last pair (n, nnz)), deps[2c], deps[2c+1] =
- * the chunk range it depends on in the wavefront (2 * nchunks ints), *reach
- * = the largest distance from a chunk to either end of its range; chunks and
- * deps may be NULL (then only the sizes are returned).
- * pEVSL_B200_WaveItem: the degree offset j and chunk c of claim idx in a
- * wavefront launch of D degrees over nc chunks with skew Lp.
- * pEVSL_B200_WaveTerms: how many degrees of the filter sum degree k adds
- * under deferral `defer` (1..3) in an application of degree maxdeg, and
- * whether it starts the sum. */
-int pEVSL_B200_WaveLayout(int n, const int *ia, const int *ja, int *nchunks, int *chunks,
-                          int *deps, int *reach);
-int pEVSL_B200_WaveItem(int nc, int D, int Lp, long idx, int *j, int *c);
-int pEVSL_B200_WaveTerms(int k, int maxdeg, int defer, int *fresh);
+/* The row chunks of the staged filter kernel (PEVSL_B200_IL_TMA=1), on the
+ * host (no GPU needed), for tests and diagnostics: for a CSR of n rows
+ * (ia 0-based), *nchunks and chunks[2c], chunks[2c+1] = first row and first
+ * entry of chunk c, 2 * nchunks + 2 ints, the last pair (n, nnz); chunks may
+ * be NULL (then only *nchunks is returned).  A chunk starts at a multiple of
+ * 4 rows and holds at most 256 rows and, unless one 4-row group alone holds
+ * more, 4096 entries. */
+int pEVSL_B200_ChunkLayout(int n, const int *ia, int *nchunks, int *chunks);
 
 /* Release cached device workspaces (they are reused across calls). */
 void pEVSL_B200_ReleaseWorkspace(void);

@@ -75,7 +75,6 @@ enum Ws {
   WS_GEN,       /* generalized problem: filter / KPM vectors  */
   WS_IL,        /* interleaved filter: three n x S blocks     */
   WS_ILMU,      /* interleaved filter: per-degree coefficients */
-  WS_WAVE,      /* wavefront filter: chunk progress + claim counters */
   WS_COUNT
 };
 
@@ -258,17 +257,6 @@ int il_tma_error();
 /* shared-memory attributes and resident grids of the staged kernels, once
  * per context (outside any capture) */
 int tma_init();
-/* all degrees of one interleaved filter application as wavefront launches
- * of several degrees each (gpu_filter_tma.cu): X0 = T_0, B0/B1 the two
- * recurrence blocks, Y the accumulator, mu the (maxdeg + 1) x S table,
- * defer the accumulator deferral of cheb_step_il_y; flags: il_wave_ints
- * ints of device memory (zeroed here).  Same bits as the degree-by-degree
- * launches. */
-bool il_wave_usable(const pevsl_devcsr *A, int S);
-size_t il_wave_ints(const pevsl_devcsr *A, int maxdeg);
-int cheb_filter_il_wave(const pevsl_devcsr *A, int S, const double *X0, double *B0, double *B1,
-                        double *Y, double cc, double dd, const double *mu, int maxdeg, int defer,
-                        int *flags);
 /* the staged kernel for one vector: cheb_step's recurrence (y every degree) */
 int cheb_step_tma(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1,
                   double *y, double cc, double t, double mu0, double muk, int first);

@@ -258,14 +258,11 @@ static void il_partition(int ne, const FilterJob *jobs, bool fp32, std::vector<I
       }
     for (size_t c0 = 0; c0 < L.size(); c0 += kMaxBatch) {
       const int cnt = (int)PEVSL_MIN((size_t)kMaxBatch, L.size() - c0);
-      /* one slice takes the interleaved path only in the wavefront form
-       * (S = 1; the vectors are then plain vectors) */
-      const bool one = cnt == 1 && il_wave_usable(A, 1);
-      if (cnt < 2 && !one) continue;
+      if (cnt < 2) continue;
       IlGroup G;
       G.A = A;
       G.cnt = cnt;
-      G.S = one ? 1 : il_width(cnt);
+      G.S = il_width(cnt);
       G.maxdeg = 0;
       G.cc = J.pol->cc;
       G.dd = J.pol->dd;
@@ -290,15 +287,6 @@ static size_t il_mu_doubles(const std::vector<IlGroup> &g) {
   return g.empty() ? 0 : g.back().mu_off + (size_t)(g.back().maxdeg + 1) * (size_t)g.back().S;
 }
 
-/* progress counters of the wavefront filter: the groups run one after
- * another, so one set sized for the largest serves all */
-static size_t il_wave_ws_ints(const std::vector<IlGroup> &g) {
-  size_t m = 0;
-  for (const IlGroup &G : g)
-    if (il_wave_usable(G.A, G.S)) m = PEVSL_MAX(m, il_wave_ints(G.A, G.maxdeg));
-  return m;
-}
-
 /* workspace and per-degree coefficient tables of the interleaved groups,
  * prepared outside any stream capture: row k of a group's table holds mu_k
  * of each of its slices (0 past a slice's degree, where its y then stays
@@ -311,8 +299,6 @@ static int il_prepare(int ne, const FilterJob *jobs, bool fp32) {
   if (!ws(WS_IL, sizeof(double) * il_ws_doubles(g))) return PEVSL_ERR_NOMEM;
   double *dmu = (double *)ws(WS_ILMU, sizeof(double) * il_mu_doubles(g));
   if (!dmu) return PEVSL_ERR_NOMEM;
-  const size_t wi = il_wave_ws_ints(g);
-  if (wi && !ws(WS_WAVE, sizeof(int) * wi)) return PEVSL_ERR_NOMEM;
   std::vector<double> tab(il_mu_doubles(g), 0.0);
   for (const IlGroup &G : g)
     for (int c = 0; c < G.cnt; c++) {
@@ -439,17 +425,14 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
   il_partition(ne, jobs, fp32, ig, taken);
   std::vector<std::array<const double *, 3>> ilv(ig.size()); /* vk, vkm1 per group */
   std::vector<int> ilw(ig.size(), 0);                          /* last degree added to y */
-  std::vector<char> ilw_wave(ig.size(), 0);                    /* run by the wavefront form */
   const int defer = il_defer_setting();
   if (!ig.empty()) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(ctx().stream, &cs);
     /* inside a capture the caller prepared the workspace and coefficients */
     if (cs == cudaStreamCaptureStatusNone) st = il_prepare(ne, jobs, fp32);
-    const size_t wi = il_wave_ws_ints(ig);
     if (!st && (!ctx().ws[WS_IL] || ctx().wsz[WS_IL] < sizeof(double) * il_ws_doubles(ig) ||
-                !ctx().ws[WS_ILMU] || ctx().wsz[WS_ILMU] < sizeof(double) * il_mu_doubles(ig) ||
-                (wi && (!ctx().ws[WS_WAVE] || ctx().wsz[WS_WAVE] < sizeof(int) * wi))))
+                !ctx().ws[WS_ILMU] || ctx().wsz[WS_ILMU] < sizeof(double) * il_mu_doubles(ig)))
       st = PEVSL_ERR_ARG; /* il_prepare not run before the capture */
     for (size_t gi = 0; gi < ig.size() && !st; gi++) {
       const IlGroup &G = ig[gi];
@@ -459,14 +442,6 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
       il_buffers(G, &X0, &B0, &B1, &Y);
       st = il_pack(G.A->nrows, G.S, xs, X0);
       ilv[gi] = {X0, nullptr, nullptr};
-      /* the wavefront form runs the group's whole application here; the
-       * degree loop below then only counts its bytes */
-      if (!st && il_wave_usable(G.A, G.S)) {
-        const double *dmu = (const double *)ctx().ws[WS_ILMU] + G.mu_off;
-        st = cheb_filter_il_wave(G.A, G.S, X0, B0, B1, Y, G.cc, G.dd, dmu, G.maxdeg, defer,
-                                 (int *)ctx().ws[WS_WAVE]);
-        ilw_wave[gi] = 1;
-      }
     }
     if (st) return st;
   }
@@ -502,9 +477,8 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
       double *gkp1 = k == 1 ? B0 : k == 2 ? B1 : const_cast<double *>(gkm1);
       const double *dmu = (const double *)ctx().ws[WS_ILMU] + G.mu_off;
       const int ny = il_terms(k, ilw[gi], G.maxdeg, defer), fresh = ny > 0 && ilw[gi] == 0;
-      if (!ilw_wave[gi])
-        st = cheb_step_il_y(G.A, G.S, gk, gk, gkm1, gkp1, Y, G.cc, (k == 1 ? 1.0 : 2.0) / G.dd,
-                            dmu, dmu + (size_t)k * G.S, ny, fresh);
+      st = cheb_step_il_y(G.A, G.S, gk, gk, gkm1, gkp1, Y, G.cc, (k == 1 ? 1.0 : 2.0) / G.dd, dmu,
+                          dmu + (size_t)k * G.S, ny, fresh);
       if (ny > 0) ilw[gi] = k;
       /* read v_k, v_{k-1} (from degree 2), write v_{k+1}; y read unless
        * fresh and written when updated */

@@ -1361,13 +1361,13 @@ int pEVSL_ParcsrCreate(int nrow, int ncol, int *row_starts, int *col_starts, pev
   return 0;
 }
 
-/* Row chunks of the staged filter kernels and their dependency ranges, from
- * a host CSR (also exported for tests; see include/pevsl_b200.h). */
-extern "C" int pEVSL_B200_WaveLayout(int n, const int *ia, const int *ja, int *nchunks,
-                                     int *chunks, int *deps, int *reach) {
-  if (n < 0 || !ia || !ja || !nchunks) return PEVSL_ERR_ARG;
-  /* chunks: at most RMAX rows and EMAX entries, starting at multiples of 4
-   * rows (16-byte aligned row-pointer and vector copies) */
+/* Row chunks of the staged filter kernel, from a host CSR (also exported
+ * for tests; see include/pevsl_b200.h). */
+extern "C" int pEVSL_B200_ChunkLayout(int n, const int *ia, int *nchunks, int *chunks) {
+  if (n < 0 || !ia || !nchunks) return PEVSL_ERR_ARG;
+  /* at most RMAX rows and EMAX entries (unless one 4-row group alone holds
+   * more), starting at multiples of 4 rows: 16-byte aligned row-pointer and
+   * vector copies */
   std::vector<int> ch;
   for (int r = 0; r < n;) {
     ch.push_back(r);
@@ -1380,47 +1380,10 @@ extern "C" int pEVSL_B200_WaveLayout(int n, const int *ia, const int *ja, int *n
     }
     r = e;
   }
-  const int wnc = (int)(ch.size() / 2);
+  *nchunks = (int)(ch.size() / 2);
   ch.push_back(n);
   ch.push_back(ia[n]);
-  /* dependency ranges: [lo, hi] of the chunks of the columns of its rows,
-   * widened to every chunk that has a column in it (prefix max of hi /
-   * suffix min of lo; a superset for unsymmetric patterns) */
-  std::vector<int> starts((size_t)wnc + 1);
-  for (int c = 0; c <= wnc; c++) starts[(size_t)c] = ch[(size_t)2 * c];
-  auto chunk_of = [&](int col) {
-    return (int)(std::upper_bound(starts.begin(), starts.end() - 1, col) - starts.begin()) - 1;
-  };
-  std::vector<int> clo((size_t)wnc), chi((size_t)wnc);
-  for (int c = 0; c < wnc; c++) {
-    int mn = INT32_MAX, mx = -1;
-    for (int k = ia[starts[(size_t)c]]; k < ia[starts[(size_t)c + 1]]; k++) {
-      if (ja[k] < 0 || ja[k] >= n) return PEVSL_ERR_ARG;
-      mn = PEVSL_MIN(mn, ja[k]);
-      mx = PEVSL_MAX(mx, ja[k]);
-    }
-    clo[(size_t)c] = mx < 0 ? c : PEVSL_MIN(c, chunk_of(mn));
-    chi[(size_t)c] = mx < 0 ? c : PEVSL_MAX(c, chunk_of(mx));
-  }
-  std::vector<int> pmax((size_t)wnc), smin((size_t)wnc);
-  for (int c = 0; c < wnc; c++) pmax[(size_t)c] = PEVSL_MAX(chi[(size_t)c], c ? pmax[(size_t)c - 1] : -1);
-  for (int c = wnc - 1; c >= 0; c--)
-    smin[(size_t)c] = PEVSL_MIN(clo[(size_t)c], c + 1 < wnc ? smin[(size_t)c + 1] : INT32_MAX);
-  int rch = 0;
-  for (int c = 0; c < wnc; c++) {
-    /* first c' with pmax >= c, last c' with smin <= c (both monotone) */
-    const int rlo = (int)(std::lower_bound(pmax.begin(), pmax.end(), c) - pmax.begin());
-    const int rhi = (int)(std::upper_bound(smin.begin(), smin.end(), c) - smin.begin()) - 1;
-    const int lo = PEVSL_MIN(clo[(size_t)c], rlo), hi = PEVSL_MAX(chi[(size_t)c], rhi);
-    if (deps) {
-      deps[(size_t)2 * c] = lo;
-      deps[(size_t)2 * c + 1] = hi;
-    }
-    rch = PEVSL_MAX(rch, PEVSL_MAX(c - lo, hi - c));
-  }
-  *nchunks = wnc;
   if (chunks) memcpy(chunks, ch.data(), sizeof(int) * ch.size());
-  if (reach) *reach = rch;
   return 0;
 }
 
@@ -1464,25 +1427,21 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
       vi[(size_t)k] = (unsigned char)hval[h];
     }
   }
-  /* row chunks of the staged kernels and their dependency ranges */
-  int wnc = 0, reach = 0;
-  if (pEVSL_B200_WaveLayout(nr, Ai->ia, Ai->ja, &wnc, nullptr, nullptr, &reach))
-    return PEVSL_ERR_ARG;
-  std::vector<int> ch((size_t)2 * wnc + 2), dep((size_t)2 * wnc);
-  pEVSL_B200_WaveLayout(nr, Ai->ia, Ai->ja, &wnc, ch.data(), dep.data(), &reach);
+  /* row chunks of the staged kernel */
+  int wnc = 0;
+  if (pEVSL_B200_ChunkLayout(nr, Ai->ia, &wnc, nullptr)) return PEVSL_ERR_ARG;
+  std::vector<int> ch((size_t)2 * wnc + 2);
+  pEVSL_B200_ChunkLayout(nr, Ai->ia, &wnc, ch.data());
   /* the parts are 256-byte multiples: a staged copy rounded up to 16 bytes
    * never leaves its part */
   const size_t b_dj = ((sizeof(short) * (size_t)nnz + 255) / 256) * 256;
   const size_t b_vi = ((size_t)nnz + 255) / 256 * 256;
   const size_t b_tab = 256 * sizeof(double) + 256 * sizeof(float);
   const size_t b_ch = (sizeof(int) * ch.size() + 255) / 256 * 256;
-  const size_t b_dep = (sizeof(int) * dep.size() + 255) / 256 * 256;
-  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab + b_ch + b_dep);
+  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab + b_ch);
   if (!base) return PEVSL_ERR_NOMEM;
   d->wchunk = (int *)(base + b_dj + b_vi + b_tab);
   d->wnc = wnc;
-  d->wdep = (int *)(base + b_dj + b_vi + b_tab + b_ch);
-  d->wreach = reach;
   std::vector<float> tab32(tab.size());
   for (size_t t = 0; t < tab.size(); t++) tab32[t] = (float)tab[t];
   d->pdj = (short *)base;
@@ -1493,7 +1452,6 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
   d->pbytes = b_dj + b_vi + b_tab;
   int st = memcpy_async(d->pdj, dj.data(), sizeof(short) * (size_t)nnz);
   if (!st) st = memcpy_async(d->wchunk, ch.data(), sizeof(int) * ch.size());
-  if (!st) st = memcpy_async(d->wdep, dep.data(), sizeof(int) * dep.size());
   if (!st) st = memcpy_async(d->pvi, vi.data(), (size_t)nnz);
   if (!st) st = memcpy_async(d->pvtab, tab.data(), sizeof(double) * tab.size());
   if (!st) st = memcpy_async(d->pvtab32, tab32.data(), sizeof(float) * tab.size());

@@ -67,11 +67,6 @@ typedef struct pevsl_devcsr {
    * PEVSL_WAVE_EMAX entries; wnc chunks, then the sentinel (nrows, nnz) */
   int *wchunk;
   int wnc;
-  /* per chunk c, wdep[2c] .. wdep[2c+1]: the chunks holding a column of one
-   * of c's rows or a row with a column in c (a superset of both), and
-   * wreach = max over c of the distance to either end */
-  int *wdep;
-  int wreach;
 } pevsl_devcsr;
 
 #define PEVSL_WAVE_RMAX 256
