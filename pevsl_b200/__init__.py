@@ -617,9 +617,12 @@ def _free_outputs(lib, lam, res, W):
         libc.free(C.cast(W, _vp))
 
 
-def cheblannr_batch(ev: "Instance", intvs, maxits, tol, vinit, filters):
+def cheblannr_batch(ev: "Instance", intvs, maxits, tol, vinit, filters, fstats=None):
     """pEVSL_B200_ChebLanNrBatch: all slices in lockstep; a list of per-slice
-    dicts like Instance.cheblannr (without vectors)."""
+    dicts like Instance.cheblannr (without vectors).  fstats: a C FILE*
+    (e.g. from open_log) that receives the solver's log, as the reference's
+    fstats argument does (SRC/cheblanNr.c:298: one line per convergence
+    test with the trace of the Ritz values above the bar)."""
     lib = ev.lib
     ns = len(filters)
     pols = (Polparams * max(ns, 1))()
@@ -639,7 +642,7 @@ def cheblannr_batch(ev: "Instance", intvs, maxits, tol, vinit, filters):
     W = (C.POINTER(Parvecs) * max(ns, 1))()
     r = lib.pEVSL_B200_ChebLanNrBatch(ev.p, ns, _ptr(iv), _ptr(mx, _ip), tol, C.byref(v.pv),
                                       pols, _ptr(nev, _ip), lam, W, res, _ptr(its, _ip),
-                                      _ptr(status, _ip), None)
+                                      _ptr(status, _ip), fstats)
     outs = []
     for i in range(ns):
         m = int(nev[i])
@@ -866,8 +869,26 @@ def gen_counters():
     return f.value, d.value, b.value, ms.value
 
 
+def open_log(path: str):
+    """A C FILE* opened for writing (libc fopen), for the solvers' fstats
+    argument; close it with close_log."""
+    libc = C.CDLL(None)
+    libc.fopen.restype = C.c_void_p
+    libc.fopen.argtypes = [C.c_char_p, C.c_char_p]
+    f = libc.fopen(path.encode(), b"w")
+    if not f:
+        raise PevslError(f"cannot open {path}")
+    return C.c_void_p(f)
+
+
+def close_log(f) -> None:
+    libc = C.CDLL(None)
+    libc.fclose.argtypes = [C.c_void_p]
+    libc.fclose(f)
+
+
 def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
-                   precision: int = PREC_FP64, setup=None) -> SliceResult:
+                   precision: int = PREC_FP64, setup=None, fstats=None) -> SliceResult:
     """Run the whole slicing path through the C API, in the reference
     drivers' order: start vector, bounds, DOS, slicer, then each slice
     (one pEVSL_ChebLanNr per slice, or all slices in lockstep through
@@ -934,7 +955,8 @@ def solve_interval(A: Matrix, s: SliceRun, batched: bool = False,
                     raise PevslError(f"pEVSL_FindPol returned {r} for slice {sl}")
                 filters.append(f)
                 intvs.append(slice_ivs[sl])
-            r, outs = cheblannr_batch(ev, intvs, [mlan] * s.nslices, s.tol, vinit, filters)
+            r, outs = cheblannr_batch(ev, intvs, [mlan] * s.nslices, s.tol, vinit, filters,
+                                      fstats)
             res.fallbacks = int(lib.pEVSL_B200_LastFallbacks())
             for f, out in zip(filters, outs):
                 if out["status"] and not res.status:
