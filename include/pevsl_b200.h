@@ -195,15 +195,6 @@ int pEVSL_B200_GemmNN(long n, int k, int m, const double *V, long ldv, const dou
 int pEVSL_B200_GemmTN(long n, int k, int m, const double *V, long ldv, const double *W, long ldw,
                       double *C, long ldc);
 
-/* The row chunks of the staged filter kernel (PEVSL_B200_IL_TMA=1), on the
- * host (no GPU needed), for tests and diagnostics: for a CSR of n rows
- * (ia 0-based), *nchunks and chunks[2c], chunks[2c+1] = first row and first
- * entry of chunk c, 2 * nchunks + 2 ints, the last pair (n, nnz); chunks may
- * be NULL (then only *nchunks is returned).  A chunk starts at a multiple of
- * 4 rows and holds at most 256 rows and, unless one 4-row group alone holds
- * more, 4096 entries. */
-int pEVSL_B200_ChunkLayout(int n, const int *ia, int *nchunks, int *chunks);
-
 /* Release cached device workspaces (they are reused across calls). */
 void pEVSL_B200_ReleaseWorkspace(void);
 

@@ -245,21 +245,6 @@ int cheb_step_il_x(const pevsl_devcsr *A, int S, const double *Xg, const double 
 int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double *Xk,
                    const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
                    const double *mu0, const double *muk, int ny, int fresh);
-/* the staged (cp.async.bulk) form of cheb_step_il_y for Xg == Xk on a
- * packed matrix with a chunk table (gpu_filter_tma.cu); il_tma_usable says
- * whether it applies; il_tma_error returns 1 (and clears the flag) when one
- * of its bounded waits ran out since the last check */
-bool il_tma_usable(const pevsl_devcsr *A, int S);
-int cheb_step_il_tma(const pevsl_devcsr *A, int S, const double *Xk, const double *Xkm1,
-                     double *Xkp1, double *Y, double cc, double t, const double *mu0,
-                     const double *muk, int ny, int fresh);
-int il_tma_error();
-/* shared-memory attributes and resident grids of the staged kernels, once
- * per context (outside any capture) */
-int tma_init();
-/* the staged kernel for one vector: cheb_step's recurrence (y every degree) */
-int cheb_step_tma(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1,
-                  double *y, double cc, double t, double mu0, double muk, int first);
 /* X[i*S + s] = xs[s][i] (S <= kMaxBatch), and ys[s][i] = X[i*S + s] for
  * the first cols columns */
 int il_pack(long n, int S, const double *const *xs, double *X);

@@ -81,12 +81,6 @@ int ensure() {
   if (fail(cudaMalloc(&g_ctx.bar, sizeof(unsigned) * 4), "cudaMalloc bar")) return PEVSL_ERR_CUDA;
   if (fail(cudaMemset(g_ctx.bar, 0, sizeof(unsigned) * 4), "cudaMemset bar")) return PEVSL_ERR_CUDA;
   g_ctx.ready = true;
-  /* launch configuration of the staged kernels, here and not at their first
-   * launch, which may fall inside a stream capture */
-  if (tma_init()) {
-    g_ctx.ready = false;
-    return PEVSL_ERR_CUDA;
-  }
   return 0;
 }
 

@@ -1720,12 +1720,6 @@ static int cheblannr_group(SliceState *SL, int ns, double tol, FILE *fstats,
         r = filter_graphed(fg, sel, jobs);
       else
         r = cheb_filter_batch((int)jobs.size(), jobs.data(), mixed);
-      /* a bounded wait of the staged filter kernel that ran out: report it
-       * before the result is used */
-      if (!r && il_tma_error()) {
-        fprintf(stderr, "pevsl_b200: staged filter kernel wait timed out\n");
-        r = PEVSL_ERR_CUDA;
-      }
     }
     t_pol.end();
     return r;

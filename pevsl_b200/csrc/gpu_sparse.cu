@@ -962,10 +962,6 @@ int spmv(const pevsl_devcsr *A, const double *x, double *y) {
 int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1, double *y,
               double cc, double t, double mu0, double muk, int first) {
   if (A->nrows <= 0) return 0;
-  /* packed matrices of at least 2^16 rows: the staged kernel (same bits);
-   * smaller ones sit in L2, where the CSR-stream kernel's finer grid wins */
-  if (A->lanes == 0 && use_packed(A) && A->nrows >= 65536 && il_tma_usable(A, 1))
-    return cheb_step_tma(A, vk, vkm1, vkp1, y, cc, t, mu0, muk, first);
   if (A->lanes == 0) {
     launch_stream(A, (const double *)A->a, vk, EpiCheb{vk, vkm1, vkp1, y, cc, t, mu0, muk, first});
     return launched("cheb_step_stream");
@@ -1196,15 +1192,17 @@ __global__ void __launch_bounds__(kThreads, 5)
   }
 }
 
-/* the pipelined form (PEVSL_B200_IL_PREFETCH=1; off by default until
- * measured faster) */
-static bool il_prefetch() {
+/* The pipelined form, by width: measured per degree at 100^3 (one B200),
+ * 2 slices 22.7 us against 26.6 us for k_cheb_il_p, 4 slices 48.1 against
+ * 46.7 us; so the default is S = 2 only.  PEVSL_B200_IL_PREFETCH: 0 never,
+ * 1 every width. */
+static bool il_prefetch(int S) {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("PEVSL_B200_IL_PREFETCH");
-    v = e ? atoi(e) != 0 : 0;
+    v = e ? atoi(e) : -1;
   }
-  return v != 0;
+  return v > 0 || (v < 0 && S == 2);
 }
 
 /* X[i*S + s] = x_s[i] and back */
@@ -1278,9 +1276,7 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
   cudaStream_t st = ctx().stream;
-  if (Xg == Xk && il_packed(A) && il_tma_usable(A, S))
-    return cheb_step_il_tma(A, S, Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, ny, fresh);
-  if (Xg == Xk && il_packed(A) && il_prefetch()) {
+  if (Xg == Xk && il_packed(A) && il_prefetch(S)) {
     /* five resident blocks per SM, each lane walking rows a grid apart */
     const unsigned gp = (unsigned)PEVSL_MIN((long)g, 5L * ctx().sms);
 #define PV_IL_PF(SS)                                                                             \
@@ -1462,32 +1458,6 @@ int pEVSL_ParcsrCreate(int nrow, int ncol, int *row_starts, int *col_starts, pev
   return 0;
 }
 
-/* Row chunks of the staged filter kernel, from a host CSR (also exported
- * for tests; see include/pevsl_b200.h). */
-extern "C" int pEVSL_B200_ChunkLayout(int n, const int *ia, int *nchunks, int *chunks) {
-  if (n < 0 || !ia || !nchunks) return PEVSL_ERR_ARG;
-  /* at most RMAX rows and EMAX entries (unless one 4-row group alone holds
-   * more), starting at multiples of 4 rows: 16-byte aligned row-pointer and
-   * vector copies */
-  std::vector<int> ch;
-  for (int r = 0; r < n;) {
-    ch.push_back(r);
-    ch.push_back(ia[r]);
-    int e = PEVSL_MIN(n, r + 4);
-    while (e < n && e - r < PEVSL_WAVE_RMAX) {
-      const int e2 = PEVSL_MIN(n, e + 4);
-      if (ia[e2] - ia[r] > PEVSL_WAVE_EMAX) break;
-      e = e2;
-    }
-    r = e;
-  }
-  *nchunks = (int)(ch.size() / 2);
-  ch.push_back(n);
-  ch.push_back(ia[n]);
-  if (chunks) memcpy(chunks, ch.data(), sizeof(int) * ch.size());
-  return 0;
-}
-
 /* Upload the caller's host CSR (the local rows, global column indices) as
  * one device CSR (SRC/parcsr.c:70-283 without the split and halo plan). */
 /* The packed copy of a matrix's entries, when every column lies within
@@ -1528,21 +1498,11 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
       vi[(size_t)k] = (unsigned char)hval[h];
     }
   }
-  /* row chunks of the staged kernel */
-  int wnc = 0;
-  if (pEVSL_B200_ChunkLayout(nr, Ai->ia, &wnc, nullptr)) return PEVSL_ERR_ARG;
-  std::vector<int> ch((size_t)2 * wnc + 2);
-  pEVSL_B200_ChunkLayout(nr, Ai->ia, &wnc, ch.data());
-  /* the parts are 256-byte multiples: a staged copy rounded up to 16 bytes
-   * never leaves its part */
   const size_t b_dj = ((sizeof(short) * (size_t)nnz + 255) / 256) * 256;
   const size_t b_vi = ((size_t)nnz + 255) / 256 * 256;
   const size_t b_tab = 256 * sizeof(double) + 256 * sizeof(float);
-  const size_t b_ch = (sizeof(int) * ch.size() + 255) / 256 * 256;
-  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab + b_ch);
+  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab);
   if (!base) return PEVSL_ERR_NOMEM;
-  d->wchunk = (int *)(base + b_dj + b_vi + b_tab);
-  d->wnc = wnc;
   std::vector<float> tab32(tab.size());
   for (size_t t = 0; t < tab.size(); t++) tab32[t] = (float)tab[t];
   d->pdj = (short *)base;
@@ -1552,7 +1512,6 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
   d->pnv = (int)tab.size();
   d->pbytes = b_dj + b_vi + b_tab;
   int st = memcpy_async(d->pdj, dj.data(), sizeof(short) * (size_t)nnz);
-  if (!st) st = memcpy_async(d->wchunk, ch.data(), sizeof(int) * ch.size());
   if (!st) st = memcpy_async(d->pvi, vi.data(), (size_t)nnz);
   if (!st) st = memcpy_async(d->pvtab, tab.data(), sizeof(double) * tab.size());
   if (!st) st = memcpy_async(d->pvtab32, tab32.data(), sizeof(float) * tab.size());
@@ -1588,9 +1547,7 @@ int pEVSL_ParcsrSetup(pevsl_Csr *Ai, pevsl_Parcsr *A) {
    * aligned parts, so that a single L2 access-policy window can cover it */
   const size_t bytes_a = ((sizeof(double) * (size_t)nnz + 255) / 256) * 256;
   const size_t bytes_ja = ((sizeof(int) * (size_t)nnz + 255) / 256) * 256;
-  /* 256-byte multiple: a staged copy of row pointers rounded up to 16
-   * bytes stays inside the block */
-  const size_t bytes_ia = ((sizeof(int) * (size_t)(nr + 1) + 255) / 256) * 256;
+  const size_t bytes_ia = sizeof(int) * (size_t)(nr + 1);
   char *base = (char *)alloc_dev(bytes_a + bytes_ja + bytes_ia);
   if (!base) {
     free(d);

@@ -60,17 +60,7 @@ typedef struct pevsl_devcsr {
   float *pvtab32;
   int pnv;
   size_t pbytes;
-  /* row chunks of the staged filter kernels (packed matrices only): chunk c
-   * holds rows wchunk[2c] .. wchunk[2c+2]-1 and entries wchunk[2c+1] ..
-   * wchunk[2c+3]-1; every chunk starts at a multiple of 4 rows and holds at
-   * most PEVSL_WAVE_RMAX rows and (unless one 4-row group alone exceeds it)
-   * PEVSL_WAVE_EMAX entries; wnc chunks, then the sentinel (nrows, nnz) */
-  int *wchunk;
-  int wnc;
 } pevsl_devcsr;
-
-#define PEVSL_WAVE_RMAX 256
-#define PEVSL_WAVE_EMAX 4096
 
 /* The device matrix behind a Parcsr, or NULL if it was never set up here. */
 pevsl_devcsr *pevsl_devcsr_of(const pevsl_Parcsr *A);

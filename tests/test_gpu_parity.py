@@ -645,9 +645,7 @@ def test_interleaved_filter_plain_entries_bit_identical(gpu):
 def _banded_heavy_matrix(n, seed):
     """Symmetric packed-eligible matrix: 6 random off-diagonals per row within
     +-30000 columns, values from a set of 64, and heavy rows of 1500
-    entries: one alone and four in one 4-row group (the row chunk holding
-    those four exceeds the 4096 entries a staged chunk can hold and takes
-    the unstaged path)."""
+    entries: one alone and four adjacent ones."""
     rng = np.random.default_rng(seed)
     vals = np.round(rng.standard_normal(64), 3)
     r, c = [], []
@@ -678,12 +676,12 @@ def _banded_heavy_matrix(n, seed):
     return Csr(n, ia, cols.astype(np.int32), vv.astype(np.float64))
 
 
-def test_staged_filter_heavy_rows_bit_identical(gpu):
-    """The staged interleaved filter on a scattered matrix with heavy rows
-    (some row chunks exceed the staging buffer and read their entries from
-    global memory): three slices in lockstep give every slice the bits of
-    solving it alone with the one-vector kernel, after 40 Lanczos steps of
-    degree-60 filters."""
+def test_interleaved_filter_heavy_rows_bit_identical(gpu):
+    """The interleaved filter on a scattered matrix with heavy rows (the
+    lanes of a row walk up to 1500 entries while their neighbours walk 7):
+    three slices in lockstep give every slice the bits of solving it alone
+    with the one-vector kernel, after 40 Lanczos steps of degree-60
+    filters."""
     A = _banded_heavy_matrix(70001, 5)
     M = dev_matrix(A)
     rows = np.repeat(np.arange(A.n), np.diff(A.ia))
