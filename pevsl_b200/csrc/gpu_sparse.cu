@@ -1118,93 +1118,6 @@ __global__ void __launch_bounds__(kThreads)
   if (ny > 0) Y[me] = il_accumulate<S>(ny, fresh, yold, w, x, xm1, mu0, muk, s);
 }
 
-/* k_cheb_il_p as a grid-stride loop with a one-row software pipeline: while
- * a lane's gathers for row r are in flight it has already issued the loads
- * of row r + stride's contiguous operands (X_k, X_{k-1}, Y and the row
- * bounds), so the DRAM streams of the next row overlap the L2 gathers of
- * this one.  Same products in the same order, same recurrence: the bits of
- * k_cheb_il_p. */
-template <int S>
-__global__ void __launch_bounds__(kThreads, 5)
-    k_cheb_il_pf(int n, const int *__restrict__ ia, const short *__restrict__ dj,
-                 const unsigned char *__restrict__ vi, const double *__restrict__ vtab, int nv,
-                 const double *__restrict__ Xk, const double *Xkm1, double *Xkp1, double *Y,
-                 double cc, double t, const double *__restrict__ mu0,
-                 const double *__restrict__ muk, int ny, int fresh) {
-  __shared__ double vt[256];
-  for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
-  __syncthreads();
-  constexpr int RPW = 32 / S;
-  const int lane = threadIdx.x & 31, s = lane % S;
-  const long stride = (long)gridDim.x * (blockDim.x >> 5) * RPW;
-  long row = ((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5) * RPW + lane / S;
-  const bool read_y = ny > 0 && !fresh;
-  double x = 0.0, xm1 = 0.0, yold = 0.0;
-  int jb = 0, je = 0;
-  if (row < n) {
-    const size_t me = (size_t)row * S + s;
-    x = Xk[me];
-    if (Xkm1) xm1 = Xkm1[me];
-    if (read_y) yold = Y[me];
-    jb = __ldg(ia + row);
-    je = __ldg(ia + row + 1);
-  }
-  while (row < n) {
-    const long nrow = row + stride;
-    double nx = 0.0, nxm1 = 0.0, nyold = 0.0;
-    int njb = 0, nje = 0;
-    if (nrow < n) {
-      const size_t nme = (size_t)nrow * S + s;
-      nx = Xk[nme];
-      if (Xkm1) nxm1 = Xkm1[nme];
-      if (read_y) nyold = Y[nme];
-      njb = __ldg(ia + nrow);
-      nje = __ldg(ia + nrow + 1);
-    }
-    const int g0 = (int)(row & ~31L);
-    const size_t me = (size_t)row * S + s;
-    double r = 0.0;
-    int j = jb;
-    for (; j + 3 < je; j += 4) {
-      const int c0 = g0 + __ldg(dj + j), c1 = g0 + __ldg(dj + j + 1);
-      const int c2 = g0 + __ldg(dj + j + 2), c3 = g0 + __ldg(dj + j + 3);
-      const double a0 = vt[__ldg(vi + j)], a1 = vt[__ldg(vi + j + 1)];
-      const double a2 = vt[__ldg(vi + j + 2)], a3 = vt[__ldg(vi + j + 3)];
-      const double x0 = __ldg(Xk + (size_t)c0 * S + s), x1 = __ldg(Xk + (size_t)c1 * S + s);
-      const double x2 = __ldg(Xk + (size_t)c2 * S + s), x3 = __ldg(Xk + (size_t)c3 * S + s);
-      r = __dadd_rn(r, __dmul_rn(a0, x0));
-      r = __dadd_rn(r, __dmul_rn(a1, x1));
-      r = __dadd_rn(r, __dmul_rn(a2, x2));
-      r = __dadd_rn(r, __dmul_rn(a3, x3));
-    }
-    for (; j < je; j++)
-      r = __dadd_rn(r, __dmul_rn(vt[__ldg(vi + j)], __ldg(Xk + (size_t)(g0 + __ldg(dj + j)) * S + s)));
-    double w = __dmul_rn(__fma_rn(-cc, x, r), t);
-    if (Xkm1) w = __dsub_rn(w, xm1);
-    Xkp1[me] = w;
-    if (ny > 0) Y[me] = il_accumulate<S>(ny, fresh, yold, w, x, xm1, mu0, muk, s);
-    row = nrow;
-    x = nx;
-    xm1 = nxm1;
-    yold = nyold;
-    jb = njb;
-    je = nje;
-  }
-}
-
-/* The pipelined form, by width: measured per degree at 100^3 (one B200),
- * 2 slices 22.7 us against 26.6 us for k_cheb_il_p, 4 slices 48.1 against
- * 46.7 us; so the default is S = 2 only.  PEVSL_B200_IL_PREFETCH: 0 never,
- * 1 every width. */
-static bool il_prefetch(int S) {
-  static int v = -1;
-  if (v < 0) {
-    const char *e = getenv("PEVSL_B200_IL_PREFETCH");
-    v = e ? atoi(e) : -1;
-  }
-  return v > 0 || (v < 0 && S == 2);
-}
-
 /* X[i*S + s] = x_s[i] and back */
 __global__ void k_il_pack(long n, int S, CPtrs xs, double *X) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n * S;
@@ -1276,22 +1189,6 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
   cudaStream_t st = ctx().stream;
-  if (Xg == Xk && il_packed(A) && il_prefetch(S)) {
-    /* five resident blocks per SM, each lane walking rows a grid apart */
-    const unsigned gp = (unsigned)PEVSL_MIN((long)g, 5L * ctx().sms);
-#define PV_IL_PF(SS)                                                                             \
-  k_cheb_il_pf<SS><<<gp, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, \
-                                            Xk, Xkm1, Xkp1, Y, cc, t, mu0, muk, ny, fresh)
-    switch (S) {
-      case 2: PV_IL_PF(2); break;
-      case 4: PV_IL_PF(4); break;
-      case 8: PV_IL_PF(8); break;
-      case 16: PV_IL_PF(16); break;
-      default: return PEVSL_ERR_ARG;
-    }
-#undef PV_IL_PF
-    return launched("cheb_step_il_pf");
-  }
   if (il_packed(A)) {
 #define PV_IL_P(SS)                                                                          \
   k_cheb_il_p<SS><<<g, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, \
