@@ -199,6 +199,26 @@ static int interleave_setting() {
 
 static int il_width(int nlive) { return nlive <= 2 ? 2 : nlive <= 4 ? 4 : nlive <= 8 ? 8 : 16; }
 
+/* Slices per interleaved group.  A group's whole filter application runs
+ * before the next group's, and its working set from one degree to the next
+ * -- three row-interleaved vector blocks (24 n bytes per slice) and the
+ * matrix -- stays in the 126 MB L2 when it is at most half of it; wider
+ * groups stream it from HBM at every degree.  So a group holds the most
+ * slices (2, 4, 8 or 16) that fit in 64 MB, at least 2.  Measured per
+ * degree at 100^3 (n = 1e6, packed matrix 25 MB): 2 slices 20.1 us (0.64 of
+ * the HBM peak in algorithmic bytes, L2-resident), 4 slices 44.0-46.7 us.
+ * PEVSL_B200_IL_MAXS caps it by hand (2..16). */
+static int il_group_cap(const pevsl_devcsr *A) {
+  const char *e = getenv("PEVSL_B200_IL_MAXS"); /* read per call: tests change it */
+  const int env = e ? atoi(e) : 0;
+  if (env >= 2) return PEVSL_MIN(env, kMaxBatch);
+  const double mat = 3.0 * (double)A->nnz + 4.0 * (A->nrows + 1.0);
+  int cap = 2;
+  for (int S = 4; S <= kMaxBatch; S *= 2)
+    if (24.0 * (double)A->nrows * S + mat <= 64.0 * 1024 * 1024) cap = S;
+  return cap;
+}
+
 /* Degrees per accumulator update in the interleaved filter
  * (PEVSL_B200_IL_DEFER: 1, 2 or 3, the default).  With D > 1 a launch adds
  * the terms of the last D degrees to y (the first update at degree
@@ -256,8 +276,9 @@ static void il_partition(int ne, const FilterJob *jobs, bool fp32, std::vector<I
         seen[f] = 1;
         L.push_back(f);
       }
-    for (size_t c0 = 0; c0 < L.size(); c0 += kMaxBatch) {
-      const int cnt = (int)PEVSL_MIN((size_t)kMaxBatch, L.size() - c0);
+    const size_t cap = (size_t)il_group_cap(A);
+    for (size_t c0 = 0; c0 < L.size(); c0 += cap) {
+      const int cnt = (int)PEVSL_MIN(cap, L.size() - c0);
       if (cnt < 2) continue;
       IlGroup G;
       G.A = A;
@@ -464,18 +485,18 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
     }
     vkm1[i] = nullptr;
   }
-  std::vector<ChebEntry> en(nlive);
-  for (int k = 1; k <= maxdeg && !st; k++) {
-    int nb = 0;
-    double bytes = 0.0;
-    for (size_t gi = 0; gi < ig.size() && !st; gi++) {
-      const IlGroup &G = ig[gi];
-      if (k > G.maxdeg) continue;
-      double *X0, *B0, *B1, *Y;
-      il_buffers(G, &X0, &B0, &B1, &Y);
+  /* the interleaved groups one after another, each through all its
+   * degrees, so that a group's working set stays in L2 between degrees
+   * (il_group_cap); the groups are independent, so every slice's bits are
+   * those of the degree-major order */
+  for (size_t gi = 0; gi < ig.size() && !st; gi++) {
+    const IlGroup &G = ig[gi];
+    double *X0, *B0, *B1, *Y;
+    il_buffers(G, &X0, &B0, &B1, &Y);
+    const double *dmu = (const double *)ctx().ws[WS_ILMU] + G.mu_off;
+    for (int k = 1; k <= G.maxdeg && !st; k++) {
       const double *gk = ilv[gi][0], *gkm1 = ilv[gi][1];
       double *gkp1 = k == 1 ? B0 : k == 2 ? B1 : const_cast<double *>(gkm1);
-      const double *dmu = (const double *)ctx().ws[WS_ILMU] + G.mu_off;
       const int ny = il_terms(k, ilw[gi], G.maxdeg, defer), fresh = ny > 0 && ilw[gi] == 0;
       st = cheb_step_il_y(G.A, G.S, gk, gk, gkm1, gkp1, Y, G.cc, (k == 1 ? 1.0 : 2.0) / G.dd, dmu,
                           dmu + (size_t)k * G.S, ny, fresh);
@@ -483,11 +504,19 @@ static int cheb_filter_batch(int ne, const FilterJob *jobs, bool fp32) {
       /* read v_k, v_{k-1} (from degree 2), write v_{k+1}; y read unless
        * fresh and written when updated */
       const double vec = (k == 1 ? 16.0 : 24.0) + (ny > 0 ? (fresh ? 8.0 : 16.0) : 0.0);
-      bytes += il_entry_bytes(G.A) * (double)G.A->nnz + 4.0 * (G.A->nrows + 1.0) +
-               vec * (double)G.A->nrows * G.S;
+      g_filter_bytes += il_entry_bytes(G.A) * (double)G.A->nnz + 4.0 * (G.A->nrows + 1.0) +
+                        vec * (double)G.A->nrows * G.S;
+      g_filter_launches++;
       ilv[gi][1] = gk;
       ilv[gi][0] = gkp1;
     }
+  }
+  bool others = false;
+  for (int i = 0; i < nlive && !others; i++) others = !taken[(size_t)live[i]];
+  std::vector<ChebEntry> en(nlive);
+  for (int k = 1; k <= maxdeg && !st && others; k++) {
+    int nb = 0;
+    double bytes = 0.0;
     for (int i = 0; i < nlive; i++) {
       const FilterJob &J = jobs[live[i]];
       const pevsl_Polparams *pol = J.pol;

@@ -613,6 +613,30 @@ def test_interleaved_filter_bit_identical(gpu):
         assert np.max(np.abs(b["lam"] - ex)) <= 1e-10 * np.max(np.abs(ex))
 
 
+def test_interleaved_groups_one_after_another_bit_identical(gpu, monkeypatch):
+    """Five slices of one matrix in lockstep with the interleaved groups
+    capped at two slices (PEVSL_B200_IL_MAXS=2: groups of 2, 2 and 1, each
+    group's whole filter application before the next, as for matrices whose
+    wider groups would not stay in L2): every slice gets the bits of solving
+    it alone and the exact count."""
+    monkeypatch.setenv("PEVSL_B200_IL_MAXS", "2")
+    grid = (41, 41, 41)
+    M, intvs, fl = _lap_slices(grid, 0.3, 0.38, 5)
+    v = np.cos(np.arange(M.n) * 0.37)
+    with pv.Instance(M) as ev:
+        r, batch = pv.cheblannr_batch(ev, intvs, [200] * 5, 1e-8, v, fl)
+    assert r == 0
+    monkeypatch.delenv("PEVSL_B200_IL_MAXS")
+    for iv, f, b in zip(intvs, fl, batch):
+        with pv.Instance(M) as ev:
+            r, (one,) = pv.cheblannr_batch(ev, [iv], [200], 1e-8, v, [f])
+        assert r == 0
+        assert one["nev"] == b["nev"] and one["its"] == b["its"]
+        assert np.array_equal(one["lam"], b["lam"]) and np.array_equal(one["res"], b["res"])
+        ex = exact_eig_lap(*grid, iv[0], iv[1])
+        assert b["nev"] == len(ex)
+
+
 def test_interleaved_filter_plain_entries_bit_identical(gpu):
     """The interleaved kernel on a matrix without packed entries (random
     edge coefficients: 270 641 distinct values), filters of degrees 225,
