@@ -959,9 +959,28 @@ int spmv(const pevsl_devcsr *A, const double *x, double *y) {
   return launched("spmv");
 }
 
+/* the ELL kernel and its switch (defined with the interleaved kernels) */
+template <int S>
+__global__ void k_cheb_il_e(int n, const short *__restrict__ edj,
+                            const unsigned char *__restrict__ evi, int ew,
+                            const double *__restrict__ vtab, int nv,
+                            const double *__restrict__ Xk, const double *Xkm1, double *Xkp1,
+                            double *Y, double cc, double t, const double *__restrict__ mu0,
+                            const double *__restrict__ muk, double mu0s, double muks, int ny,
+                            int fresh);
+static bool ell_enabled(const pevsl_devcsr *A);
+
 int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, double *vkp1, double *y,
               double cc, double t, double mu0, double muk, int first) {
   if (A->nrows <= 0) return 0;
+  if (A->lanes == 0 && use_packed(A) && ell_enabled(A) && A->nrows >= 65536) {
+    /* one lane per row on the ELL copy: the same bits as the stream kernel */
+    const unsigned g = (unsigned)((A->nrows + kThreads - 1) / kThreads);
+    k_cheb_il_e<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab,
+                                                       A->pnv, vk, vkm1, vkp1, y, cc, t, nullptr,
+                                                       nullptr, mu0, muk, 1, first);
+    return launched("cheb_step_ell");
+  }
   if (A->lanes == 0) {
     launch_stream(A, (const double *)A->a, vk, EpiCheb{vk, vkm1, vkp1, y, cc, t, mu0, muk, first});
     return launched("cheb_step_stream");
@@ -1118,6 +1137,77 @@ __global__ void __launch_bounds__(kThreads)
   if (ny > 0) Y[me] = il_accumulate<S>(ny, fresh, yold, w, x, xm1, mu0, muk, s);
 }
 
+/* k_cheb_il_p on the ELL copy of the packed entries: row r's j-th entry
+ * sits at (r / 32) * 32 * ew + j * 32 + r % 32, so a lane computes its
+ * entries' addresses from its row alone and issues their loads together
+ * with the vector loads -- the row-pointer load and the wait on it are
+ * gone -- then up to eight gathers at once.  Padding (edj = INT16_MIN)
+ * follows a row's entries and is skipped, never added, so the products are
+ * added in the same order as k_cheb_il_p's: the same bits.  S = 1 is the
+ * one-vector degree (y updated every degree with the scalar mu0s / muks,
+ * the arithmetic of cheb_update_v). */
+template <int S>
+__global__ void __launch_bounds__(kThreads)
+    k_cheb_il_e(int n, const short *__restrict__ edj, const unsigned char *__restrict__ evi,
+                int ew, const double *__restrict__ vtab, int nv, const double *__restrict__ Xk,
+                const double *Xkm1, double *Xkp1, double *Y, double cc, double t,
+                const double *__restrict__ mu0, const double *__restrict__ muk, double mu0s,
+                double muks, int ny, int fresh) {
+  __shared__ double vt[256];
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
+  __syncthreads();
+  constexpr int RPW = 32 / S;
+  const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31, s = lane % S;
+  const long row = gw * RPW + lane / S;
+  if (row >= n) return;
+  const int g0 = (int)(row & ~31L);
+  const size_t me = (size_t)row * S + s;
+  const bool read_y = S == 1 ? !fresh : (ny > 0 && !fresh);
+  const double x = Xk[me];
+  const double xm1 = Xkm1 ? Xkm1[me] : 0.0;
+  const double yold = read_y ? Y[me] : 0.0;
+  const size_t b = (size_t)(row >> 5) * 32 * (size_t)ew + (size_t)(row & 31);
+  double r = 0.0;
+  for (int j0 = 0; j0 < ew; j0 += 8) {
+    int dv[8];
+    unsigned iv[8];
+    double xv[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      dv[u] = INT16_MIN;
+      iv[u] = 0;
+      if (j0 + u < ew) {
+        dv[u] = __ldg(edj + b + (size_t)(j0 + u) * 32);
+        iv[u] = __ldg(evi + b + (size_t)(j0 + u) * 32);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+      xv[u] = dv[u] != INT16_MIN ? __ldg(Xk + (size_t)(g0 + dv[u]) * S + s) : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+      if (dv[u] != INT16_MIN) r = __dadd_rn(r, __dmul_rn(vt[iv[u]], xv[u]));
+  }
+  double w = __dmul_rn(__fma_rn(-cc, x, r), t);
+  if (Xkm1) w = __dsub_rn(w, xm1);
+  Xkp1[me] = w;
+  if (S == 1)
+    Y[me] = fresh ? __fma_rn(muks, w, __dmul_rn(mu0s, x)) : __fma_rn(muks, w, yold);
+  else if (ny > 0)
+    Y[me] = il_accumulate<S>(ny, fresh, yold, w, x, xm1, mu0, muk, s);
+}
+
+/* the ELL kernels (PEVSL_B200_ELL=1; off by default until measured) */
+static bool ell_enabled(const pevsl_devcsr *A) {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("PEVSL_B200_ELL");
+    v = e ? atoi(e) != 0 : 0;
+  }
+  return v && A->edj != nullptr;
+}
+
 /* X[i*S + s] = x_s[i] and back */
 __global__ void k_il_pack(long n, int S, CPtrs xs, double *X) {
   for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n * S;
@@ -1189,6 +1279,20 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
   cudaStream_t st = ctx().stream;
+  if (Xg == Xk && il_packed(A) && ell_enabled(A)) {
+#define PV_IL_E(SS)                                                                             \
+  k_cheb_il_e<SS><<<g, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, Xk, \
+                                          Xkm1, Xkp1, Y, cc, t, mu0, muk, 0.0, 0.0, ny, fresh)
+    switch (S) {
+      case 2: PV_IL_E(2); break;
+      case 4: PV_IL_E(4); break;
+      case 8: PV_IL_E(8); break;
+      case 16: PV_IL_E(16); break;
+      default: return PEVSL_ERR_ARG;
+    }
+#undef PV_IL_E
+    return launched("cheb_step_il_ell");
+  }
   if (il_packed(A)) {
 #define PV_IL_P(SS)                                                                          \
   k_cheb_il_p<SS><<<g, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, \
@@ -1380,7 +1484,8 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
     const long g0 = (long)(i & ~31);
     for (int k = Ai->ia[i]; k < Ai->ia[i + 1]; k++) {
       const long off = (long)Ai->ja[k] - g0;
-      if (off < -32768 || off > 32767) return 0;
+      /* INT16_MIN is kept free: it marks the ELL layout's padding */
+      if (off <= -32768 || off > 32767) return 0;
       dj[(size_t)k] = (short)off;
       uint64_t key;
       memcpy(&key, &Ai->a[k], sizeof key);
@@ -1398,8 +1503,32 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
   const size_t b_dj = ((sizeof(short) * (size_t)nnz + 255) / 256) * 256;
   const size_t b_vi = ((size_t)nnz + 255) / 256 * 256;
   const size_t b_tab = 256 * sizeof(double) + 256 * sizeof(float);
-  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab);
+  /* ELL copy: width = the longest row, when that is at most 16 and pads
+   * the entries by less than a quarter */
+  const int ew = d->max_row_nnz;
+  const size_t nslice = ((size_t)nr + 31) / 32;
+  const size_t ecount = nslice * 32 * (size_t)ew;
+  const bool ell = ew >= 1 && ew <= 16 && (double)ecount <= 1.25 * (double)nnz;
+  const size_t b_edj = ell ? (sizeof(short) * ecount + 255) / 256 * 256 : 0;
+  const size_t b_evi = ell ? (ecount + 255) / 256 * 256 : 0;
+  char *base = (char *)alloc_dev(b_dj + b_vi + b_tab + b_edj + b_evi);
   if (!base) return PEVSL_ERR_NOMEM;
+  std::vector<short> edj;
+  std::vector<unsigned char> evi;
+  if (ell) {
+    edj.assign(ecount, (short)INT16_MIN);
+    evi.assign(ecount, 0);
+    for (int i = 0; i < nr; i++) {
+      const size_t b = (size_t)(i / 32) * 32 * (size_t)ew + (size_t)(i % 32);
+      for (int k = Ai->ia[i], j = 0; k < Ai->ia[i + 1]; k++, j++) {
+        edj[b + (size_t)j * 32] = dj[(size_t)k];
+        evi[b + (size_t)j * 32] = vi[(size_t)k];
+      }
+    }
+    d->edj = (short *)(base + b_dj + b_vi + b_tab);
+    d->evi = (unsigned char *)(base + b_dj + b_vi + b_tab + b_edj);
+    d->ew = ew;
+  }
   std::vector<float> tab32(tab.size());
   for (size_t t = 0; t < tab.size(); t++) tab32[t] = (float)tab[t];
   d->pdj = (short *)base;
@@ -1410,6 +1539,8 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
   d->pbytes = b_dj + b_vi + b_tab;
   int st = memcpy_async(d->pdj, dj.data(), sizeof(short) * (size_t)nnz);
   if (!st) st = memcpy_async(d->pvi, vi.data(), (size_t)nnz);
+  if (!st && ell) st = memcpy_async(d->edj, edj.data(), sizeof(short) * ecount);
+  if (!st && ell) st = memcpy_async(d->evi, evi.data(), ecount);
   if (!st) st = memcpy_async(d->pvtab, tab.data(), sizeof(double) * tab.size());
   if (!st) st = memcpy_async(d->pvtab32, tab32.data(), sizeof(float) * tab.size());
   if (!st) st = sync();

@@ -60,6 +60,13 @@ typedef struct pevsl_devcsr {
   float *pvtab32;
   int pnv;
   size_t pbytes;
+  /* the same packed entries in ELL layout (NULL unless every row has at
+   * most ew <= 16 entries and the padding stays under a quarter): row r's
+   * j-th entry at (r / 32) * 32 * ew + j * 32 + r % 32; padding has
+   * edj = INT16_MIN.  A row's entries are addressed from r alone. */
+  short *edj;
+  unsigned char *evi;
+  int ew;
 } pevsl_devcsr;
 
 /* The device matrix behind a Parcsr, or NULL if it was never set up here. */
