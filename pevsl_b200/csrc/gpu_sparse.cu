@@ -1198,11 +1198,84 @@ __global__ void __launch_bounds__(kThreads)
     Y[me] = il_accumulate<S>(ny, fresh, yold, w, x, xm1, mu0, muk, s);
 }
 
-/* the ELL kernels (PEVSL_B200_ELL=1; off by default until measured) */
-static bool ell_enabled(const pevsl_devcsr *A) {
+/* Two interleaved vectors on the ELL copy with one thread per row: each
+ * gather is one 16-byte load of both vectors' entries (X as double2), each
+ * entry's offset and value index are loaded once for both, and the two
+ * products of an entry go to two sums, each added in entry order -- the
+ * bits of k_cheb_il_p<2>. */
+__global__ void __launch_bounds__(kThreads, 4)
+    k_cheb_il2_e(int n, const short *__restrict__ edj, const unsigned char *__restrict__ evi,
+                 int ew, const double *__restrict__ vtab, int nv, const double2 *__restrict__ Xk,
+                 const double2 *Xkm1, double2 *Xkp1, double2 *Y, double cc, double t,
+                 const double *__restrict__ mu0, const double *__restrict__ muk, int ny,
+                 int fresh) {
+  __shared__ double vt[256];
+  for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
+  __syncthreads();
+  const long row = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (row >= n) return;
+  const int g0 = (int)(row & ~31L);
+  const double2 x = Xk[row];
+  const double2 xm1 = Xkm1 ? Xkm1[row] : make_double2(0.0, 0.0);
+  const double2 yold = (ny > 0 && !fresh) ? Y[row] : make_double2(0.0, 0.0);
+  const size_t b = (size_t)(row >> 5) * 32 * (size_t)ew + (size_t)(row & 31);
+  double r0 = 0.0, r1 = 0.0;
+  for (int j0 = 0; j0 < ew; j0 += 8) {
+    int dv[8];
+    unsigned iv[8];
+    double2 xv[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      dv[u] = INT16_MIN;
+      iv[u] = 0;
+      if (j0 + u < ew) {
+        dv[u] = __ldg(edj + b + (size_t)(j0 + u) * 32);
+        iv[u] = __ldg(evi + b + (size_t)(j0 + u) * 32);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+      xv[u] = dv[u] != INT16_MIN ? __ldg(Xk + g0 + dv[u]) : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+      if (dv[u] != INT16_MIN) {
+        const double a = vt[iv[u]];
+        r0 = __dadd_rn(r0, __dmul_rn(a, xv[u].x));
+        r1 = __dadd_rn(r1, __dmul_rn(a, xv[u].y));
+      }
+  }
+  double w0 = __dmul_rn(__fma_rn(-cc, x.x, r0), t);
+  double w1 = __dmul_rn(__fma_rn(-cc, x.y, r1), t);
+  if (Xkm1) {
+    w0 = __dsub_rn(w0, xm1.x);
+    w1 = __dsub_rn(w1, xm1.y);
+  }
+  Xkp1[row] = make_double2(w0, w1);
+  if (ny > 0)
+    Y[row] = make_double2(il_accumulate<2>(ny, fresh, yold.x, w0, x.x, xm1.x, mu0, muk, 0),
+                          il_accumulate<2>(ny, fresh, yold.y, w1, x.y, xm1.y, mu0, muk, 1));
+}
+
+/* The ELL kernels, where the matrix has the ELL copy: one vector (the
+ * one-thread-per-row k_cheb_il_e<1>: 11.8 against 20.8 us per degree for
+ * the stream kernel at 100^3, one B200) by default; several interleaved
+ * vectors only with PEVSL_B200_ELL=1 (k_cheb_il_e<2> measured 21.0 against
+ * 19.8 us for k_cheb_il_p<2>).  PEVSL_B200_ELL=0 turns them off. */
+static int ell_mode() {
+  static int v = -2;
+  if (v == -2) {
+    const char *e = getenv("PEVSL_B200_ELL");
+    v = e ? atoi(e) : -1;
+  }
+  return v;
+}
+static bool ell_enabled(const pevsl_devcsr *A) { return ell_mode() != 0 && A->edj != nullptr; }
+static bool ell_multi(const pevsl_devcsr *A) { return ell_mode() > 0 && A->edj != nullptr; }
+/* the two-vector ELL form (PEVSL_B200_ELL2: 1 on, default off until measured) */
+static bool ell_two(const pevsl_devcsr *A) {
   static int v = -1;
   if (v < 0) {
-    const char *e = getenv("PEVSL_B200_ELL");
+    const char *e = getenv("PEVSL_B200_ELL2");
     v = e ? atoi(e) != 0 : 0;
   }
   return v && A->edj != nullptr;
@@ -1279,7 +1352,15 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   const long rows_per_block = (kThreads / 32) * (32 / S);
   const unsigned g = (unsigned)((A->nrows + rows_per_block - 1) / rows_per_block);
   cudaStream_t st = ctx().stream;
-  if (Xg == Xk && il_packed(A) && ell_enabled(A)) {
+  if (Xg == Xk && il_packed(A) && S == 2 && ell_two(A)) {
+    const unsigned g2 = (unsigned)((A->nrows + kThreads - 1) / kThreads);
+    k_cheb_il2_e<<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+                                          (const double2 *)Xk, (const double2 *)Xkm1,
+                                          (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk, ny,
+                                          fresh);
+    return launched("cheb_step_il2_ell");
+  }
+  if (Xg == Xk && il_packed(A) && ell_multi(A)) {
 #define PV_IL_E(SS)                                                                             \
   k_cheb_il_e<SS><<<g, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, Xk, \
                                           Xkm1, Xkp1, Y, cc, t, mu0, muk, 0.0, 0.0, ny, fresh)
