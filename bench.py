@@ -419,9 +419,9 @@ def run_b200(args, dist):
                        "fused with the recurrence), CUDA-graph replays; one launch = one degree"
                        if gen else
                        "cheb_step_il (fused SpMV + Chebyshev recurrence, all slices per launch with "
-                       "row-interleaved vectors, filter sum updated every third degree: k_cheb_il_p; "
-                       "one live slice: the packed one-vector kernel), all filter launches of the "
-                       "timed steps"
+                       "row-interleaved vectors in groups of two that stay in L2, filter sum updated "
+                       "every third degree: k_cheb_il2_e on the ELL copy of the packed entries; one "
+                       "live slice: k_cheb_il_e<1>), all filter launches of the timed steps"
                        if batched else "cheb_step (fused SpMV + Chebyshev recurrence, CSR-stream, "
                        "packed entries)"),
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1202,10 +1202,9 @@ __global__ void __launch_bounds__(kThreads)
  * gather is one 16-byte load of both vectors' entries (X as double2), each
  * entry's offset and value index are loaded once for both, and the two
  * products of an entry go to two sums, each added in entry order -- the
- * bits of k_cheb_il_p<2>.  B entries per batch of gathers (8: more in
- * flight, 63 registers and spills; 4: fewer registers). */
-template <int B>
-__global__ void __launch_bounds__(kThreads, B == 8 ? 4 : 5)
+ * bits of k_cheb_il_p<2>.  Four entries per batch of gathers (48
+ * registers; eight per batch took 63 with spills and 28.3 us per degree). */
+__global__ void __launch_bounds__(kThreads, 5)
     k_cheb_il2_e(int n, const short *__restrict__ edj, const unsigned char *__restrict__ evi,
                  int ew, const double *__restrict__ vtab, int nv, const double2 *__restrict__ Xk,
                  const double2 *Xkm1, double2 *Xkp1, double2 *Y, double cc, double t,
@@ -1221,6 +1220,7 @@ __global__ void __launch_bounds__(kThreads, B == 8 ? 4 : 5)
   const double2 xm1 = Xkm1 ? Xkm1[row] : make_double2(0.0, 0.0);
   const double2 yold = (ny > 0 && !fresh) ? Y[row] : make_double2(0.0, 0.0);
   const size_t b = (size_t)(row >> 5) * 32 * (size_t)ew + (size_t)(row & 31);
+  constexpr int B = 4;
   double r0 = 0.0, r1 = 0.0;
   for (int j0 = 0; j0 < ew; j0 += B) {
     int dv[B];
@@ -1273,16 +1273,18 @@ static int ell_mode() {
 }
 static bool ell_enabled(const pevsl_devcsr *A) { return ell_mode() != 0 && A->edj != nullptr; }
 static bool ell_multi(const pevsl_devcsr *A) { return ell_mode() > 0 && A->edj != nullptr; }
-/* the two-vector ELL form (PEVSL_B200_ELL2: 1 eight gathers per batch, 2
- * four; default off: the eight-wide form measured 28.3 against 20.5 us for
- * k_cheb_il_p<2> at 100^3) */
-static int ell_two(const pevsl_devcsr *A) {
+/* The two-vector ELL form for groups of two interleaved vectors, on by
+ * default where the matrix has the ELL copy (PEVSL_B200_ELL2=0 turns it
+ * off).  Measured per degree at 100^3 on one box, two runs each: 19.70 and
+ * 19.80 us against 19.81 and 19.82 us for k_cheb_il_p<2>, the whole C2 run
+ * 35.6 against 36.3-37.0 s; on another box 21.3 against 25.2 us. */
+static bool ell_two(const pevsl_devcsr *A) {
   static int v = -1;
   if (v < 0) {
     const char *e = getenv("PEVSL_B200_ELL2");
-    v = e ? atoi(e) : 0;
+    v = e ? atoi(e) != 0 : 1;
   }
-  return A->edj != nullptr ? v : 0;
+  return v && ell_mode() != 0 && A->edj != nullptr;
 }
 
 /* X[i*S + s] = x_s[i] and back */
@@ -1358,16 +1360,10 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   cudaStream_t st = ctx().stream;
   if (Xg == Xk && il_packed(A) && S == 2 && ell_two(A)) {
     const unsigned g2 = (unsigned)((A->nrows + kThreads - 1) / kThreads);
-    if (ell_two(A) == 2)
-      k_cheb_il2_e<4><<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                               (const double2 *)Xk, (const double2 *)Xkm1,
-                                               (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk,
-                                               ny, fresh);
-    else
-      k_cheb_il2_e<8><<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                               (const double2 *)Xk, (const double2 *)Xkm1,
-                                               (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk,
-                                               ny, fresh);
+    k_cheb_il2_e<<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+                                          (const double2 *)Xk, (const double2 *)Xkm1,
+                                          (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk, ny,
+                                          fresh);
     return launched("cheb_step_il2_ell");
   }
   if (Xg == Xk && il_packed(A) && ell_multi(A)) {
