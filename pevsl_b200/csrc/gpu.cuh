@@ -259,6 +259,9 @@ double il_entry_bytes(const pevsl_devcsr *A);
 void matrix_window(const pevsl_devcsr *A);
 /* choose the CSR-stream rows per lane of a matrix by timing (once) */
 int stream_tune(pevsl_devcsr *A);
+/* choose the CSR or ELL form of the one- and two-vector filter degrees of a
+ * packed matrix with an ELL copy by timing both (at set-up) */
+int filter_tune(pevsl_devcsr *A);
 
 /* One entry of the persistent filter: y = p(A) x for its own matrix and
  * polynomial (mu on the device).  FP64 entries: b0, b1 are two work vectors

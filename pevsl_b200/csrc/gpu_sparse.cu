@@ -1263,11 +1263,14 @@ __global__ void __launch_bounds__(kThreads, MINB)
                           il_accumulate<2>(ny, fresh, yold.y, w1, x.y, xm1.y, mu0, muk, 1));
 }
 
-/* The ELL kernels, where the matrix has the ELL copy: one vector (the
- * one-thread-per-row k_cheb_il_e<1>: 11.8 against 20.8 us per degree for
- * the stream kernel at 100^3, one B200) by default; several interleaved
- * vectors only with PEVSL_B200_ELL=1 (k_cheb_il_e<2> measured 21.0 against
- * 19.8 us for k_cheb_il_p<2>).  PEVSL_B200_ELL=0 turns them off. */
+/* Which filter-degree form runs, where the matrix has the ELL copy.  One
+ * vector: k_cheb_il_e<1> or the CSR-stream kernel; groups of two:
+ * k_cheb_il2_e or k_cheb_il_p<2> -- each chosen per matrix by timing both
+ * on this GPU at set-up (filter_tune; measured at 100^3: one vector 11.8
+ * against 20.8 us, groups of two 19.7-21.3 against 19.8-25.2 us from box to
+ * box).  PEVSL_B200_ELL: 0 never ELL, 1 always (and k_cheb_il_e<S> for
+ * wider groups, measured 21.0 against 19.8 us at two); PEVSL_B200_ELL2:
+ * 0 / 1 forces the form of the groups of two. */
 static int ell_mode() {
   static int v = -2;
   if (v == -2) {
@@ -1276,20 +1279,112 @@ static int ell_mode() {
   }
   return v;
 }
-static bool ell_enabled(const pevsl_devcsr *A) { return ell_mode() != 0 && A->edj != nullptr; }
-static bool ell_multi(const pevsl_devcsr *A) { return ell_mode() > 0 && A->edj != nullptr; }
-/* The two-vector ELL form for groups of two interleaved vectors, on by
- * default where the matrix has the ELL copy (PEVSL_B200_ELL2=0 turns it
- * off).  Measured per degree at 100^3 on one box, two runs each: 19.70 and
- * 19.80 us against 19.81 and 19.82 us for k_cheb_il_p<2>, the whole C2 run
- * 35.6 against 36.3-37.0 s; on another box 21.3 against 25.2 us. */
-static bool ell_two(const pevsl_devcsr *A) {
-  static int v = -1;
-  if (v < 0) {
+static int ell2_mode() {
+  static int v = -2;
+  if (v == -2) {
     const char *e = getenv("PEVSL_B200_ELL2");
-    v = e ? atoi(e) != 0 : 1;
+    v = e ? (atoi(e) != 0) : -1;
   }
-  return v && ell_mode() != 0 && A->edj != nullptr;
+  return v;
+}
+static bool ell_enabled(const pevsl_devcsr *A) {
+  if (!A->edj || ell_mode() == 0) return false;
+  return ell_mode() > 0 || A->ell1;
+}
+static bool ell_multi(const pevsl_devcsr *A) { return ell_mode() > 0 && A->edj != nullptr; }
+static bool ell_two(const pevsl_devcsr *A) {
+  if (!A->edj || ell_mode() == 0) return false;
+  if (ell2_mode() >= 0) return ell2_mode() == 1;
+  return ell_mode() > 0 || A->ell2;
+}
+
+/* Choose the filter-degree forms of a packed matrix with an ELL copy by
+ * timing both on this GPU: one vector (CSR-stream against k_cheb_il_e<1>)
+ * and groups of two interleaved vectors (k_cheb_il_p<2> against
+ * k_cheb_il2_e), ten launches each after three warm-up ones, two rounds in
+ * alternating order, on scratch vectors.  Both forms give the same bits, so
+ * the choice never changes a result.  Runs at set-up, outside any capture;
+ * about 2 ms at 100^3. */
+int filter_tune(pevsl_devcsr *A) {
+  A->ell1 = A->ell2 = 0;
+  if (!A->edj || A->nrows < 65536) return 0;
+  if (ell_mode() == 0) return 0;
+  if (ell_mode() > 0) {
+    A->ell1 = A->ell2 = 1;
+    return 0;
+  }
+  const long n = A->nrows;
+  double *buf = nullptr;
+  if (cudaMalloc(&buf, sizeof(double) * (8 * (size_t)n + 64)) != cudaSuccess) {
+    cudaGetLastError();
+    A->ell1 = A->ell2 = 1; /* untimed: the forms measured faster */
+    return 0;
+  }
+  cudaStream_t st = ctx().stream;
+  cudaMemsetAsync(buf, 0, sizeof(double) * (8 * (size_t)n + 64), st);
+  double *X = buf, *Xm = buf + 2 * n, *Xp = buf + 4 * n, *Y = buf + 6 * n, *mu = buf + 8 * n;
+  const unsigned g1 = (unsigned)((n + kThreads - 1) / kThreads);
+  const unsigned g2 = (unsigned)((n + (kThreads / 2) - 1) / (kThreads / 2));
+  const EpiCheb epi{X, Xm, Xp, Y, 0.5, 0.5, 0.0, 0.5, 0};
+  auto one_csr = [&] {
+    k_csr_stream_packed<double, EpiCheb><<<stream_grid(A->nrows, 1), kThreads, 0, st>>>(
+        A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, X, epi);
+  };
+  auto one_ell = [&] {
+    k_cheb_il_e<1><<<g1, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, X,
+                                            Xm, Xp, Y, 0.5, 0.5, nullptr, nullptr, 0.0, 0.5, 1, 0);
+  };
+  auto two_csr = [&] {
+    k_cheb_il_p<2><<<g2, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, X,
+                                            X, Xm, Xp, Y, 0.5, 0.5, mu, mu + 2, 0, 0);
+  };
+  auto two_ell = [&] {
+    k_cheb_il2_e<5><<<g1, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+                                             (const double2 *)X, (const double2 *)Xm,
+                                             (double2 *)Xp, (double2 *)Y, 0.5, 0.5, mu, mu + 2, 0,
+                                             0);
+  };
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  auto timed = [&](auto &&launch) {
+    for (int i = 0; i < 3; i++) launch();
+    cudaEventRecord(e0, st);
+    for (int i = 0; i < 10; i++) launch();
+    cudaEventRecord(e1, st);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  float t1c = 0.f, t1e = 0.f, t2c = 0.f, t2e = 0.f;
+  for (int round = 0; round < 2; round++) {
+    if (round == 0) {
+      t1c += timed(one_csr);
+      t1e += timed(one_ell);
+      t2c += timed(two_csr);
+      t2e += timed(two_ell);
+    } else {
+      t1e += timed(one_ell);
+      t1c += timed(one_csr);
+      t2e += timed(two_ell);
+      t2c += timed(two_csr);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(st);
+  cudaFree(buf);
+  if (fail(cudaGetLastError(), "filter_tune")) return PEVSL_ERR_CUDA;
+  ctx().launches += 4 * 2 * 13;
+  A->ell1 = t1e > 0.f && t1e < t1c;
+  A->ell2 = t2e > 0.f && t2e < t2c;
+  if (getenv("PEVSL_B200_VERBOSE"))
+    fprintf(stderr,
+            "filter_tune n=%ld: one vector CSR %.2f / ELL %.2f us, two vectors CSR %.2f / ELL "
+            "%.2f us -> ell1 %d ell2 %d\n",
+            n, t1c * 50.f, t1e * 50.f, t2c * 50.f, t2e * 50.f, A->ell1, A->ell2);
+  return 0;
 }
 
 /* X[i*S + s] = x_s[i] and back */
@@ -1652,6 +1747,7 @@ static int pack_entries(pevsl_devcsr *d, const pevsl_Csr *Ai) {
   if (!st) st = memcpy_async(d->pvtab, tab.data(), sizeof(double) * tab.size());
   if (!st) st = memcpy_async(d->pvtab32, tab32.data(), sizeof(float) * tab.size());
   if (!st) st = sync();
+  if (!st && ell) st = filter_tune(d);
   return st;
 }
 

@@ -67,6 +67,10 @@ typedef struct pevsl_devcsr {
   short *edj;
   unsigned char *evi;
   int ew;
+  /* the filter-degree forms chosen for this matrix by timing both on the
+   * GPU at set-up (filter_tune): one vector and groups of two on the ELL
+   * copy (1) or on the packed CSR entries (0) */
+  int ell1, ell2;
 } pevsl_devcsr;
 
 /* The device matrix behind a Parcsr, or NULL if it was never set up here. */
