@@ -1202,10 +1202,12 @@ __global__ void __launch_bounds__(kThreads)
  * gather is one 16-byte load of both vectors' entries (X as double2), each
  * entry's offset and value index are loaded once for both, and the two
  * products of an entry go to two sums, each added in entry order -- the
- * bits of k_cheb_il_p<2>.  Four entries per batch of gathers (48
- * registers; eight per batch took 63 with spills and 28.3 us per degree). */
-template <int MINB>
-__global__ void __launch_bounds__(kThreads, MINB)
+ * bits of k_cheb_il_p<2>.  Four entries per batch of gathers, 48 registers,
+ * five blocks per SM.  Measured per degree at 100^3 on one box: 19.8 us;
+ * built for six blocks (40 registers, Y loaded after the gathers) 20.2-21.1
+ * us, for eight (32 registers, spills) 24.7-28.1 us; eight entries per
+ * batch (63 registers, spills) 28.3 us. */
+__global__ void __launch_bounds__(kThreads, 5)
     k_cheb_il2_e(int n, const short *__restrict__ edj, const unsigned char *__restrict__ evi,
                  int ew, const double *__restrict__ vtab, int nv, const double2 *__restrict__ Xk,
                  const double2 *Xkm1, double2 *Xkp1, double2 *Y, double cc, double t,
@@ -1219,10 +1221,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
   const int g0 = (int)(row & ~31L);
   const double2 x = Xk[row];
   const double2 xm1 = Xkm1 ? Xkm1[row] : make_double2(0.0, 0.0);
-  /* MINB > 5: Y (needed by the epilogue of one launch in three) is loaded
-   * after the gathers, shortening its live range */
-  double2 yold = make_double2(0.0, 0.0);
-  if (MINB <= 5 && ny > 0 && !fresh) yold = Y[row];
+  const double2 yold = (ny > 0 && !fresh) ? Y[row] : make_double2(0.0, 0.0);
   const size_t b = (size_t)(row >> 5) * 32 * (size_t)ew + (size_t)(row & 31);
   constexpr int B = 4;
   double r0 = 0.0, r1 = 0.0;
@@ -1257,7 +1256,6 @@ __global__ void __launch_bounds__(kThreads, MINB)
     w1 = __dsub_rn(w1, xm1.y);
   }
   Xkp1[row] = make_double2(w0, w1);
-  if (MINB > 5 && ny > 0 && !fresh) yold = Y[row];
   if (ny > 0)
     Y[row] = make_double2(il_accumulate<2>(ny, fresh, yold.x, w0, x.x, xm1.x, mu0, muk, 0),
                           il_accumulate<2>(ny, fresh, yold.y, w1, x.y, xm1.y, mu0, muk, 1));
@@ -1339,10 +1337,9 @@ int filter_tune(pevsl_devcsr *A) {
                                             X, Xm, Xp, Y, 0.5, 0.5, mu, mu + 2, 0, 0);
   };
   auto two_ell = [&] {
-    k_cheb_il2_e<5><<<g1, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                             (const double2 *)X, (const double2 *)Xm,
-                                             (double2 *)Xp, (double2 *)Y, 0.5, 0.5, mu, mu + 2, 0,
-                                             0);
+    k_cheb_il2_e<<<g1, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+                                          (const double2 *)X, (const double2 *)Xm, (double2 *)Xp,
+                                          (double2 *)Y, 0.5, 0.5, mu, mu + 2, 0, 0);
   };
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -1460,26 +1457,10 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   cudaStream_t st = ctx().stream;
   if (Xg == Xk && il_packed(A) && S == 2 && ell_two(A)) {
     const unsigned g2 = (unsigned)((A->nrows + kThreads - 1) / kThreads);
-    static int occ = -1; /* PEVSL_B200_IL2_OCC=6 or 8: the six / eight blocks per SM builds */
-    if (occ < 0) {
-      const char *e = getenv("PEVSL_B200_IL2_OCC");
-      occ = e ? atoi(e) : 5;
-    }
-    if (occ == 8)
-      k_cheb_il2_e<8><<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                               (const double2 *)Xk, (const double2 *)Xkm1,
-                                               (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk,
-                                               ny, fresh);
-    else if (occ == 6)
-      k_cheb_il2_e<6><<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                               (const double2 *)Xk, (const double2 *)Xkm1,
-                                               (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk,
-                                               ny, fresh);
-    else
-      k_cheb_il2_e<5><<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                               (const double2 *)Xk, (const double2 *)Xkm1,
-                                               (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk,
-                                               ny, fresh);
+    k_cheb_il2_e<<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+                                          (const double2 *)Xk, (const double2 *)Xkm1,
+                                          (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk, ny,
+                                          fresh);
     return launched("cheb_step_il2_ell");
   }
   if (Xg == Xk && il_packed(A) && ell_multi(A)) {
