@@ -30,6 +30,50 @@
 
 namespace pv {
 
+/* Programmatic dependent launch of the ELL filter-degree kernels.  A degree
+ * launched with the stream-serialisation attribute may be scheduled while
+ * the previous degree's last blocks still run: its blocks stage the value
+ * table in shared memory, then wait (griddepcontrol.wait) until the
+ * previous grid has completed and its writes are visible, and only then
+ * read a vector.  A block lets the next degree be scheduled
+ * (griddepcontrol.launch_dependents) only after its own wait, so the early
+ * part of degree k+1 overlaps degree k and nothing older.  What the early
+ * part reads, the value table, is written at set-up, followed by a device
+ * synchronisation, and never again while the matrix lives.  Without the
+ * attribute the wait returns at once.  (Loading the first entries of a row
+ * before the wait as well took the one-vector kernel from 32 to 48
+ * registers and measured slower.) */
+__device__ __forceinline__ void pdl_wait_then_release() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+/* PEVSL_B200_PDL: 1 (default) launches the ELL filter degrees with the
+ * attribute, 0 as plain stream-ordered launches */
+static int pdl_mode() {
+  static int v = -1;
+  if (v < 0) {
+    const char *e = getenv("PEVSL_B200_PDL");
+    v = e ? atoi(e) != 0 : 1;
+  }
+  return v;
+}
+
+template <class... KA, class... AA>
+static void launch_pdl(void (*k)(KA...), unsigned grid, cudaStream_t st, AA &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = pdl_mode();
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, std::forward<AA>(args)...);
+}
+
 template <int L>
 __device__ __forceinline__ unsigned group_mask() {
   if constexpr (L == 32) {
@@ -345,6 +389,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   __shared__ T vt[256];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
   __syncthreads();
+  pdl_wait_then_release();
   stream_rows_e<1, T, Epi, true>(n, ia, EntriesPacked<T>{dj, vi, vt}, x, epi, blockIdx.x, prod);
 }
 
@@ -354,6 +399,7 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 5 : 1)
     k_csr_stream(int n, const int *__restrict__ ia, const int *__restrict__ ja,
                  const T *__restrict__ a, const T *__restrict__ x, Epi epi) {
   __shared__ T prod[kThreads / 32][kStreamChunk * R];
+  pdl_wait_then_release();
   stream_rows<R>(n, ia, ja, a, x, epi, blockIdx.x, prod);
 }
 
@@ -384,6 +430,7 @@ __global__ void __launch_bounds__(kThreads, R == 1 ? 4 : 1)
     k_csr_stream_batch(int n0, const int *__restrict__ ia0, const int *__restrict__ ja0,
                        const T *__restrict__ a0, const __grid_constant__ StreamBatch<T, Epi, CAP> b) {
   __shared__ T prod[kThreads / 32][kStreamChunk * R];
+  pdl_wait_then_release();
   if constexpr (SHARED) {
     const int e = (int)(blockIdx.x % (unsigned)b.nb);
     stream_rows<R>(n0, ia0, ja0, a0, (const T *)b.epi[e].vk, b.epi[e],
@@ -410,6 +457,7 @@ __global__ void __launch_bounds__(kThreads, 4)
   __shared__ T vt[256];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
   __syncthreads();
+  pdl_wait_then_release();
   const int e = (int)(blockIdx.x % (unsigned)b.nb);
   stream_rows_e<1, T, Epi, true>(n0, ia0, EntriesPacked<T>{dj, vi, vt}, (const T *)b.epi[e].vk,
                                  b.epi[e], (long)(blockIdx.x / (unsigned)b.nb), prod);
@@ -812,11 +860,11 @@ int stream_tune(pevsl_devcsr *A) {
     for (int it = 0; it < 6; it++) {
       if (it == 1) cudaEventRecord(e0, st);
       if (R == 2)
-        k_csr_stream<2><<<stream_grid(n, 2), kThreads, 0, st>>>(A->nrows, A->ia, A->ja,
-                                                                (const double *)A->a, x, epi);
+        launch_pdl(k_csr_stream<2, double, EpiCheb>, stream_grid(n, 2), st, A->nrows, A->ia, A->ja,
+                   (const double *)A->a, x, epi);
       else
-        k_csr_stream<1><<<stream_grid(n, 1), kThreads, 0, st>>>(A->nrows, A->ia, A->ja,
-                                                                (const double *)A->a, x, epi);
+        launch_pdl(k_csr_stream<1, double, EpiCheb>, stream_grid(n, 1), st, A->nrows, A->ia, A->ja,
+                   (const double *)A->a, x, epi);
     }
     cudaEventRecord(e1, st);
     cudaEventSynchronize(e1);
@@ -882,8 +930,8 @@ static const T *packed_table(const pevsl_devcsr *A) {
 template <class T, class Epi>
 static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const Epi &epi) {
   if (use_packed(A)) {
-    k_csr_stream_packed<T, Epi><<<stream_grid(A->nrows, 1), kThreads, 0, ctx().stream>>>(
-        A->nrows, A->ia, A->pdj, A->pvi, packed_table<T>(A), A->pnv, x, epi);
+    launch_pdl(k_csr_stream_packed<T, Epi>, stream_grid(A->nrows, 1), ctx().stream, A->nrows,
+               A->ia, A->pdj, A->pvi, packed_table<T>(A), A->pnv, x, epi);
     return;
   }
   if (!A->stream_r) {
@@ -892,11 +940,11 @@ static void launch_stream(const pevsl_devcsr *A, const T *a, const T *x, const E
       stream_tune(const_cast<pevsl_devcsr *>(A));
   }
   if (stream_r(A) == 2)
-    k_csr_stream<2><<<stream_grid(A->nrows, 2), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja,
-                                                                             a, x, epi);
+    launch_pdl(k_csr_stream<2, T, Epi>, stream_grid(A->nrows, 2), ctx().stream, A->nrows, A->ia,
+               A->ja, a, x, epi);
   else
-    k_csr_stream<1><<<stream_grid(A->nrows, 1), kThreads, 0, ctx().stream>>>(A->nrows, A->ia, A->ja,
-                                                                             a, x, epi);
+    launch_pdl(k_csr_stream<1, T, Epi>, stream_grid(A->nrows, 1), ctx().stream, A->nrows, A->ia,
+               A->ja, a, x, epi);
 }
 
 /* fill the table from the entries (matrices from e[i].A) and launch */
@@ -933,18 +981,18 @@ static int launch_stream_batch(int nb, const ChebEntry *en, Make make, const cha
     const pevsl_devcsr *A = en[0].A;
     const long rb = (n0 + kThreads - 1) / kThreads;
     const unsigned gp = (unsigned)(rb * nb);
-    k_csr_stream_batch_packed<T, Epi, CAP><<<gp, kThreads, 0, ctx().stream>>>(
-        n0, ia0, A->pdj, A->pvi, packed_table<T>(A), A->pnv, b);
+    launch_pdl(k_csr_stream_batch_packed<T, Epi, CAP>, gp, ctx().stream, n0, ia0, A->pdj, A->pvi,
+               packed_table<T>(A), A->pnv, b);
   } else if (b.shared) {
     if (R == 2)
-      k_csr_stream_batch<2, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+      launch_pdl(k_csr_stream_batch<2, T, Epi, CAP, true>, g, ctx().stream, n0, ia0, ja0, a0, b);
     else
-      k_csr_stream_batch<1, T, Epi, CAP, true><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+      launch_pdl(k_csr_stream_batch<1, T, Epi, CAP, true>, g, ctx().stream, n0, ia0, ja0, a0, b);
   } else {
     if (R == 2)
-      k_csr_stream_batch<2, T, Epi, CAP, false><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+      launch_pdl(k_csr_stream_batch<2, T, Epi, CAP, false>, g, ctx().stream, n0, ia0, ja0, a0, b);
     else
-      k_csr_stream_batch<1, T, Epi, CAP, false><<<g, kThreads, 0, ctx().stream>>>(n0, ia0, ja0, a0, b);
+      launch_pdl(k_csr_stream_batch<1, T, Epi, CAP, false>, g, ctx().stream, n0, ia0, ja0, a0, b);
   }
   return launched(what);
 }
@@ -976,9 +1024,8 @@ int cheb_step(const pevsl_devcsr *A, const double *vk, const double *vkm1, doubl
   if (A->lanes == 0 && use_packed(A) && ell_enabled(A) && A->nrows >= 65536) {
     /* one lane per row on the ELL copy: the same bits as the stream kernel */
     const unsigned g = (unsigned)((A->nrows + kThreads - 1) / kThreads);
-    k_cheb_il_e<1><<<g, kThreads, 0, ctx().stream>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab,
-                                                       A->pnv, vk, vkm1, vkp1, y, cc, t, nullptr,
-                                                       nullptr, mu0, muk, 1, first);
+    launch_pdl(k_cheb_il_e<1>, g, ctx().stream, A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+               vk, vkm1, vkp1, y, cc, t, nullptr, nullptr, mu0, muk, 1, first);
     return launched("cheb_step_ell");
   }
   if (A->lanes == 0) {
@@ -1104,6 +1151,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ double vt[256];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
   __syncthreads();
+  pdl_wait_then_release();
   constexpr int RPW = 32 / S;
   const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, s = lane % S;
@@ -1156,6 +1204,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ double vt[256];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
   __syncthreads();
+  pdl_wait_then_release();
   constexpr int RPW = 32 / S;
   const long gw = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, s = lane % S;
@@ -1216,6 +1265,7 @@ __global__ void __launch_bounds__(kThreads, 5)
   __shared__ double vt[256];
   for (int i = threadIdx.x; i < nv; i += blockDim.x) vt[i] = vtab[i];
   __syncthreads();
+  pdl_wait_then_release();
   const long row = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (row >= n) return;
   const int g0 = (int)(row & ~31L);
@@ -1325,21 +1375,21 @@ int filter_tune(pevsl_devcsr *A) {
   const unsigned g2 = (unsigned)((n + (kThreads / 2) - 1) / (kThreads / 2));
   const EpiCheb epi{X, Xm, Xp, Y, 0.5, 0.5, 0.0, 0.5, 0};
   auto one_csr = [&] {
-    k_csr_stream_packed<double, EpiCheb><<<stream_grid(A->nrows, 1), kThreads, 0, st>>>(
-        A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, X, epi);
+    launch_pdl(k_csr_stream_packed<double, EpiCheb>, stream_grid(A->nrows, 1), st, A->nrows, A->ia,
+               A->pdj, A->pvi, A->pvtab, A->pnv, X, epi);
   };
   auto one_ell = [&] {
-    k_cheb_il_e<1><<<g1, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, X,
-                                            Xm, Xp, Y, 0.5, 0.5, nullptr, nullptr, 0.0, 0.5, 1, 0);
+    launch_pdl(k_cheb_il_e<1>, g1, st, A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, X, Xm,
+               Xp, Y, 0.5, 0.5, nullptr, nullptr, 0.0, 0.5, 1, 0);
   };
   auto two_csr = [&] {
     k_cheb_il_p<2><<<g2, kThreads, 0, st>>>(A->nrows, A->ia, A->pdj, A->pvi, A->pvtab, A->pnv, X,
                                             X, Xm, Xp, Y, 0.5, 0.5, mu, mu + 2, 0, 0);
   };
   auto two_ell = [&] {
-    k_cheb_il2_e<<<g1, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                          (const double2 *)X, (const double2 *)Xm, (double2 *)Xp,
-                                          (double2 *)Y, 0.5, 0.5, mu, mu + 2, 0, 0);
+    launch_pdl(k_cheb_il2_e, g1, st, A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+               (const double2 *)X, (const double2 *)Xm, (double2 *)Xp, (double2 *)Y, 0.5, 0.5, mu,
+               mu + 2, 0, 0);
   };
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
@@ -1457,16 +1507,15 @@ int cheb_step_il_y(const pevsl_devcsr *A, int S, const double *Xg, const double 
   cudaStream_t st = ctx().stream;
   if (Xg == Xk && il_packed(A) && S == 2 && ell_two(A)) {
     const unsigned g2 = (unsigned)((A->nrows + kThreads - 1) / kThreads);
-    k_cheb_il2_e<<<g2, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
-                                          (const double2 *)Xk, (const double2 *)Xkm1,
-                                          (double2 *)Xkp1, (double2 *)Y, cc, t, mu0, muk, ny,
-                                          fresh);
+    launch_pdl(k_cheb_il2_e, g2, st, A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv,
+               (const double2 *)Xk, (const double2 *)Xkm1, (double2 *)Xkp1, (double2 *)Y, cc, t,
+               mu0, muk, ny, fresh);
     return launched("cheb_step_il2_ell");
   }
   if (Xg == Xk && il_packed(A) && ell_multi(A)) {
 #define PV_IL_E(SS)                                                                             \
-  k_cheb_il_e<SS><<<g, kThreads, 0, st>>>(A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, Xk, \
-                                          Xkm1, Xkp1, Y, cc, t, mu0, muk, 0.0, 0.0, ny, fresh)
+  launch_pdl(k_cheb_il_e<SS>, g, st, A->nrows, A->edj, A->evi, A->ew, A->pvtab, A->pnv, Xk, Xkm1, \
+             Xkp1, Y, cc, t, mu0, muk, 0.0, 0.0, ny, fresh)
     switch (S) {
       case 2: PV_IL_E(2); break;
       case 4: PV_IL_E(4); break;
