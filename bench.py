@@ -636,7 +636,9 @@ def run_reference(args, dist):
     on this workload, one process per slice as the reference's MPI groups.
     A step times a bounded sample: each process runs the reference's
     pEVSL_ChebAv with its slice's filter (pEVSL_FindPol on the reference's
-    own slice ends) for about 20 s; the time of the whole run is
+    own slice ends) for 180 s / (warm-up + timed steps), between 2 and 20 s,
+    so that the whole arm ends within about four minutes at any step count
+    (the driver's 25 steps: about 7 s each); the time of the whole run is
     extrapolated from it to the per-slice filter degrees and Lanczos steps
     of the reference's own run of the workload (ref_golden)."""
     if dist.rank != 0:
@@ -676,13 +678,15 @@ def run_reference(args, dist):
     cores = min(os.cpu_count() or 1, nsl)
     ctx = mp.get_context("spawn")
     times, per = [], []
+    sample_target = min(20.0, max(2.0, 180.0 / max(1, args.warmup + args.steps)))
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         q = ctx.Queue()
         procs = []
         for s in range(nsl):
             deg, cc, dd, mu = filters[s]
-            p = ctx.Process(target=_ref_slice_worker, args=(q, n, ia, ja, a, deg, cc, dd, mu, 20.0))
+            p = ctx.Process(target=_ref_slice_worker,
+                            args=(q, n, ia, ja, a, deg, cc, dd, mu, sample_target))
             p.start()
             procs.append(p)
         per = [q.get() for _ in procs]
@@ -700,7 +704,8 @@ def run_reference(args, dist):
     sample_s = float(np.mean(times)) if times else 0.0
     measured = g.get("seconds_per_slice")
     how = (f"reference pEVSL_ChebAv (oracle/_ref, one core per process, {nsl} processes in "
-           f"parallel) for ~20 s per slice with each slice's own filter: {per_deg*1e3:.2f} ms per "
+           f"parallel) for ~{sample_target:.0f} s per slice and step with each slice's own "
+           f"filter: {per_deg*1e3:.2f} ms per "
            f"degree; extrapolated x{total_t / max(sample_s, 1e-9):.0f} to the reference run's "
            f"per-slice Lanczos steps {g['its']} and filter degrees {g['deg']} "
            f"({g['fixture']}) + the KPM matvecs split over {cores} processes + <=200 bounds "
