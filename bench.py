@@ -631,6 +631,12 @@ def ref_golden(workload):
         "fixture": name + (f":{key}" if key else "")}
 
 
+def reference_sample_seconds(warmup, steps):
+    """Seconds of the reference's pEVSL_ChebAv each slice process runs per
+    step of the reference arm: 180 s over all steps, between 2 and 20 s."""
+    return min(20.0, max(2.0, 180.0 / max(1, warmup + steps)))
+
+
 def run_reference(args, dist):
     """The reference's own CPU code (oracle/_ref, compiled from its sources)
     on this workload, one process per slice as the reference's MPI groups.
@@ -678,7 +684,7 @@ def run_reference(args, dist):
     cores = min(os.cpu_count() or 1, nsl)
     ctx = mp.get_context("spawn")
     times, per = [], []
-    sample_target = min(20.0, max(2.0, 180.0 / max(1, args.warmup + args.steps)))
+    sample_target = reference_sample_seconds(args.warmup, args.steps)
     for it in range(args.warmup + args.steps):
         t0 = time.perf_counter()
         q = ctx.Queue()

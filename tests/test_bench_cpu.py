@@ -49,3 +49,17 @@ def test_reference_arm_contract_and_isolation():
     assert out["config"]["nev_per_slice"] == g["nev"]
     loaded = [ln for ln in p.stdout.splitlines() if ln.startswith("LOADED")]
     assert loaded == ["LOADED False True"]
+
+
+def test_reference_arm_fits_the_drivers_step_counts():
+    """The reference arm's per-step sample shrinks with the step count so the
+    whole arm stays near three minutes of sampling: 20 s per step for the
+    default few steps, about 7 s at the driver's 5 + 20, never under 2 s."""
+    sys.path.insert(0, ROOT)
+    import bench
+    assert bench.reference_sample_seconds(3, 1) == 20.0
+    assert abs(bench.reference_sample_seconds(5, 20) - 7.2) < 1e-12
+    assert bench.reference_sample_seconds(50, 200) == 2.0
+    for w, k in ((3, 1), (5, 20), (10, 100)):
+        assert (w + k) * bench.reference_sample_seconds(w, k) <= 200.0 + 1e-9 or \
+            bench.reference_sample_seconds(w, k) == 2.0
