@@ -1381,9 +1381,11 @@ static Il2Kernel il2_kernel(int ew) {
 /* Which filter-degree form runs, where the matrix has the ELL copy.  One
  * vector: k_cheb_il_e<1> or the CSR-stream kernel; groups of two:
  * k_cheb_il2_e or k_cheb_il_p<2> -- each chosen per matrix by timing both
- * on this GPU at set-up (filter_tune; measured at 100^3: one vector 11.8
- * against 20.8 us, groups of two 19.7-21.3 against 19.8-25.2 us from box to
- * box).  PEVSL_B200_ELL: 0 never ELL, 1 always (and k_cheb_il_e<S> for
+ * on this GPU at set-up (filter_tune; measured at 100^3 with the any-width
+ * ELL builds: one vector 11.8 against 20.8 us, groups of two 19.7-21.3
+ * against 19.8-25.2 us from box to box; the width-7 builds: 11.4 and
+ * 16.4-16.6 us).  Under a profiler that serialises launches the timings
+ * are not a run's: force the forms there.  PEVSL_B200_ELL: 0 never ELL, 1 always (and k_cheb_il_e<S> for
  * wider groups, measured 21.0 against 19.8 us at two); PEVSL_B200_ELL2:
  * 0 / 1 forces the form of the groups of two. */
 static int ell_mode() {
